@@ -1,0 +1,270 @@
+/*
+ * efie_b200.h -- C ABI of the B200-native EFIE method-of-moments hot path.
+ *
+ * Drop-in boundary for the reference's CUDA MEX entry points
+ * (mahmut26/Matlab-cuda-efief-vs-cpu).  Every entry point takes plain host
+ * pointers laid out exactly as MATLAB hands them to a MEX function:
+ * column-major arrays, 1-based int32 index values, complex128 as interleaved
+ * (re, im) pairs.  No torch or CUDA types appear in the signatures.  A MEX
+ * wrapper only marshals mxArray <-> pointers and maps efie_status to the
+ * reference's error identifiers with efie_status_id().
+ *
+ * Threading: a context is not thread-safe; use one context per host thread.
+ * Errors never leak device memory: buffers are owned by the context (or plan)
+ * and released by efie_ctx_destroy / efie_plan_destroy.
+ */
+#ifndef EFIE_B200_H
+#define EFIE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } efie_c128;
+
+/* Status codes.  efie_status_id() returns the reference's mexErrMsgIdAndTxt
+ * identifier for each (e.g. "mex:port"); the message of the last failure on
+ * the calling thread is returned by efie_last_error(). */
+typedef enum efie_status {
+    EFIE_OK = 0,
+    EFIE_ERR_ARGS = 1,        /* mex:args     */
+    EFIE_ERR_V = 2,           /* mex:V        */
+    EFIE_ERR_F = 3,           /* mex:F        */
+    EFIE_ERR_E = 4,           /* mex:E        */
+    EFIE_ERR_RWG = 5,         /* mex:rwg  (plusTri/minusTri/sign/rp/rm/Ap/Am/len) */
+    EFIE_ERR_PORT = 6,        /* mex:port     */
+    EFIE_ERR_PREPACK = 7,     /* mex:prepack  */
+    EFIE_ERR_R_REG = 8,       /* mex:r_reg    */
+    EFIE_ERR_W_REG = 9,       /* mex:w_reg    */
+    EFIE_ERR_NEARMAT = 10,    /* mex:nearMat  */
+    EFIE_ERR_SELF_R = 11,     /* mex:self_r   */
+    EFIE_ERR_SELF_W = 12,     /* mex:self_w   */
+    EFIE_ERR_SELF_A = 13,     /* mex:self_a   */
+    EFIE_ERR_NEAR_R = 14,     /* mex:near_r   */
+    EFIE_ERR_NEAR_W = 15,     /* mex:near_w   */
+    EFIE_ERR_AEQTRI = 16,     /* mex:aeqTri   */
+    EFIE_ERR_RHS = 17,        /* mex:rhs      */
+    EFIE_ERR_EPS = 18,        /* mex:eps      */
+    EFIE_ERR_EXC = 19,        /* mex:exc      */
+    EFIE_ERR_FREQS = 20,      /* mex:freqs    */
+    EFIE_ERR_CUDA = 21,       /* cuda:rt      */
+    EFIE_ERR_CUSOLVER = 22,   /* cuda:cusolver */
+    EFIE_ERR_SINGULAR = 23,   /* efie:singular  (LU pivot zero; the reference never checks info) */
+    EFIE_ERR_NOMEM = 24,      /* efie:nomem     */
+    EFIE_ERR_TIMEOUT = 25,    /* efie:timeout   (a bounded device wait gave up) */
+    EFIE_ERR_MESH = 26        /* efie:mesh      (topology error in the mesh builders) */
+} efie_status;
+
+const char *efie_status_id(efie_status s);
+const char *efie_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Context                                                                 */
+/* ---------------------------------------------------------------------- */
+typedef struct efie_ctx efie_ctx;
+
+efie_status efie_ctx_create(int device, efie_ctx **out);
+void efie_ctx_destroy(efie_ctx *ctx);
+/* Launch every kernel of this context on `stream` (a cudaStream_t, 0 = the
+ * context's own stream). */
+efie_status efie_ctx_set_stream(efie_ctx *ctx, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Boundary data: the arrays the MEX entry points receive                  */
+/* ---------------------------------------------------------------------- */
+
+/* V,F,E,plusTri,minusTri,plusSign,minusSign,rp,rm,Ap,Am,len
+ * (patch_sweep_fastquad_cuda.cu:463-471; ggassemble_ZV_EFIE_RWG_DIFF_GPU_FAST.cu:548-559) */
+typedef struct efie_mesh {
+    int32_t Nv, Nt, Ne;
+    const double *V;           /* [Nv x 3]                           */
+    const int32_t *F;          /* [Nt x 3] 1-based                   */
+    const int32_t *E;          /* [Ne x 2] 1-based  (rwg.edge)       */
+    const int32_t *plusTri;    /* [Ne] 1-based                       */
+    const int32_t *minusTri;   /* [Ne] 1-based                       */
+    const int32_t *plusSign;   /* [Ne] +1/-1                         */
+    const int32_t *minusSign;  /* [Ne] +1/-1                         */
+    const double *rp, *rm;     /* [Ne x 3] free vertices             */
+    const double *Ap, *Am;     /* [Ne] triangle areas                */
+    const double *len;         /* [Ne] edge lengths                  */
+} efie_mesh;
+
+/* The prepack struct of efie_precompute_pack.m:43-58 (dimensions as read by
+ * patch_sweep_fastquad_cuda.cu:559-567).  Pointers are read-only inputs for
+ * the assembly entry points and outputs of efie_precompute_pack(). */
+typedef struct efie_prepack {
+    int32_t Nt, Nq, Nq2, NsS, NsN;
+    double *r_reg;             /* [Nq x 3 x Nt]                      */
+    double *w_reg;             /* [Nq x Nt]   (weights include 2A)   */
+    uint8_t *nearMat;          /* [Nt x Nt]                          */
+    double *self_r;            /* [Nq2 x 3 x NsS x Nt]               */
+    double *self_w;            /* [Nq2 x NsS x Nt]                   */
+    double *self_a;            /* [NsS x Nt]                         */
+    double *near_r;            /* [Nq2 x 3 x NsN x Nt]               */
+    double *near_w;            /* [Nq2 x NsN x Nt]                   */
+    double *aeqTri;            /* [Nt]                               */
+    double near_alpha;
+    double self_alpha;         /* carried, unused by the kernels (as in the reference) */
+} efie_prepack;
+
+/* ---------------------------------------------------------------------- */
+/* Assembly-only entry points                                              */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces ggassemble_ZV_EFIE_RWG_DIFF_GPU_FAST.cu:542-843 (mexFunction):
+ * [Z,Vrhs] = ggassemble_...(V,F,E,plusTri,minusTri,plusSign,minusSign,rp,rm,
+ *                            Ap,Am,len,prepack,k,omega,mu,eps,excvec)
+ * excvec = [patchEdge, groundEdge, V0, spreadRadius].
+ * Z: [Ne x Ne] complex128 column-major; Vrhs: [Ne] complex128 (imag 0). */
+efie_status efie_ggassemble_zv(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre,
+                               efie_c128 k, double omega, double mu, efie_c128 eps,
+                               const double excvec[4], efie_c128 *Z, efie_c128 *Vrhs);
+
+/* Replaces gassemble_ZV_EFIE_RWG_DIFF_GPU_FAST.cu:125-435 (mexFunction), the
+ * one-point centroid assembly: exc = [patchEdge, groundEdge, V0,
+ * spreadRadius, selfAlpha]. */
+efie_status efie_gassemble_zv(efie_ctx *ctx, const efie_mesh *mesh,
+                              efie_c128 k, double omega, double mu, efie_c128 eps,
+                              const double exc[5], efie_c128 *Z, efie_c128 *Vrhs);
+
+/* ---------------------------------------------------------------------- */
+/* Frequency sweeps (assemble + solve + port reduction per frequency)      */
+/* ---------------------------------------------------------------------- */
+typedef enum efie_solver {
+    EFIE_SOLVER_FP64 = 0,   /* complex128 LU (cuSOLVER Zgetrf/Zgetrs), the plain FP64 GPU path */
+    EFIE_SOLVER_MIXED = 1   /* complex64 tensor-core LU + FP64 iterative refinement           */
+} efie_solver;
+
+typedef enum efie_port_model {
+    EFIE_PORT_GAUSS = 0,     /* Iport = sum((wPatch - wGnd) .* len .* I)  (fastquad.cu:777-785) */
+    EFIE_PORT_EDGE_DIFF = 1  /* Iport = I(patchEdge) - I(groundEdge)      (patch_sweep_cuda.cu:484-491) */
+} efie_port_model;
+
+typedef enum efie_scheme {
+    EFIE_SCHEME_REF = 0,     /* reference quadrature: cached subdivision + softening */
+    EFIE_SCHEME_EXTRACT = 1  /* regular rule everywhere + analytic 1/R extraction on
+                                self and vertex-adjacent triangle pairs            */
+} efie_scheme;
+
+typedef struct efie_sweep_opts {
+    int32_t solver;          /* efie_solver; default EFIE_SOLVER_MIXED          */
+    int32_t port_model;      /* efie_port_model; default EFIE_PORT_GAUSS        */
+    int32_t scheme;          /* efie_scheme; default EFIE_SCHEME_REF            */
+    double refine_tol;       /* relative residual target; default 1e-10         */
+    int32_t refine_max_iter; /* default 30                                      */
+    int32_t lu_nb;           /* LU panel width (0 = autotuned choice)           */
+    int32_t timing;          /* 1 = record per-phase CUDA-event timings         */
+} efie_sweep_opts;
+
+/* Fill `o` with the defaults listed above. */
+void efie_sweep_opts_default(efie_sweep_opts *o);
+
+typedef struct efie_sweep_stats {
+    int32_t n_freq;
+    int32_t refine_iters_max;   /* worst-case refinement iterations over the sweep */
+    int32_t n_fp64_fallback;    /* frequencies re-solved with the complex128 LU    */
+    double max_relres;          /* worst final relative residual ||V - Z I||/||V|| */
+    double ms_assemble;         /* summed device time per phase (timing = 1)       */
+    double ms_factor;
+    double ms_solve;            /* triangular solves + residuals + reduction       */
+    int32_t n_gemm_launches;    /* tensor-core trailing-update launches            */
+    double ms_gemm;             /* summed device time of those launches            */
+    double gemm_flop;           /* their algorithmic real flops (8 m n k each)     */
+    int32_t n_qpe_launches;     /* regular-pair quadrature launches                */
+    double ms_qpe;
+    double qpe_count;           /* point-pair evaluations in those launches        */
+} efie_sweep_stats;
+
+/* Replaces patch_sweep_fastquad_cuda.cu:461-844 (mexFunction):
+ * [Zin,S11] = patch_sweep_fastquad_cuda(V,F,E,plusTri,minusTri,plusSign,
+ *     minusSign,rp,rm,Ap,Am,len,prepack,freqs,mu,eps,patchEdge,groundEdge,
+ *     V0,spreadRadius,Z0).
+ * opts may be NULL (defaults).  I (optional, may be NULL) receives the
+ * solution currents [Ne x Nf] column-major; stats may be NULL. */
+efie_status efie_patch_sweep_fastquad(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre,
+                                      const double *freqs, int32_t Nf, double mu, efie_c128 eps,
+                                      int32_t patchEdge, int32_t groundEdge, double V0,
+                                      double spreadRadius, double Z0, const efie_sweep_opts *opts,
+                                      efie_c128 *Zin, efie_c128 *S11, efie_c128 *I,
+                                      efie_sweep_stats *stats);
+
+/* Replaces patch_sweep_cuda.cu:172-527 (mexFunction): centroid assembly with
+ * selfAlpha fixed at 0.20 (:269) and the edge-difference port model
+ * (:484-494).  opts->port_model is ignored (always EFIE_PORT_EDGE_DIFF). */
+efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh *mesh,
+                                      const double *freqs, int32_t Nf, double mu, efie_c128 eps,
+                                      int32_t patchEdge, int32_t groundEdge, double V0,
+                                      double spreadRadius, double Z0, const efie_sweep_opts *opts,
+                                      efie_c128 *Zin, efie_c128 *S11, efie_c128 *I,
+                                      efie_sweep_stats *stats);
+
+/* ---------------------------------------------------------------------- */
+/* Plans: geometry uploaded once, sweeps re-run with device-resident data  */
+/* ---------------------------------------------------------------------- */
+typedef struct efie_plan efie_plan;
+
+/* Upload the geometry of a patch_sweep_fastquad_cuda call once.  pre may be
+ * NULL when opts->scheme == EFIE_SCHEME_EXTRACT; `rule_order` then selects the
+ * regular rule (a tri_quad_rule order or EFIE_QUAD_DUNAVANT7). */
+efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre,
+                             double mu, efie_c128 eps, int32_t patchEdge, int32_t groundEdge,
+                             double V0, double spreadRadius, double Z0,
+                             const efie_sweep_opts *opts, int32_t rule_order, efie_plan **out);
+efie_status efie_plan_run(efie_plan *plan, const double *freqs, int32_t Nf,
+                          efie_c128 *Zin, efie_c128 *S11, efie_c128 *I, efie_sweep_stats *stats);
+void efie_plan_destroy(efie_plan *plan);
+
+/* ---------------------------------------------------------------------- */
+/* Boundary-data producers (MATLAB-side in the reference)                  */
+/* ---------------------------------------------------------------------- */
+
+/* make_patch_with_ground_mesh.m:1-46.  vertex_order 0 reproduces the
+ * reference exactly (vertices numbered y-fastest by meshgrid(:), faces
+ * indexed x-fastest); 1 numbers vertices x-fastest so that every face is a
+ * half rectangle.  V: [Nv x 3], F: [Nt x 3] with
+ * Nv = (Npx+1)(Npy+1) + (Ngx+1)(Ngy+1), Nt = 2(Npx Npy + Ngx Ngy). */
+efie_status efie_make_patch_with_ground_mesh(double Lp, double Wp, double Lg, double Wg, double h,
+                                             int32_t Npx, int32_t Npy, int32_t Ngx, int32_t Ngy,
+                                             int32_t vertex_order, double *V, int32_t *F);
+
+/* build_rwg_interior.m:1-103.  Call once with capacity 0 to get *Ne, then
+ * again with capacity == *Ne and output arrays sized for it (column-major,
+ * leading dimension Ne): edge [Ne x 2], rp/rm/center [Ne x 3]. */
+efie_status efie_build_rwg_interior(int32_t Nv, const double *V, int32_t Nt, const int32_t *F,
+                                    int32_t capacity, int32_t *Ne,
+                                    int32_t *edge, int32_t *plusTri, int32_t *minusTri,
+                                    int32_t *plusSign, int32_t *minusSign,
+                                    double *rp, double *rm, double *Ap, double *Am,
+                                    double *len, double *center, int32_t *zSign);
+
+/* pick_port_edge_by_point_and_layer.m:1-11 (first minimum on ties).
+ * center [Ne x 3]; returns the 1-based edge in *eidx. */
+efie_status efie_pick_port_edge(int32_t Ne, const double *center, const int32_t *zSign,
+                                const double p[3], int32_t layerSign, int32_t *eidx);
+
+/* Rule selector for the Dunavant (1985) 7-point degree-5 rule, which the
+ * reference lacks; every other order keeps tri_quad_rule.m's meaning
+ * (1 -> 1 point, 2 -> 3 points, anything else -> the 6-point rule). */
+#define EFIE_QUAD_DUNAVANT7 (-7)
+
+/* Number of points of tri_quad_rule(order) (tri_quad_rule.m:1-23). */
+int32_t efie_quad_rule_size(int32_t order);
+
+typedef struct efie_precompute_opts {
+    int32_t quad_order, near_order, self_subdiv, near_subdiv;
+    double near_sing_eps, self_alpha, near_alpha;
+} efie_precompute_opts;
+
+/* efie_precompute.m:1-97 + efie_precompute_pack.m:1-59.  `out` carries the
+ * dimensions (Nt, Nq = efie_quad_rule_size(quad_order), Nq2 =
+ * efie_quad_rule_size(near_order), NsS = 4^self_subdiv, NsN = 4^near_subdiv)
+ * and caller-allocated arrays of those sizes. */
+efie_status efie_precompute_pack(int32_t Nv, const double *V, int32_t Nt, const int32_t *F,
+                                 const efie_precompute_opts *opts, efie_prepack *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EFIE_B200_H */

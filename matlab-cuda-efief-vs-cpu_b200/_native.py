@@ -1,0 +1,159 @@
+"""ctypes binding of libefie_b200.so (the C ABI declared in include/efie_b200.h).
+
+The library is built in-tree by ``build.py``; there is no fallback: if the
+shared object is missing or no CUDA device is present, calls raise.
+"""
+from __future__ import annotations
+
+import atexit
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libefie_b200.so")
+
+c_double_p = C.POINTER(C.c_double)
+c_int32_p = C.POINTER(C.c_int32)
+c_uint8_p = C.POINTER(C.c_uint8)
+
+
+class c128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+class EfieMesh(C.Structure):
+    _fields_ = [("Nv", C.c_int32), ("Nt", C.c_int32), ("Ne", C.c_int32),
+                ("V", c_double_p), ("F", c_int32_p), ("E", c_int32_p),
+                ("plusTri", c_int32_p), ("minusTri", c_int32_p),
+                ("plusSign", c_int32_p), ("minusSign", c_int32_p),
+                ("rp", c_double_p), ("rm", c_double_p),
+                ("Ap", c_double_p), ("Am", c_double_p), ("len", c_double_p)]
+
+
+class EfiePrepack(C.Structure):
+    _fields_ = [("Nt", C.c_int32), ("Nq", C.c_int32), ("Nq2", C.c_int32),
+                ("NsS", C.c_int32), ("NsN", C.c_int32),
+                ("r_reg", c_double_p), ("w_reg", c_double_p), ("nearMat", c_uint8_p),
+                ("self_r", c_double_p), ("self_w", c_double_p), ("self_a", c_double_p),
+                ("near_r", c_double_p), ("near_w", c_double_p), ("aeqTri", c_double_p),
+                ("near_alpha", C.c_double), ("self_alpha", C.c_double)]
+
+
+class EfieSweepOpts(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("port_model", C.c_int32), ("scheme", C.c_int32),
+                ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
+                ("lu_nb", C.c_int32), ("timing", C.c_int32)]
+
+
+class EfieSweepStats(C.Structure):
+    _fields_ = [("n_freq", C.c_int32), ("refine_iters_max", C.c_int32),
+                ("n_fp64_fallback", C.c_int32), ("max_relres", C.c_double),
+                ("ms_assemble", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
+                ("n_gemm_launches", C.c_int32), ("ms_gemm", C.c_double), ("gemm_flop", C.c_double),
+                ("n_qpe_launches", C.c_int32), ("ms_qpe", C.c_double), ("qpe_count", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class EfiePrecomputeOpts(C.Structure):
+    _fields_ = [("quad_order", C.c_int32), ("near_order", C.c_int32),
+                ("self_subdiv", C.c_int32), ("near_subdiv", C.c_int32),
+                ("near_sing_eps", C.c_double), ("self_alpha", C.c_double),
+                ("near_alpha", C.c_double)]
+
+
+SOLVER_FP64, SOLVER_MIXED = 0, 1
+PORT_GAUSS, PORT_EDGE_DIFF = 0, 1
+SCHEME_REF, SCHEME_EXTRACT = 0, 1
+QUAD_DUNAVANT7 = -7
+
+# Every exported symbol of include/efie_b200.h with (restype, argtypes).
+_P = C.c_void_p
+SIGNATURES = {
+    "efie_status_id": (C.c_char_p, [C.c_int]),
+    "efie_last_error": (C.c_char_p, []),
+    "efie_ctx_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "efie_ctx_destroy": (None, [_P]),
+    "efie_ctx_set_stream": (C.c_int, [_P, _P]),
+    "efie_ggassemble_zv": (C.c_int, [_P, C.POINTER(EfieMesh), C.POINTER(EfiePrepack), c128, C.c_double,
+                                     C.c_double, c128, c_double_p, _P, _P]),
+    "efie_gassemble_zv": (C.c_int, [_P, C.POINTER(EfieMesh), c128, C.c_double, C.c_double, c128,
+                                    c_double_p, _P, _P]),
+    "efie_sweep_opts_default": (None, [C.POINTER(EfieSweepOpts)]),
+    "efie_patch_sweep_fastquad": (C.c_int, [_P, C.POINTER(EfieMesh), C.POINTER(EfiePrepack), c_double_p,
+                                            C.c_int32, C.c_double, c128, C.c_int32, C.c_int32, C.c_double,
+                                            C.c_double, C.c_double, C.POINTER(EfieSweepOpts), _P, _P, _P,
+                                            C.POINTER(EfieSweepStats)]),
+    "efie_patch_sweep_centroid": (C.c_int, [_P, C.POINTER(EfieMesh), c_double_p, C.c_int32, C.c_double,
+                                            c128, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                            C.POINTER(EfieSweepOpts), _P, _P, _P, C.POINTER(EfieSweepStats)]),
+    "efie_plan_create": (C.c_int, [_P, C.POINTER(EfieMesh), C.POINTER(EfiePrepack), C.c_double, c128,
+                                   C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                   C.POINTER(EfieSweepOpts), C.c_int32, C.POINTER(_P)]),
+    "efie_plan_run": (C.c_int, [_P, c_double_p, C.c_int32, _P, _P, _P, C.POINTER(EfieSweepStats)]),
+    "efie_plan_destroy": (None, [_P]),
+    "efie_make_patch_with_ground_mesh": (C.c_int, [C.c_double] * 5 + [C.c_int32] * 5 + [c_double_p, c_int32_p]),
+    "efie_build_rwg_interior": (C.c_int, [C.c_int32, c_double_p, C.c_int32, c_int32_p, C.c_int32, c_int32_p,
+                                          c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p,
+                                          c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
+                                          c_double_p, c_int32_p]),
+    "efie_pick_port_edge": (C.c_int, [C.c_int32, c_double_p, c_int32_p, c_double_p, C.c_int32, c_int32_p]),
+    "efie_quad_rule_size": (C.c_int32, [C.c_int32]),
+    "efie_precompute_pack": (C.c_int, [C.c_int32, c_double_p, C.c_int32, c_int32_p,
+                                       C.POINTER(EfiePrecomputeOpts), C.POINTER(EfiePrepack)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libefie_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libefie_b200.so is not built: run __graft_entry__.build() "
+                               "or python matlab-cuda-efief-vs-cpu_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MexError(RuntimeError):
+    """Error carrying the reference's mexErrMsgIdAndTxt identifier."""
+
+    def __init__(self, identifier, message):
+        super().__init__("%s: %s" % (identifier, message))
+        self.identifier = identifier
+        self.message = message
+
+
+def check(status):
+    if status != 0:
+        L = lib()
+        raise MexError(L.efie_status_id(status).decode(), L.efie_last_error().decode())
+
+
+_ctx = None
+
+
+def context(device=0):
+    """Process-wide context (created on first use, destroyed at exit like mexAtExit)."""
+    global _ctx
+    if _ctx is None:
+        h = C.c_void_p()
+        check(lib().efie_ctx_create(device, C.byref(h)))
+        _ctx = h
+        atexit.register(_destroy_ctx)
+    return _ctx
+
+
+def _destroy_ctx():
+    global _ctx
+    if _ctx is not None and _lib is not None:
+        _lib.efie_ctx_destroy(_ctx)
+    _ctx = None

@@ -1,0 +1,605 @@
+// FP64 impedance-matrix assembly on sm_100a.
+//
+// The reference evaluates every RWG pair (m,n) by looping over its four
+// triangle pairs and recomputing the quadrature (kernel_Z_fastquad,
+// patch_sweep_fastquad_cuda.cu:347-412).  A triangle pair is shared by up to
+// 3x3 RWG pairs, so here the quadrature runs once per triangle pair and
+// produces eight complex moments in local coordinates (rho = r - o_t):
+//   S0 = sum W G,  S1 = sum W G rho_i,  S2 = sum W G rho'_j,  S3 = sum W G rho_i.rho'_j
+// With the RWG basis written as f = c (r - v), div = 2c
+// (rwg_eval_on_triangle.m:10-28: plus side c = s+ l/(2A+), v = r+; minus side
+// c = -s- l/(2A-), v = r-), every RWG pair entry is
+//   Ivec = c_m c_n [S3 - d_n.S1 - d_m.S2 + (d_m.d_n) S0],  Isca = 4 c_m c_n S0
+// with d = v - o.  Pair regimes follow Z_entry (CPU_FAST.m:48-54): self when
+// t1 == t2, near when nearMat(t1,t2), else regular.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "efie_internal.h"
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct Mom {
+    double v[16];  // S0(re,im) S1x S1y S1z S2x S2y S2z S3 (re,im each)
+};
+
+__device__ __forceinline__ void green(double kr, double ki, double R, double &gr, double &gi) {
+    // exp(-j k R)/(4 pi R), k = kr + j ki  (patch_sweep_fastquad_cuda.cu:60-71)
+    double s, c;
+    sincos(kr * R, &s, &c);
+    double inv = 1.0 / (4.0 * kPi * R);
+    if (ki != 0.0) inv *= exp(ki * R);
+    gr = c * inv;
+    gi = -s * inv;
+}
+
+__device__ __forceinline__ size_t pair_slot(int t1, int t2, int Nt, bool sym) {
+    if (!sym) return (size_t)t1 + (size_t)Nt * (size_t)t2;
+    int lo = min(t1, t2), hi = max(t1, t2);
+    return (size_t)hi * (size_t)(hi + 1) / 2 + (size_t)lo;
+}
+
+__device__ __forceinline__ void store_mom(double *dst, const double *a) {
+    double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+    for (int i = 0; i < 8; i++) d2[i] = make_double2(a[2 * i], a[2 * i + 1]);
+}
+
+// ---------------------------------------------------------------------------
+// Regular pairs: one thread per triangle pair, NQ points per triangle.
+// Block = 32 (t1) x 8 (t2).  Regular quadrature of CPU_FAST.m:63-89 with
+// R = max(R, 1e-15).
+// ---------------------------------------------------------------------------
+template <int NQ>
+__global__ void __launch_bounds__(256) k_regular_moments(
+    int Nt, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
+    const uint8_t *__restrict__ skip, double kr, double ki, double *__restrict__ mom) {
+    __shared__ double4 sp[8][NQ];
+    __shared__ double4 so[8];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int t1 = blockIdx.x * 32 + tx;
+    const int t2b = blockIdx.y * 8;
+    if (sym && blockIdx.x * 32 > t2b + 7) return;  // whole tile below the diagonal
+    for (int i = threadIdx.x; i < 8 * NQ; i += blockDim.x) {
+        int tt = t2b + i / NQ;
+        sp[i / NQ][i % NQ] = tt < Nt ? pts[(size_t)tt * NQ + i % NQ] : make_double4(0, 0, 0, 0);
+    }
+    if (threadIdx.x < 8) {
+        int tt = t2b + threadIdx.x;
+        so[threadIdx.x] = tt < Nt ? origin[tt] : make_double4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    const int t2 = t2b + ty;
+    if (t1 >= Nt || t2 >= Nt) return;
+    if (sym && t1 > t2) return;
+    if (skip[(size_t)t1 + (size_t)Nt * t2]) return;
+    double4 p1[NQ];
+#pragma unroll
+    for (int p = 0; p < NQ; p++) p1[p] = pts[(size_t)t1 * NQ + p];
+    const double4 o1 = origin[t1], o2 = so[ty];
+    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
+    double m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NQ; q++) {
+        const double4 pq = sp[ty][q];
+        const double ax = dox - pq.x, ay = doy - pq.y, az = doz - pq.z;
+        double t0r = 0, t0i = 0, t1r[3] = {0, 0, 0}, t1i[3] = {0, 0, 0};
+#pragma unroll
+        for (int p = 0; p < NQ; p++) {
+            const double dx = ax + p1[p].x, dy = ay + p1[p].y, dz = az + p1[p].z;
+            double R = sqrt(dx * dx + dy * dy + dz * dz);
+            R = fmax(R, 1e-15);
+            double gr, gi;
+            green(kr, ki, R, gr, gi);
+            gr *= p1[p].w;
+            gi *= p1[p].w;
+            t0r += gr;
+            t0i += gi;
+            t1r[0] += gr * p1[p].x; t1i[0] += gi * p1[p].x;
+            t1r[1] += gr * p1[p].y; t1i[1] += gi * p1[p].y;
+            t1r[2] += gr * p1[p].z; t1i[2] += gi * p1[p].z;
+        }
+        const double w = pq.w;
+        m[0] += w * t0r; m[1] += w * t0i;
+        m[2] += w * t1r[0]; m[3] += w * t1i[0];
+        m[4] += w * t1r[1]; m[5] += w * t1i[1];
+        m[6] += w * t1r[2]; m[7] += w * t1i[2];
+        m[8] += w * t0r * pq.x; m[9] += w * t0i * pq.x;
+        m[10] += w * t0r * pq.y; m[11] += w * t0i * pq.y;
+        m[12] += w * t0r * pq.z; m[13] += w * t0i * pq.z;
+        m[14] += w * (pq.x * t1r[0] + pq.y * t1r[1] + pq.z * t1r[2]);
+        m[15] += w * (pq.x * t1i[0] + pq.y * t1i[1] + pq.z * t1i[2]);
+    }
+    store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+}
+
+// Generic point count (any Nq a prepack may carry).
+__global__ void __launch_bounds__(256) k_regular_moments_any(
+    int Nt, int Nq, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
+    const uint8_t *__restrict__ skip, double kr, double ki, double *__restrict__ mom) {
+    const int t1 = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int t2 = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (t1 >= Nt || t2 >= Nt) return;
+    if (sym && t1 > t2) return;
+    if (skip[(size_t)t1 + (size_t)Nt * t2]) return;
+    const double4 o1 = origin[t1], o2 = origin[t2];
+    double m[16];
+    for (int i = 0; i < 16; i++) m[i] = 0.0;
+    for (int q = 0; q < Nq; q++) {
+        const double4 pq = pts[(size_t)t2 * Nq + q];
+        for (int p = 0; p < Nq; p++) {
+            const double4 pp = pts[(size_t)t1 * Nq + p];
+            const double dx = (o1.x - o2.x) + pp.x - pq.x, dy = (o1.y - o2.y) + pp.y - pq.y,
+                         dz = (o1.z - o2.z) + pp.z - pq.z;
+            double R = fmax(sqrt(dx * dx + dy * dy + dz * dz), 1e-15);
+            double gr, gi;
+            green(kr, ki, R, gr, gi);
+            const double w = pp.w * pq.w;
+            gr *= w;
+            gi *= w;
+            m[0] += gr; m[1] += gi;
+            m[2] += gr * pp.x; m[3] += gi * pp.x; m[4] += gr * pp.y; m[5] += gi * pp.y;
+            m[6] += gr * pp.z; m[7] += gi * pp.z;
+            m[8] += gr * pq.x; m[9] += gi * pq.x; m[10] += gr * pq.y; m[11] += gi * pq.y;
+            m[12] += gr * pq.z; m[13] += gi * pq.z;
+            const double dd = pp.x * pq.x + pp.y * pq.y + pp.z * pq.z;
+            m[14] += gr * dd; m[15] += gi * dd;
+        }
+    }
+    store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One point pair into the 16 moment accumulators.
+__device__ __forceinline__ void acc_qpe(double *m, const double4 &pp, const double4 &pq, double gr, double gi) {
+    const double w = pp.w * pq.w;
+    gr *= w;
+    gi *= w;
+    m[0] += gr; m[1] += gi;
+    m[2] += gr * pp.x; m[3] += gi * pp.x; m[4] += gr * pp.y; m[5] += gi * pp.y;
+    m[6] += gr * pp.z; m[7] += gi * pp.z;
+    m[8] += gr * pq.x; m[9] += gi * pq.x; m[10] += gr * pq.y; m[11] += gi * pq.y;
+    m[12] += gr * pq.z; m[13] += gi * pq.z;
+    const double dd = pp.x * pq.x + pp.y * pq.y + pp.z * pq.z;
+    m[14] += gr * dd; m[15] += gi * dd;
+}
+
+// ---------------------------------------------------------------------------
+// Near pairs (CPU_FAST.m:92-136; fastquad.cu:175-257): one warp per pair, the
+// lanes share the point pairs of the subdivided rules; softening
+// R = sqrt(R^2 + a^2), a = near_alpha * min(aeq(t1), aeq(t2)), then R >= 1e-15.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_near_moments(
+    int Nt, bool sym, int n_pairs, const int2 *__restrict__ list, int P,
+    const double4 *__restrict__ origin, const double4 *__restrict__ pts, const double *__restrict__ aeq,
+    double near_alpha, double kr, double ki, double *__restrict__ mom) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_pairs) return;
+    const int2 pr = list[warp];
+    const int t1 = pr.x, t2 = pr.y;
+    const double4 o1 = origin[t1], o2 = origin[t2];
+    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
+    const double a = near_alpha * fmin(aeq[t1], aeq[t2]);
+    const double a2 = a * a;
+    double m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = 0.0;
+    const int total = P * P;
+    for (int e = lane; e < total; e += 32) {
+        const int p = e / P, q = e - p * P;
+        const double4 pp = pts[(size_t)t1 * P + p];
+        const double4 pq = pts[(size_t)t2 * P + q];
+        const double dx = dox + pp.x - pq.x, dy = doy + pp.y - pq.y, dz = doz + pp.z - pq.z;
+        double R = sqrt(dx * dx + dy * dy + dz * dz);
+        R = sqrt(R * R + a2);
+        R = fmax(R, 1e-15);
+        double gr, gi;
+        green(kr, ki, R, gr, gi);
+        acc_qpe(m, pp, pq, gr, gi);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
+    if (lane == 0) store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+}
+
+// ---------------------------------------------------------------------------
+// Self pairs (CPU_FAST.m:139-183; fastquad.cu:260-345): one warp per
+// triangle; softening R = sqrt(R^2 + aS(p)^2) only between points of the same
+// sub-triangle, R = max(R, 1e-15) otherwise.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_self_moments(
+    int Nt, bool sym, int P, int Nq2, const double4 *__restrict__ pts, const double *__restrict__ self_a,
+    int NsS, double kr, double ki, double *__restrict__ mom) {
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= Nt) return;
+    double m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = 0.0;
+    const int total = P * P;
+    for (int e = lane; e < total; e += 32) {
+        const int p = e / P, q = e - p * P;
+        const double4 pp = pts[(size_t)t * P + p];
+        const double4 pq = pts[(size_t)t * P + q];
+        const double dx = pp.x - pq.x, dy = pp.y - pq.y, dz = pp.z - pq.z;
+        double R = sqrt(dx * dx + dy * dy + dz * dz);
+        const int sp = p / Nq2, sq = q / Nq2;
+        if (sp == sq) {
+            const double aS = self_a[(size_t)t * NsS + sp];
+            R = sqrt(R * R + aS * aS);
+        } else {
+            R = fmax(R, 1e-15);
+        }
+        double gr, gi;
+        green(kr, ki, R, gr, gi);
+        acc_qpe(m, pp, pq, gr, gi);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
+    if (lane == 0) store_mom(mom + 16 * pair_slot(t, t, Nt, sym), m);
+}
+
+// ---------------------------------------------------------------------------
+// Gather: Z(m,n) = sum over the 4 triangle pairs of alpha Ivec + beta Isca,
+// in the reference's (im, in) order (kernel_Z_fastquad, fastquad.cu:373-409).
+// Thread per entry, m fastest (column-major Z, coalesced stores).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gather_z(
+    int Ne, int Nt, bool sym, const int *__restrict__ etri, const double4 *__restrict__ ecd,
+    const double *__restrict__ mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+    const int m = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (m >= Ne || n >= Ne) return;
+    double zr = 0.0, zi = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+        const int t1 = etri[a * Ne + m];
+        if (t1 < 0) continue;
+        const double4 dm = ecd[a * Ne + m];
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const int t2 = etri[b * Ne + n];
+            if (t2 < 0) continue;
+            const double4 dn = ecd[b * Ne + n];
+            const double2 *s = reinterpret_cast<const double2 *>(mom + 16 * pair_slot(t1, t2, Nt, sym));
+            const double2 S0 = s[0], S3 = s[7];
+            double2 S1x = s[1], S1y = s[2], S1z = s[3], S2x = s[4], S2y = s[5], S2z = s[6];
+            if (sym && t1 > t2) {  // stored for (t2, t1): swap the one-sided moments
+                double2 tx = S1x, ty = S1y, tz = S1z;
+                S1x = S2x; S1y = S2y; S1z = S2z;
+                S2x = tx; S2y = ty; S2z = tz;
+            }
+            const double dd = dm.x * dn.x + dm.y * dn.y + dm.z * dn.z;
+            const double ivr = S3.x - (dn.x * S1x.x + dn.y * S1y.x + dn.z * S1z.x)
+                               - (dm.x * S2x.x + dm.y * S2y.x + dm.z * S2z.x) + dd * S0.x;
+            const double ivi = S3.y - (dn.x * S1x.y + dn.y * S1y.y + dn.z * S1z.y)
+                               - (dm.x * S2x.y + dm.y * S2y.y + dm.z * S2z.y) + dd * S0.y;
+            const double cc = dm.w * dn.w;
+            const double Ivr = cc * ivr, Ivi = cc * ivi;
+            const double Isr = 4.0 * cc * S0.x, Isi = 4.0 * cc * S0.y;
+            zr += (alr * Ivr - ali * Ivi) + (ber * Isr - bei * Isi);
+            zi += (alr * Ivi + ali * Ivr) + (ber * Isi + bei * Isr);
+        }
+    }
+    Z[(size_t)m + (size_t)Ne * n] = make_double2(zr, zi);
+}
+
+// ---------------------------------------------------------------------------
+// Centroid (one point, weight = area) assembly: kernel_Z_centroid of
+// gassemble_ZV_EFIE_RWG_DIFF_GPU_FAST.cu:49-106 with the host side data of
+// :221-299.  side[2*Ne] = {pos.xyz, f.xyz, div, w, t(1-based, as double)}.
+// ---------------------------------------------------------------------------
+struct Side {
+    double px, py, pz, fx, fy, fz, div, w, t, pad;
+};
+
+__global__ void __launch_bounds__(256) k_centroid_z(int Ne, const Side *__restrict__ side,
+                                                    const double *__restrict__ asoft, double kr, double ki,
+                                                    double alr, double ali, double ber, double bei,
+                                                    double2 *__restrict__ Z) {
+    const int m = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (m >= Ne || n >= Ne) return;
+    double zr = 0.0, zi = 0.0;
+    for (int sa = 0; sa < 2; sa++) {
+        const Side A = side[2 * m + sa];
+        if (A.w == 0.0 || A.t == 0.0) continue;
+        for (int sb = 0; sb < 2; sb++) {
+            const Side B = side[2 * n + sb];
+            if (B.w == 0.0 || B.t == 0.0) continue;
+            const double dx = A.px - B.px, dy = A.py - B.py, dz = A.pz - B.pz;
+            double R = sqrt(dx * dx + dy * dy + dz * dz);
+            if (A.t == B.t) {
+                const double a = asoft[(int)A.t - 1];
+                R = sqrt(R * R + a * a);
+            }
+            R = fmax(R, 1e-15);
+            double gr, gi;
+            green(kr, ki, R, gr, gi);
+            const double ff = A.fx * B.fx + A.fy * B.fy + A.fz * B.fz;
+            const double dv = A.div * B.div;
+            const double w = A.w * B.w;
+            const double vr = gr * (ff * w), vi = gi * (ff * w);
+            const double sr = gr * (dv * w), si = gi * (dv * w);
+            zr += (alr * vr - ali * vi) + (ber * sr - bei * si);
+            zi += (alr * vi + ali * vr) + (ber * si + bei * sr);
+        }
+    }
+    Z[(size_t)m + (size_t)Ne * n] = make_double2(zr, zi);
+}
+
+}  // namespace
+
+Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps) {
+    Physics p;
+    p.kr = k.re;
+    p.ki = k.im;
+    // alpha = j w mu ; beta = 1/(j w eps)  (ggassemble.cu:678-686)
+    p.alr = 0.0;
+    p.ali = omega * mu;
+    const double dr = -omega * eps.im, di = omega * eps.re, d2 = dr * dr + di * di;
+    p.ber = dr / d2;
+    p.bei = -di / d2;
+    return p;
+}
+
+Physics efie_physics(double freq, double mu, efie_c128 eps) {
+    // patch_sweep_fastquad_cuda.cu:714-743: principal sqrt by the polar form
+    const double omega = 2.0 * kPi * freq;
+    const double ar = mu * eps.re, ai = mu * eps.im;
+    const double r = std::sqrt(ar * ar + ai * ai), ang = std::atan2(ai, ar);
+    const double sr = std::sqrt(r), half = 0.5 * ang;
+    efie_c128 k = {omega * (sr * std::cos(half)), omega * (sr * std::sin(half))};
+    return efie_physics_k(k, omega, mu, eps);
+}
+
+// Host-side repacking of the boundary arrays into the device layout.
+efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
+                             int rule_order, GeomDev &g) {
+    const int Ne = mesh->Ne, Nt = mesh->Nt, Nv = mesh->Nv;
+    g.Ne = Ne;
+    g.Nt = Nt;
+    g.scheme = scheme;
+    g.near_alpha = pre ? pre->near_alpha : 0.0;
+    // origins: triangle centroids from V/F
+    std::vector<double4> origin(Nt);
+    for (int t = 0; t < Nt; t++) {
+        double c[3] = {0, 0, 0};
+        for (int j = 0; j < 3; j++) {
+            const int v = mesh->F[t + (size_t)j * Nt] - 1;
+            for (int k = 0; k < 3; k++) c[k] += mesh->V[v + (size_t)k * Nv];
+        }
+        origin[t] = make_double4(c[0] / 3.0, c[1] / 3.0, c[2] / 3.0, 0.0);
+    }
+    auto up = [&](DevBuf &b, const void *src, size_t bytes) -> efie_status {
+        EFIE_TRY(b.reserve(bytes));
+        EFIE_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return EFIE_OK;
+    };
+    // edges: per side triangle (0-based, -1 = none), delta = v - o, c
+    std::vector<int> etri(2 * (size_t)Ne);
+    std::vector<double4> ecd(2 * (size_t)Ne);
+    for (int e = 0; e < Ne; e++) {
+        const int tp = mesh->plusTri[e], tm = mesh->minusTri[e];
+        const double l = mesh->len[e];
+        for (int sd = 0; sd < 2; sd++) {
+            int t = sd == 0 ? tp : tm;
+            // rwg_eval_point picks the plus formula whenever t == plusTri
+            // (fastquad.cu:82-95), also for a degenerate edge with tp == tm.
+            const bool plus = (sd == 0) || (tm == tp);
+            double c;
+            const double *v = plus ? mesh->rp : mesh->rm;
+            if (plus) c = (double)mesh->plusSign[e] * (l / (2.0 * mesh->Ap[e]));
+            else c = -((double)mesh->minusSign[e] * (l / (2.0 * mesh->Am[e])));
+            if (t <= 0) {
+                etri[sd * (size_t)Ne + e] = -1;
+                ecd[sd * (size_t)Ne + e] = make_double4(0, 0, 0, 0);
+                continue;
+            }
+            const double4 o = origin[t - 1];
+            etri[sd * (size_t)Ne + e] = t - 1;
+            ecd[sd * (size_t)Ne + e] = make_double4(v[e] - o.x, v[e + Ne] - o.y, v[e + 2 * (size_t)Ne] - o.z, c);
+        }
+    }
+    EFIE_TRY(up(g.origin, origin.data(), sizeof(double4) * Nt));
+    EFIE_TRY(up(g.edge_tri, etri.data(), sizeof(int) * etri.size()));
+    EFIE_TRY(up(g.edge_cd, ecd.data(), sizeof(double4) * ecd.size()));
+
+    std::vector<uint8_t> mask((size_t)Nt * Nt, 0);
+    if (scheme == EFIE_SCHEME_REF) {
+        const int Nq = pre->Nq, Nq2 = pre->Nq2, NsS = pre->NsS, NsN = pre->NsN;
+        g.Nq = Nq;
+        g.Nq2 = Nq2;
+        g.NsS = NsS;
+        g.NsN = NsN;
+        std::vector<double4> reg((size_t)Nt * Nq), nearp((size_t)Nt * NsN * Nq2), selfp((size_t)Nt * NsS * Nq2);
+        for (int t = 0; t < Nt; t++) {
+            const double4 o = origin[t];
+            for (int i = 0; i < Nq; i++) {
+                const double *r = pre->r_reg + i + (size_t)Nq * 3 * t;
+                reg[(size_t)t * Nq + i] = make_double4(r[0] - o.x, r[Nq] - o.y, r[2 * Nq] - o.z,
+                                                       pre->w_reg[i + (size_t)Nq * t]);
+            }
+            for (int p = 0; p < NsN; p++)
+                for (int i = 0; i < Nq2; i++) {
+                    const double *r = pre->near_r + i + (size_t)Nq2 * 3 * p + (size_t)Nq2 * 3 * NsN * t;
+                    nearp[((size_t)t * NsN + p) * Nq2 + i] =
+                        make_double4(r[0] - o.x, r[Nq2] - o.y, r[2 * Nq2] - o.z,
+                                     pre->near_w[i + (size_t)Nq2 * p + (size_t)Nq2 * NsN * t]);
+                }
+            for (int p = 0; p < NsS; p++)
+                for (int i = 0; i < Nq2; i++) {
+                    const double *r = pre->self_r + i + (size_t)Nq2 * 3 * p + (size_t)Nq2 * 3 * NsS * t;
+                    selfp[((size_t)t * NsS + p) * Nq2 + i] =
+                        make_double4(r[0] - o.x, r[Nq2] - o.y, r[2 * Nq2] - o.z,
+                                     pre->self_w[i + (size_t)Nq2 * p + (size_t)Nq2 * NsS * t]);
+                }
+        }
+        EFIE_TRY(up(g.reg_pts, reg.data(), sizeof(double4) * reg.size()));
+        EFIE_TRY(up(g.near_pts, nearp.data(), sizeof(double4) * nearp.size()));
+        EFIE_TRY(up(g.self_pts, selfp.data(), sizeof(double4) * selfp.size()));
+        EFIE_TRY(up(g.self_a, pre->self_a, sizeof(double) * (size_t)Nt * NsS));
+        EFIE_TRY(up(g.aeq, pre->aeqTri, sizeof(double) * Nt));
+        // pair regimes; symmetric storage only if nearMat is symmetric
+        bool sym = true;
+        for (int t2 = 0; t2 < Nt && sym; t2++)
+            for (int t1 = 0; t1 < t2; t1++)
+                if ((pre->nearMat[(size_t)t1 + (size_t)Nt * t2] != 0) != (pre->nearMat[(size_t)t2 + (size_t)Nt * t1] != 0)) {
+                    sym = false;
+                    break;
+                }
+        g.symmetric = sym;
+        std::vector<int2> list;
+        for (int t2 = 0; t2 < Nt; t2++)
+            for (int t1 = 0; t1 < Nt; t1++) {
+                const bool self = t1 == t2;
+                const bool nr = !self && pre->nearMat[(size_t)t1 + (size_t)Nt * t2] != 0;
+                mask[(size_t)t1 + (size_t)Nt * t2] = (self || nr) ? 1 : 0;
+                if (nr && (!sym || t1 < t2)) list.push_back(make_int2(t1, t2));
+            }
+        g.n_near = (int)list.size();
+        EFIE_TRY(up(g.near_list, list.data(), sizeof(int2) * (list.empty() ? 1 : list.size())));
+    } else {
+        return efie_fail(EFIE_ERR_ARGS, "scheme not available in this build");
+    }
+    (void)rule_order;
+    EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
+    g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
+    EFIE_TRY(g.moments.reserve(sizeof(double) * 16 * g.npairs));
+    return EFIE_OK;
+}
+
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z, efie_sweep_stats *st,
+                                 bool timing) {
+    cudaStream_t s = ctx->stream;
+    const int Nt = g.Nt, Ne = g.Ne;
+    double *mom = g.moments.as<double>();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        EFIE_CUDA(cudaEventCreate(&e0));
+        EFIE_CUDA(cudaEventCreate(&e1));
+        EFIE_CUDA(cudaEventRecord(e0, s));
+    }
+    dim3 grid((Nt + 31) / 32, (Nt + 7) / 8);
+    const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
+    const uint8_t *skip = g.near_mask.as<uint8_t>();
+    switch (g.Nq) {
+    case 1: k_regular_moments<1><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
+    case 3: k_regular_moments<3><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
+    case 6: k_regular_moments<6><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
+    case 7: k_regular_moments<7><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
+    default:
+        k_regular_moments_any<<<grid, 256, 0, s>>>(Nt, g.Nq, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom);
+    }
+    EFIE_CUDA(cudaGetLastError());
+    if (timing) EFIE_CUDA(cudaEventRecord(e1, s));
+    if (g.n_near > 0) {
+        const int P = g.NsN * g.Nq2;
+        k_near_moments<<<(g.n_near + 7) / 8, 256, 0, s>>>(Nt, g.symmetric, g.n_near, g.near_list.as<int2>(), P, org,
+                                                        g.near_pts.as<double4>(), g.aeq.as<double>(), g.near_alpha,
+                                                        ph.kr, ph.ki, mom);
+        EFIE_CUDA(cudaGetLastError());
+    }
+    {
+        const int P = g.NsS * g.Nq2;
+        k_self_moments<<<(Nt + 7) / 8, 256, 0, s>>>(Nt, g.symmetric, P, g.Nq2, g.self_pts.as<double4>(),
+                                                   g.self_a.as<double>(), g.NsS, ph.kr, ph.ki, mom);
+        EFIE_CUDA(cudaGetLastError());
+    }
+    dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
+    k_gather_z<<<gg, 256, 0, s>>>(Ne, Nt, g.symmetric, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr,
+                                  ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
+    EFIE_CUDA(cudaGetLastError());
+    if (timing) {
+        float ms = 0.f;
+        EFIE_CUDA(cudaEventSynchronize(e1));
+        EFIE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (st) {
+            st->n_qpe_launches += 1;
+            st->ms_qpe += ms;
+            // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
+            const double all = g.symmetric ? 0.5 * (double)Nt * (Nt + 1) : (double)Nt * Nt;
+            const double regular = all - (double)g.n_near - (double)Nt;
+            st->qpe_count += regular * (double)g.Nq * g.Nq;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return EFIE_OK;
+}
+
+efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, double selfAlpha, const Physics &ph,
+                                          void *Z, DevBuf &scratch) {
+    const int Ne = mesh->Ne, Nt = mesh->Nt, Nv = mesh->Nv;
+    // gassemble.cu:221-299: centroids, areas, softening, side data (host, FP64)
+    std::vector<double> cent(3 * (size_t)Nt), asoft(Nt);
+    for (int t = 0; t < Nt; t++) {
+        int id[3];
+        for (int j = 0; j < 3; j++) {
+            id[j] = mesh->F[t + (size_t)j * Nt] - 1;
+            if (id[j] < 0 || id[j] >= Nv) return efie_fail(EFIE_ERR_F, "F has invalid indices.");
+        }
+        double r[3][3];
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) r[j][k] = mesh->V[id[j] + (size_t)k * Nv];
+        for (int k = 0; k < 3; k++) cent[3 * t + k] = (r[0][k] + r[1][k] + r[2][k]) / 3.0;
+        const double e1[3] = {r[1][0] - r[0][0], r[1][1] - r[0][1], r[1][2] - r[0][2]};
+        const double e2[3] = {r[2][0] - r[0][0], r[2][1] - r[0][1], r[2][2] - r[0][2]};
+        const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                     cz = e1[0] * e2[1] - e1[1] * e2[0];
+        const double A = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+        asoft[t] = selfAlpha * std::sqrt(A / kPi);
+    }
+    std::vector<Side> side(2 * (size_t)Ne);
+    for (int e = 0; e < Ne; e++) {
+        for (int sd = 0; sd < 2; sd++) {
+            Side &o = side[2 * (size_t)e + sd];
+            std::memset(&o, 0, sizeof(Side));
+            const int t = sd == 0 ? mesh->plusTri[e] : mesh->minusTri[e];
+            const double A = sd == 0 ? mesh->Ap[e] : mesh->Am[e];
+            o.t = t;
+            o.w = t > 0 ? A : 0.0;
+            if (t > 0) {
+                o.px = cent[3 * (t - 1)];
+                o.py = cent[3 * (t - 1) + 1];
+                o.pz = cent[3 * (t - 1) + 2];
+            }
+            if (t > 0 && A > 0) {
+                const double l = mesh->len[e];
+                const int sg = sd == 0 ? mesh->plusSign[e] : mesh->minusSign[e];
+                const double sc = (double)sg * (l / (2.0 * A));
+                const double *v = sd == 0 ? mesh->rp : mesh->rm;
+                const double vx = v[e], vy = v[e + Ne], vz = v[e + 2 * (size_t)Ne];
+                if (sd == 0) {
+                    o.fx = sc * (o.px - vx); o.fy = sc * (o.py - vy); o.fz = sc * (o.pz - vz);
+                    o.div = (double)sg * (l / A);
+                } else {
+                    o.fx = sc * (vx - o.px); o.fy = sc * (vy - o.py); o.fz = sc * (vz - o.pz);
+                    o.div = (double)sg * (-(l / A));
+                }
+            }
+        }
+    }
+    const size_t side_bytes = sizeof(Side) * side.size();
+    EFIE_TRY(scratch.reserve(side_bytes + sizeof(double) * Nt + 256));
+    char *base = scratch.as<char>();
+    EFIE_CUDA(cudaMemcpyAsync(base, side.data(), side_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    double *d_asoft = reinterpret_cast<double *>(base + ((side_bytes + 255) / 256) * 256);
+    EFIE_CUDA(cudaMemcpyAsync(d_asoft, asoft.data(), sizeof(double) * Nt, cudaMemcpyHostToDevice, ctx->stream));
+    dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
+    k_centroid_z<<<gg, 256, 0, ctx->stream>>>(Ne, reinterpret_cast<const Side *>(base), d_asoft, ph.kr, ph.ki, ph.alr,
+                                              ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
+    EFIE_CUDA(cudaGetLastError());
+    return EFIE_OK;
+}

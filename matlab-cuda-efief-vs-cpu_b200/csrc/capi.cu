@@ -1,0 +1,581 @@
+// C ABI of libefie_b200: argument checks that mirror the reference MEX
+// functions, host-side RHS, plans and frequency sweeps.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "efie_internal.h"
+#include "solve.h"
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+efie_status efie_fail(efie_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+extern "C" const char *efie_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" const char *efie_status_id(efie_status s) {
+    switch (s) {
+    case EFIE_OK: return "";
+    case EFIE_ERR_ARGS: return "mex:args";
+    case EFIE_ERR_V: return "mex:V";
+    case EFIE_ERR_F: return "mex:F";
+    case EFIE_ERR_E: return "mex:E";
+    case EFIE_ERR_RWG: return "mex:rwg";
+    case EFIE_ERR_PORT: return "mex:port";
+    case EFIE_ERR_PREPACK: return "mex:prepack";
+    case EFIE_ERR_R_REG: return "mex:r_reg";
+    case EFIE_ERR_W_REG: return "mex:w_reg";
+    case EFIE_ERR_NEARMAT: return "mex:nearMat";
+    case EFIE_ERR_SELF_R: return "mex:self_r";
+    case EFIE_ERR_SELF_W: return "mex:self_w";
+    case EFIE_ERR_SELF_A: return "mex:self_a";
+    case EFIE_ERR_NEAR_R: return "mex:near_r";
+    case EFIE_ERR_NEAR_W: return "mex:near_w";
+    case EFIE_ERR_AEQTRI: return "mex:aeqTri";
+    case EFIE_ERR_RHS: return "mex:rhs";
+    case EFIE_ERR_EPS: return "mex:eps";
+    case EFIE_ERR_EXC: return "mex:exc";
+    case EFIE_ERR_FREQS: return "mex:freqs";
+    case EFIE_ERR_CUDA: return "cuda:rt";
+    case EFIE_ERR_CUSOLVER: return "cuda:cusolver";
+    case EFIE_ERR_SINGULAR: return "efie:singular";
+    case EFIE_ERR_NOMEM: return "efie:nomem";
+    case EFIE_ERR_TIMEOUT: return "efie:timeout";
+    case EFIE_ERR_MESH: return "efie:mesh";
+    }
+    return "efie:unknown";
+}
+
+extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
+    if (!o) return;
+    o->solver = EFIE_SOLVER_MIXED;
+    o->port_model = EFIE_PORT_GAUSS;
+    o->scheme = EFIE_SCHEME_REF;
+    o->refine_tol = 1e-10;
+    o->refine_max_iter = 30;
+    o->lu_nb = 0;
+    o->timing = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+extern "C" efie_status efie_ctx_create(int device, efie_ctx **out) {
+    if (!out) return efie_fail(EFIE_ERR_ARGS, "efie_ctx_create: null output");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= device || device < 0)
+        return efie_fail(EFIE_ERR_CUDA, std::string("no CUDA device ") + std::to_string(device) + ": " +
+                                            (e == cudaSuccess ? "out of range" : cudaGetErrorString(e)));
+    EFIE_CUDA(cudaSetDevice(device));
+    efie_ctx *c = new (std::nothrow) efie_ctx();
+    if (!c) return efie_fail(EFIE_ERR_NOMEM, "efie_ctx_create: out of host memory");
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete c;
+        return efie_fail(EFIE_ERR_CUDA, "cudaGetDeviceProperties failed");
+    }
+    c->num_sms = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return efie_fail(EFIE_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    c->stream = c->own_stream;
+    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return efie_fail(EFIE_ERR_CUSOLVER, "cusolverDnCreate failed");
+    }
+    cusolverDnSetStream(c->solver, c->stream);
+    *out = c;
+    return EFIE_OK;
+}
+
+extern "C" void efie_ctx_destroy(efie_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->solver) cusolverDnDestroy(ctx->solver);
+    ctx->status.release();
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+extern "C" efie_status efie_ctx_set_stream(efie_ctx *ctx, void *stream) {
+    if (!ctx) return efie_fail(EFIE_ERR_ARGS, "null context");
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    if (cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
+        return efie_fail(EFIE_ERR_CUSOLVER, "cusolverDnSetStream failed");
+    return EFIE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Argument checks (the reference's mexErrMsgIdAndTxt identifiers)
+// ---------------------------------------------------------------------------
+namespace {
+
+efie_status check_mesh(const efie_mesh *m, bool need_E) {
+    if (!m) return efie_fail(EFIE_ERR_ARGS, "null mesh");
+    if (!m->V || m->Nv < 1) return efie_fail(EFIE_ERR_V, "V must be [Nv x 3] double.");
+    if (!m->F || m->Nt < 1) return efie_fail(EFIE_ERR_F, "F must be [Nt x 3] int32.");
+    if (m->Ne < 0 || (need_E && !m->E)) return efie_fail(EFIE_ERR_E, "E must be [Ne x 2] int32.");
+    if (m->Ne > 0 && (!m->plusTri || !m->minusTri || !m->plusSign || !m->minusSign || !m->rp || !m->rm ||
+                      !m->Ap || !m->Am || !m->len))
+        return efie_fail(EFIE_ERR_RWG, "missing RWG arrays.");
+    for (int64_t i = 0; i < 3 * (int64_t)m->Nt; i++)
+        if (m->F[i] < 1 || m->F[i] > m->Nv) return efie_fail(EFIE_ERR_F, "F has invalid indices.");
+    if (need_E)
+        for (int64_t i = 0; i < 2 * (int64_t)m->Ne; i++)
+            if (m->E[i] < 1 || m->E[i] > m->Nv) return efie_fail(EFIE_ERR_E, "E has invalid indices.");
+    for (int e = 0; e < m->Ne; e++) {
+        if (m->plusTri[e] < 0 || m->plusTri[e] > m->Nt || m->minusTri[e] < 0 || m->minusTri[e] > m->Nt)
+            return efie_fail(EFIE_ERR_RWG, "plusTri/minusTri out of range.");
+        if ((m->plusTri[e] > 0 && !(m->Ap[e] != 0.0)) || (m->minusTri[e] > 0 && !(m->Am[e] != 0.0)))
+            return efie_fail(EFIE_ERR_RWG, "Ap/Am must be nonzero on supported triangles.");
+    }
+    return EFIE_OK;
+}
+
+efie_status check_prepack(const efie_mesh *m, const efie_prepack *p) {
+    if (!p) return efie_fail(EFIE_ERR_PREPACK, "prepack must be a struct from efie_precompute_pack.");
+    if (!p->r_reg || p->Nq < 1) return efie_fail(EFIE_ERR_R_REG, "r_reg must be [Nq x 3 x Nt] double.");
+    if (!p->w_reg) return efie_fail(EFIE_ERR_W_REG, "w_reg must be [Nq x Nt] double.");
+    if (!p->nearMat) return efie_fail(EFIE_ERR_NEARMAT, "nearMat must be uint8 [Nt x Nt].");
+    if (!p->self_r || p->Nq2 < 1 || p->NsS < 1) return efie_fail(EFIE_ERR_SELF_R, "self_r must be [Nq2 x 3 x NsS x Nt].");
+    if (!p->self_w) return efie_fail(EFIE_ERR_SELF_W, "self_w must be [Nq2 x NsS x Nt].");
+    if (!p->self_a) return efie_fail(EFIE_ERR_SELF_A, "self_a must be [NsS x Nt].");
+    if (!p->near_r || p->NsN < 1) return efie_fail(EFIE_ERR_NEAR_R, "near_r must be [Nq2 x 3 x NsN x Nt].");
+    if (!p->near_w) return efie_fail(EFIE_ERR_NEAR_W, "near_w must be [Nq2 x NsN x Nt].");
+    if (!p->aeqTri || p->Nt != m->Nt) return efie_fail(EFIE_ERR_AEQTRI, "aeqTri must be [Nt x 1].");
+    return EFIE_OK;
+}
+
+// build_Vrhs_gaussian (ggassemble_ZV_EFIE_RWG_DIFF_GPU_FAST.cu:492-540) /
+// build_weights_gaussian (patch_sweep_fastquad_cuda.cu:415-459), FP64 on the host.
+efie_status gauss_weights(const efie_mesh *m, int edge1, double spread, std::vector<double> &w) {
+    const int Ne = m->Ne, Nv = m->Nv;
+    std::vector<double> cx(Ne), cy(Ne), cz(Ne);
+    double zmin = 1e100, zmax = -1e100;
+    for (int e = 0; e < Ne; e++) {
+        const int a = m->E[e] - 1, b = m->E[e + Ne] - 1;
+        cx[e] = 0.5 * (m->V[a] + m->V[b]);
+        cy[e] = 0.5 * (m->V[a + Nv] + m->V[b + Nv]);
+        cz[e] = 0.5 * (m->V[a + 2 * (size_t)Nv] + m->V[b + 2 * (size_t)Nv]);
+        zmin = std::min(zmin, cz[e]);
+        zmax = std::max(zmax, cz[e]);
+    }
+    const double zmid = 0.5 * (zmin + zmax);
+    const int e0 = edge1 - 1;
+    const int layer0 = cz[e0] > zmid ? 1 : -1;
+    w.assign(Ne, 0.0);
+    double sumw = 0.0;
+    for (int e = 0; e < Ne; e++) {
+        const int layer = cz[e] > zmid ? 1 : -1;
+        if (layer != layer0) continue;
+        const double dx = cx[e] - cx[e0], dy = cy[e] - cy[e0], dz = cz[e] - cz[e0];
+        const double dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+        const double v = std::exp(-(dist / spread) * (dist / spread));
+        w[e] = v;
+        sumw += v;
+    }
+    if (!(sumw >= 1e-30)) return efie_fail(EFIE_ERR_RHS, "spreadRadius too small (no weights).");
+    for (int e = 0; e < Ne; e++) w[e] /= sumw;
+    return EFIE_OK;
+}
+
+efie_status build_rhs(const efie_mesh *m, int pe, int ge, double V0, double spread, std::vector<double> &rhs,
+                      std::vector<double> *wport) {
+    std::vector<double> wP, wG;
+    EFIE_TRY(gauss_weights(m, pe, spread, wP));
+    EFIE_TRY(gauss_weights(m, ge, spread, wG));
+    rhs.resize(m->Ne);
+    for (int e = 0; e < m->Ne; e++) rhs[e] = (+V0 / 2.0) * wP[e] + (-V0 / 2.0) * wG[e];
+    if (wport) {
+        wport->resize(m->Ne);
+        for (int e = 0; e < m->Ne; e++) (*wport)[e] = (wP[e] - wG[e]) * m->len[e];  // fastquad.cu:780
+    }
+    return EFIE_OK;
+}
+
+efie_status check_port(const efie_mesh *m, int pe, int ge) {
+    if (!(pe >= 1 && pe <= m->Ne)) return efie_fail(EFIE_ERR_PORT, "patchEdge out of range.");
+    if (!(ge >= 1 && ge <= m->Ne)) return efie_fail(EFIE_ERR_PORT, "groundEdge out of range.");
+    return EFIE_OK;
+}
+
+efie_status check_eps(double omega, efie_c128 eps) {
+    const double dr = -omega * eps.im, di = omega * eps.re;
+    if (!(dr * dr + di * di > 0.0)) return efie_fail(EFIE_ERR_EPS, "eps causes denom=0.");
+    return EFIE_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Assembly-only entry points
+// ---------------------------------------------------------------------------
+extern "C" efie_status efie_ggassemble_zv(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre,
+                                          efie_c128 k, double omega, double mu, efie_c128 eps,
+                                          const double excvec[4], efie_c128 *Z, efie_c128 *Vrhs) {
+    if (!ctx) return efie_fail(EFIE_ERR_ARGS, "null context");
+    EFIE_TRY(check_mesh(mesh, true));
+    EFIE_TRY(check_prepack(mesh, pre));
+    if (!excvec) return efie_fail(EFIE_ERR_EXC, "excvec must be [patchEdge, groundEdge, V0, spreadRadius].");
+    const int pe = (int)excvec[0], ge = (int)excvec[1];
+    EFIE_TRY(check_port(mesh, pe, ge));
+    if (!Z || !Vrhs) return efie_fail(EFIE_ERR_ARGS, "null output");
+    DeviceGuard dg(ctx->device);
+    std::vector<double> rhs;
+    EFIE_TRY(build_rhs(mesh, pe, ge, excvec[2], excvec[3], rhs, nullptr));
+    EFIE_TRY(check_eps(omega, eps));
+    const Physics ph = efie_physics_k(k, omega, mu, eps);
+    const int Ne = mesh->Ne;
+    GeomDev g;
+    EFIE_TRY(efie_geom_upload(ctx, mesh, pre, EFIE_SCHEME_REF, 0, g));
+    DevBuf dZ;
+    EFIE_TRY(dZ.reserve(sizeof(efie_c128) * (size_t)Ne * Ne));
+    EFIE_TRY(efie_assemble_device(ctx, g, ph, dZ.p, nullptr, false));
+    EFIE_CUDA(cudaMemcpyAsync(Z, dZ.p, sizeof(efie_c128) * (size_t)Ne * Ne, cudaMemcpyDeviceToHost, ctx->stream));
+    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int e = 0; e < Ne; e++) Vrhs[e] = efie_c128{rhs[e], 0.0};
+    return EFIE_OK;
+}
+
+extern "C" efie_status efie_gassemble_zv(efie_ctx *ctx, const efie_mesh *mesh, efie_c128 k, double omega, double mu,
+                                         efie_c128 eps, const double exc[5], efie_c128 *Z, efie_c128 *Vrhs) {
+    if (!ctx) return efie_fail(EFIE_ERR_ARGS, "null context");
+    EFIE_TRY(check_mesh(mesh, true));
+    if (!exc)
+        return efie_fail(EFIE_ERR_EXC,
+                         "exc must be double vector len>=5: [patchEdge, groundEdge, V0, spreadRadius, selfAlpha].");
+    const int pe = (int)exc[0], ge = (int)exc[1];
+    EFIE_TRY(check_port(mesh, pe, ge));
+    if (!Z || !Vrhs) return efie_fail(EFIE_ERR_ARGS, "null output");
+    DeviceGuard dg(ctx->device);
+    std::vector<double> rhs;
+    EFIE_TRY(build_rhs(mesh, pe, ge, exc[2], exc[3], rhs, nullptr));
+    const Physics ph = efie_physics_k(k, omega, mu, eps);
+    const int Ne = mesh->Ne;
+    DevBuf dZ, scratch;
+    EFIE_TRY(dZ.reserve(sizeof(efie_c128) * (size_t)Ne * Ne));
+    EFIE_TRY(efie_assemble_centroid_device(ctx, mesh, exc[4], ph, dZ.p, scratch));
+    EFIE_CUDA(cudaMemcpyAsync(Z, dZ.p, sizeof(efie_c128) * (size_t)Ne * Ne, cudaMemcpyDeviceToHost, ctx->stream));
+    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int e = 0; e < Ne; e++) Vrhs[e] = efie_c128{rhs[e], 0.0};
+    return EFIE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plans and sweeps
+// ---------------------------------------------------------------------------
+struct efie_plan {
+    efie_ctx *ctx = nullptr;
+    efie_sweep_opts opts;
+    bool centroid = false;       // patch_sweep_cuda model
+    double self_alpha = 0.20;
+    int Ne = 0;
+    double mu = 0, V0 = 0, Z0 = 0;
+    efie_c128 eps{0, 0};
+    int pe = 0, ge = 0;
+    double bnorm = 0;
+    GeomDev g;
+    // centroid path keeps the host mesh arrays it needs
+    std::vector<double> hV, hrp, hrm, hAp, hAm, hlen;
+    std::vector<int32_t> hF, hpt, hmt, hps, hms;
+    efie_mesh cmesh{};
+    DevBuf Z, b, x, wport, out, scratch, ipiv, info, lwork;
+    int lwork_elems = -1;
+    SolveWork sw;
+};
+
+namespace {
+
+efie_status plan_solve_fp64(efie_plan *p, int fi, int *info_host) {
+    efie_ctx *ctx = p->ctx;
+    const int N = p->Ne;
+    cuDoubleComplex *A = p->Z.as<cuDoubleComplex>();
+    if (p->lwork_elems < 0) {
+        int lw = 0;
+        if (cusolverDnZgetrf_bufferSize(ctx->solver, N, N, A, N, &lw) != CUSOLVER_STATUS_SUCCESS)
+            return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
+        EFIE_TRY(p->lwork.reserve(sizeof(cuDoubleComplex) * (size_t)std::max(lw, 1)));
+        p->lwork_elems = lw;
+    }
+    EFIE_CUDA(cudaMemcpyAsync(p->x.p, p->b.p, sizeof(cuDoubleComplex) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    int *dinfo = p->info.as<int>() + fi;
+    if (cusolverDnZgetrf(ctx->solver, N, N, A, N, p->lwork.as<cuDoubleComplex>(), p->ipiv.as<int>(), dinfo) !=
+        CUSOLVER_STATUS_SUCCESS)
+        return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
+    if (cusolverDnZgetrs(ctx->solver, CUBLAS_OP_N, N, 1, A, N, p->ipiv.as<int>(), p->x.as<cuDoubleComplex>(), N,
+                         dinfo) != CUSOLVER_STATUS_SUCCESS)
+        return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
+    (void)info_host;
+    return EFIE_OK;
+}
+
+efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c128 eps, int pe, int ge, double V0,
+                        double spread, double Z0, const efie_sweep_opts *opts) {
+    efie_ctx *ctx = p->ctx;
+    if (opts) p->opts = *opts;
+    else efie_sweep_opts_default(&p->opts);
+    if (p->opts.solver != EFIE_SOLVER_FP64 && p->opts.solver != EFIE_SOLVER_MIXED)
+        return efie_fail(EFIE_ERR_ARGS, "unknown solver");
+    if (!(p->opts.refine_tol > 0)) p->opts.refine_tol = 1e-10;
+    if (p->opts.refine_max_iter <= 0) p->opts.refine_max_iter = 30;
+    EFIE_TRY(check_port(mesh, pe, ge));
+    const int N = mesh->Ne;
+    p->Ne = N;
+    p->mu = mu;
+    p->eps = eps;
+    p->pe = pe;
+    p->ge = ge;
+    p->V0 = V0;
+    p->Z0 = Z0;
+    std::vector<double> rhs, wport;
+    EFIE_TRY(build_rhs(mesh, pe, ge, V0, spread, rhs, &wport));
+    std::vector<efie_c128> bc(N);
+    double bn = 0;
+    for (int e = 0; e < N; e++) {
+        bc[e] = efie_c128{rhs[e], 0.0};
+        bn += rhs[e] * rhs[e];
+    }
+    p->bnorm = std::sqrt(bn);
+    EFIE_TRY(p->Z.reserve(sizeof(efie_c128) * (size_t)N * N));
+    EFIE_TRY(p->b.reserve(sizeof(efie_c128) * N));
+    EFIE_TRY(p->x.reserve(sizeof(efie_c128) * N));
+    EFIE_TRY(p->wport.reserve(sizeof(double) * N));
+    EFIE_TRY(p->ipiv.reserve(sizeof(int) * N));
+    EFIE_CUDA(cudaMemcpyAsync(p->b.p, bc.data(), sizeof(efie_c128) * N, cudaMemcpyHostToDevice, ctx->stream));
+    EFIE_CUDA(cudaMemcpyAsync(p->wport.p, wport.data(), sizeof(double) * N, cudaMemcpyHostToDevice, ctx->stream));
+    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N));
+    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
+    return EFIE_OK;
+}
+
+}  // namespace
+
+extern "C" efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, double mu,
+                                        efie_c128 eps, int32_t patchEdge, int32_t groundEdge, double V0,
+                                        double spreadRadius, double Z0, const efie_sweep_opts *opts,
+                                        int32_t rule_order, efie_plan **out) {
+    if (!ctx || !out) return efie_fail(EFIE_ERR_ARGS, "null context or output");
+    *out = nullptr;
+    EFIE_TRY(check_mesh(mesh, true));
+    const int scheme = opts ? opts->scheme : EFIE_SCHEME_REF;
+    if (scheme == EFIE_SCHEME_REF) EFIE_TRY(check_prepack(mesh, pre));
+    DeviceGuard dg(ctx->device);
+    efie_plan *p = new (std::nothrow) efie_plan();
+    if (!p) return efie_fail(EFIE_ERR_NOMEM, "out of host memory");
+    p->ctx = ctx;
+    efie_status s = plan_common(p, mesh, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, opts);
+    if (s == EFIE_OK) s = efie_geom_upload(ctx, mesh, pre, scheme, rule_order, p->g);
+    if (s == EFIE_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        s = efie_fail(EFIE_ERR_CUDA, "geometry upload failed");
+    if (s != EFIE_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return EFIE_OK;
+}
+
+extern "C" void efie_plan_destroy(efie_plan *p) {
+    if (!p) return;
+    DeviceGuard dg(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    delete p;
+}
+
+extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t Nf, efie_c128 *Zin, efie_c128 *S11,
+                                     efie_c128 *I, efie_sweep_stats *st) {
+    if (!p) return efie_fail(EFIE_ERR_ARGS, "null plan");
+    if (Nf < 0 || (Nf > 0 && (!freqs || !Zin || !S11))) return efie_fail(EFIE_ERR_FREQS, "freqs must be double vector.");
+    efie_ctx *ctx = p->ctx;
+    DeviceGuard dg(ctx->device);
+    const int N = p->Ne;
+    const bool timing = p->opts.timing != 0;
+    efie_sweep_stats local{};
+    efie_sweep_stats *S = st ? st : &local;
+    std::memset(S, 0, sizeof(*S));
+    S->n_freq = Nf;
+    EFIE_TRY(p->out.reserve(sizeof(efie_c128) * 2 * std::max(Nf, 1)));
+    EFIE_TRY(p->info.reserve(sizeof(int) * std::max(Nf, 1)));
+    EFIE_CUDA(cudaMemsetAsync(p->info.p, 0, sizeof(int) * std::max(Nf, 1), ctx->stream));
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (timing)
+        for (auto &e : ev) EFIE_CUDA(cudaEventCreate(&e));
+    auto elapsed = [&](cudaEvent_t a, cudaEvent_t b) -> double {
+        float ms = 0.f;
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    };
+    efie_status rc = EFIE_OK;
+    for (int fi = 0; fi < Nf && rc == EFIE_OK; fi++) {
+        if (!(freqs[fi] > 0.0) || !std::isfinite(freqs[fi])) {
+            rc = efie_fail(EFIE_ERR_FREQS, "frequencies must be positive and finite.");
+            break;
+        }
+        const Physics ph = efie_physics(freqs[fi], p->mu, p->eps);
+        if (timing) cudaEventRecord(ev[0], ctx->stream);
+        if (p->centroid) rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph, p->Z.p, p->scratch);
+        else rc = efie_assemble_device(ctx, p->g, ph, p->Z.p, S, timing);
+        if (rc != EFIE_OK) break;
+        if (timing) cudaEventRecord(ev[1], ctx->stream);
+        bool use_fp64 = p->opts.solver == EFIE_SOLVER_FP64;
+        if (!use_fp64) {
+            rc = efie_mixed_factor(ctx, p->sw, p->Z.p, S, timing);
+            if (rc != EFIE_OK) break;
+            if (timing) cudaEventRecord(ev[2], ctx->stream);
+            int iters = 0;
+            double rel = 0;
+            bool conv = false;
+            rc = efie_mixed_refine(ctx, p->sw, p->Z.p, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
+                                   p->opts.refine_max_iter, &iters, &rel, &conv);
+            if (rc != EFIE_OK) break;
+            int err = 0;
+            rc = efie_mixed_error_flag(ctx, p->sw, &err);
+            if (rc != EFIE_OK) break;
+            if (timing) {
+                cudaEventRecord(ev[3], ctx->stream);
+                S->ms_assemble += elapsed(ev[0], ev[1]);
+                S->ms_factor += elapsed(ev[1], ev[2]);
+                S->ms_solve += elapsed(ev[2], ev[3]);
+            }
+            S->refine_iters_max = std::max(S->refine_iters_max, iters);
+            if (!conv || err) {
+                // zero pivot or stalled refinement: complex128 LU for this frequency
+                S->n_fp64_fallback++;
+                use_fp64 = true;
+            } else {
+                S->max_relres = std::max(S->max_relres, rel);
+            }
+        }
+        if (use_fp64) {
+            if (timing) cudaEventRecord(ev[2], ctx->stream);
+            rc = plan_solve_fp64(p, fi, nullptr);
+            if (rc != EFIE_OK) break;
+            if (timing && p->opts.solver == EFIE_SOLVER_FP64) {
+                cudaEventRecord(ev[3], ctx->stream);
+                S->ms_assemble += elapsed(ev[0], ev[1]);
+                S->ms_factor += elapsed(ev[2], ev[3]);
+            }
+        }
+        rc = efie_port_reduce(ctx, N, p->x.p, p->wport.as<double>(), p->centroid ? EFIE_PORT_EDGE_DIFF : p->opts.port_model,
+                              p->pe - 1, p->ge - 1, p->V0, p->Z0, p->out.as<efie_c128>() + 2 * fi);
+        if (rc != EFIE_OK) break;
+        if (I) {
+            cudaError_t e = cudaMemcpyAsync(I + (size_t)fi * N, p->x.p, sizeof(efie_c128) * N, cudaMemcpyDeviceToHost,
+                                            ctx->stream);
+            if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
+        }
+    }
+    if (rc == EFIE_OK && Nf > 0) {
+        std::vector<efie_c128> res(2 * (size_t)Nf);
+        std::vector<int> info(Nf);
+        cudaError_t e = cudaMemcpyAsync(res.data(), p->out.p, sizeof(efie_c128) * 2 * Nf, cudaMemcpyDeviceToHost,
+                                        ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(info.data(), p->info.p, sizeof(int) * Nf, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
+        else {
+            for (int fi = 0; fi < Nf; fi++) {
+                Zin[fi] = res[2 * fi];
+                S11[fi] = res[2 * fi + 1];
+            }
+            for (int fi = 0; fi < Nf; fi++)
+                if (info[fi] != 0) {
+                    rc = efie_fail(EFIE_ERR_SINGULAR, "Z is singular at frequency index " + std::to_string(fi + 1) +
+                                                          " (getrf info " + std::to_string(info[fi]) + ").");
+                    break;
+                }
+        }
+    } else {
+        cudaStreamSynchronize(ctx->stream);
+    }
+    if (timing)
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    return rc;
+}
+
+extern "C" efie_status efie_patch_sweep_fastquad(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre,
+                                                 const double *freqs, int32_t Nf, double mu, efie_c128 eps,
+                                                 int32_t patchEdge, int32_t groundEdge, double V0, double spreadRadius,
+                                                 double Z0, const efie_sweep_opts *opts, efie_c128 *Zin,
+                                                 efie_c128 *S11, efie_c128 *I, efie_sweep_stats *stats) {
+    efie_plan *p = nullptr;
+    efie_sweep_opts o;
+    if (opts) o = *opts;
+    else efie_sweep_opts_default(&o);
+    o.scheme = EFIE_SCHEME_REF;
+    EFIE_TRY(efie_plan_create(ctx, mesh, pre, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, &o, 0, &p));
+    efie_status s = efie_plan_run(p, freqs, Nf, Zin, S11, I, stats);
+    efie_plan_destroy(p);
+    return s;
+}
+
+extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh *mesh, const double *freqs, int32_t Nf,
+                                                 double mu, efie_c128 eps, int32_t patchEdge, int32_t groundEdge,
+                                                 double V0, double spreadRadius, double Z0,
+                                                 const efie_sweep_opts *opts, efie_c128 *Zin, efie_c128 *S11,
+                                                 efie_c128 *I, efie_sweep_stats *stats) {
+    if (!ctx) return efie_fail(EFIE_ERR_ARGS, "null context");
+    EFIE_TRY(check_mesh(mesh, true));
+    DeviceGuard dg(ctx->device);
+    efie_plan *p = new (std::nothrow) efie_plan();
+    if (!p) return efie_fail(EFIE_ERR_NOMEM, "out of host memory");
+    p->ctx = ctx;
+    p->centroid = true;
+    p->self_alpha = 0.20;  // patch_sweep_cuda.cu:269
+    efie_sweep_opts o;
+    if (opts) o = *opts;
+    else efie_sweep_opts_default(&o);
+    o.port_model = EFIE_PORT_EDGE_DIFF;
+    efie_status s = plan_common(p, mesh, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, &o);
+    if (s == EFIE_OK) {
+        const int Ne = mesh->Ne, Nt = mesh->Nt, Nv = mesh->Nv;
+        p->hV.assign(mesh->V, mesh->V + 3 * (size_t)Nv);
+        p->hF.assign(mesh->F, mesh->F + 3 * (size_t)Nt);
+        p->hpt.assign(mesh->plusTri, mesh->plusTri + Ne);
+        p->hmt.assign(mesh->minusTri, mesh->minusTri + Ne);
+        p->hps.assign(mesh->plusSign, mesh->plusSign + Ne);
+        p->hms.assign(mesh->minusSign, mesh->minusSign + Ne);
+        p->hrp.assign(mesh->rp, mesh->rp + 3 * (size_t)Ne);
+        p->hrm.assign(mesh->rm, mesh->rm + 3 * (size_t)Ne);
+        p->hAp.assign(mesh->Ap, mesh->Ap + Ne);
+        p->hAm.assign(mesh->Am, mesh->Am + Ne);
+        p->hlen.assign(mesh->len, mesh->len + Ne);
+        p->cmesh = efie_mesh{Nv, Nt, Ne, p->hV.data(), p->hF.data(), nullptr, p->hpt.data(), p->hmt.data(),
+                             p->hps.data(), p->hms.data(), p->hrp.data(), p->hrm.data(), p->hAp.data(),
+                             p->hAm.data(), p->hlen.data()};
+        // k by std::sqrt of the complex product (patch_sweep_cuda.cu:447) equals
+        // the polar form used by efie_physics up to rounding.
+        s = efie_plan_run(p, freqs, Nf, Zin, S11, I, stats);
+    }
+    efie_plan_destroy(p);
+    return s;
+}

@@ -1,0 +1,108 @@
+// Internal declarations shared by the native sources of libefie_b200.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/efie_b200.h"
+
+// Record `msg` as the calling thread's last error and return `s`.
+efie_status efie_fail(efie_status s, const std::string &msg);
+
+// tri_quad_rule points/weights (u, v, w arrays of at least 7 entries).
+int efie_quad_rule(int order, double *u, double *v, double *w);
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#define EFIE_CUDA(call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return efie_fail(EFIE_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define EFIE_TRY(call)                         \
+    do {                                       \
+        efie_status s_ = (call);               \
+        if (s_ != EFIE_OK) return s_;          \
+    } while (0)
+
+// A device allocation owned by a context or plan; grows, never shrinks.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    efie_status reserve(size_t n) {
+        if (n <= bytes) return EFIE_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n ? n : 1);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return efie_fail(EFIE_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return EFIE_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    ~DevBuf() { release(); }
+};
+
+struct efie_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    int num_sms = 0;
+    int cc_major = 0;
+    DevBuf status;   // device-side error flags of bounded waits (int32[8])
+};
+
+// Device geometry of one sweep/assembly problem (uploaded once per plan).
+struct GeomDev {
+    int Ne = 0, Nt = 0, Nq = 0, Nq2 = 0, NsS = 0, NsN = 0;
+    int n_near = 0;           // number of near (t1 < t2) pairs
+    bool symmetric = true;    // nearMat symmetric -> regular moments only for t1 <= t2
+    int scheme = EFIE_SCHEME_REF;
+    double near_alpha = 0.0;
+    DevBuf origin;            // double4[Nt]  (origin of local coordinates)
+    DevBuf reg_pts;           // double4[Nt*Nq]  (rho - relative to origin, w)
+    DevBuf near_pts;          // double4[Nt*NsN*Nq2]
+    DevBuf self_pts;          // double4[Nt*NsS*Nq2]
+    DevBuf self_a;            // double[Nt*NsS]
+    DevBuf aeq;               // double[Nt]
+    DevBuf near_mask;         // uint8[Nt*Nt] (1 = near or self: not a regular pair)
+    DevBuf near_list;         // int2[n_near] (t1 < t2)
+    DevBuf edge_tri;          // int32[2*Ne] (side 0 = plus, 1 = minus; -1 = none)
+    DevBuf edge_cd;           // double4[2*Ne] (delta = free vertex - origin, c)
+    DevBuf tri_vtx;           // double4[3*Nt] vertices relative to origin (extraction scheme)
+    DevBuf adj_list;          // int2[] vertex-adjacent pairs t1 < t2 (extraction scheme)
+    int n_adj = 0;
+    DevBuf moments;           // double[16 * npairs]
+    size_t npairs = 0;
+};
+
+// Per-frequency physics: k = w sqrt(mu eps) (principal branch), alpha = j w mu,
+// beta = 1/(j w eps)  (patch_sweep_fastquad_cuda.cu:713-743).
+struct Physics {
+    double kr, ki, alr, ali, ber, bei;
+};
+Physics efie_physics(double freq, double mu, efie_c128 eps);
+Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
+
+// assemble.cu
+efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
+                             int rule_order, GeomDev &g);
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/,
+                                 efie_sweep_stats *st, bool timing);
+efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, double selfAlpha,
+                                          const Physics &ph, void *Z, DevBuf &scratch);
+#endif

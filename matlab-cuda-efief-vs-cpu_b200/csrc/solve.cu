@@ -1,0 +1,639 @@
+// Mixed-precision dense solve of Z x = V on sm_100a.
+//
+// The reference factors Z in complex128 with cusolverDnZgetrf/Zgetrs
+// (patch_sweep_fastquad_cuda.cu:765-771).  Here Z (complex128, column-major,
+// as assembled) is kept for the residual, and a complex64 copy is factored
+// without pivoting (Z is complex symmetric and, for these EFIE matrices,
+// strongly diagonal: element growth stays near 1); FP64 iterative
+// refinement then recovers the complex128 solution:
+//     x = 0, r = V;  repeat { d = U^-1 L^-1 r (complex64);  x += d;
+//                            r = V - Z x (complex128) }  until ||r|| <= tol ||V||.
+// A zero pivot or a refinement that stalls makes the caller re-solve that
+// frequency with the complex128 LU.
+//
+// Layout of the complex64 working matrix: two FP32 planes (re, im),
+// row-major, leading dimension ld (multiple of 4).  Z is symmetric, so the
+// row-major planes are filled from the column-major Z by a tiled transpose.
+#include <cmath>
+#include <vector>
+
+#include "efie_internal.h"
+#include "solve.h"
+
+namespace {
+
+constexpr int NB = 64;  // diagonal block size of the LU and the triangular solves
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// ---------------------------------------------------------------------------
+// Z (c128, column-major Ne x Ne) -> planes (row-major, ld).  32x32 tiles.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__restrict__ Z, float *__restrict__ Ar,
+                                                     float *__restrict__ Ai, int ld) {
+    __shared__ float tr[32][33], ti[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // bx: column block of Z, by: row block of Z
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        const int row = by + tx, col = bx + r;  // coalesced along rows of the column-major Z
+        double2 v = (row < N && col < N) ? Z[(size_t)row + (size_t)N * col] : make_double2(0, 0);
+        tr[r][tx] = (float)v.x;
+        ti[r][tx] = (float)v.y;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int row = by + r, col = bx + tx;  // row-major plane, coalesced along columns
+        if (row < N && col < N) {
+            Ar[(size_t)row * ld + col] = tr[tx][r];
+            Ai[(size_t)row * ld + col] = ti[tx][r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal block: unblocked LU (no pivoting) of A[k:k+kb, k:k+kb] and the
+// inverses of its unit-lower L and upper U factors (kept for the panel
+// products and the triangular solves).  One CTA of 1024 threads.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__restrict__ Ar, float *__restrict__ Ai,
+                                                      int ld, float2 *__restrict__ Linv, float2 *__restrict__ Uinv,
+                                                      int *__restrict__ err) {
+    extern __shared__ float2 dyn[];
+    float2(*a)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);
+    float2(*w)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += 1024) {
+        const int i = e / NB, j = e % NB;
+        float2 v = make_float2(0.f, 0.f);
+        if (i < kb && j < kb) v = make_float2(Ar[(size_t)(k + i) * ld + k + j], Ai[(size_t)(k + i) * ld + k + j]);
+        else if (i == j) v = make_float2(1.f, 0.f);  // pad to identity
+        a[i][j] = v;
+    }
+    __syncthreads();
+    for (int j = 0; j < NB - 1; j++) {
+        const float2 p = a[j][j];
+        const float den = p.x * p.x + p.y * p.y;
+        if (tid == 0 && !(den > 0.f)) atomicExch(err, 1);
+        const float2 pinv = make_float2(p.x / den, -p.y / den);
+        if (tid > j && tid < NB) a[tid][j] = cmulf(a[tid][j], pinv);
+        __syncthreads();
+        for (int e = tid; e < NB * NB; e += 1024) {
+            const int i = e / NB, c = e % NB;
+            if (i > j && c > j) {
+                const float2 l = a[i][j], u = a[j][c];
+                a[i][c].x -= l.x * u.x - l.y * u.y;
+                a[i][c].y -= l.x * u.y + l.y * u.x;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const float2 p = a[NB - 1][NB - 1];
+        if (!(p.x * p.x + p.y * p.y > 0.f)) atomicExch(err, 1);
+    }
+    // write the factors back
+    for (int e = tid; e < NB * NB; e += 1024) {
+        const int i = e / NB, j = e % NB;
+        if (i < kb && j < kb) {
+            Ar[(size_t)(k + i) * ld + k + j] = a[i][j].x;
+            Ai[(size_t)(k + i) * ld + k + j] = a[i][j].y;
+        }
+    }
+    // Linv: unit lower; column c by forward substitution.  16 threads per column.
+    const int c = tid >> 4, sub = tid & 15;
+    for (int i = 0; i < NB; i++) {
+        float2 s = make_float2(0.f, 0.f);
+        for (int j = c + sub; j < i; j += 16) {
+            const float2 l = a[i][j], x = w[j][c];
+            s.x += l.x * x.x - l.y * x.y;
+            s.y += l.x * x.y + l.y * x.x;
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            s.x += __shfl_xor_sync(0xffffffffu, s.x, o, 16);
+            s.y += __shfl_xor_sync(0xffffffffu, s.y, o, 16);
+        }
+        if (sub == 0) w[i][c] = (i < c) ? make_float2(0.f, 0.f) : (i == c ? make_float2(1.f, 0.f) : make_float2(-s.x, -s.y));
+        __syncthreads();
+    }
+    for (int e = tid; e < NB * NB; e += 1024) Linv[e] = w[e / NB][e % NB];
+    __syncthreads();
+    // Uinv: upper; column c by backward substitution.
+    for (int i = NB - 1; i >= 0; i--) {
+        float2 s = make_float2(0.f, 0.f);
+        for (int j = i + 1 + sub; j <= c; j += 16) {
+            const float2 u = a[i][j], x = w[j][c];
+            s.x += u.x * x.x - u.y * x.y;
+            s.y += u.x * x.y + u.y * x.x;
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            s.x += __shfl_xor_sync(0xffffffffu, s.x, o, 16);
+            s.y += __shfl_xor_sync(0xffffffffu, s.y, o, 16);
+        }
+        if (sub == 0) {
+            float2 r = make_float2(0.f, 0.f);
+            if (i <= c) {
+                const float2 d = a[i][i];
+                const float den = d.x * d.x + d.y * d.y;
+                const float2 rhs = (i == c) ? make_float2(1.f - s.x, -s.y) : make_float2(-s.x, -s.y);
+                r = make_float2((rhs.x * d.x + rhs.y * d.y) / den, (rhs.y * d.x - rhs.x * d.y) / den);
+            }
+            w[i][c] = r;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < NB * NB; e += 1024) Uinv[e] = w[e / NB][e % NB];
+}
+
+// ---------------------------------------------------------------------------
+// Panels: U12 = Linv * A12 (rows k..k+kb, columns right of the block) and
+// L21 = A21 * Uinv (columns k..k+kb, rows below).  One 64x64 tile per CTA,
+// in place.  blockIdx.y = 0: row panel, 1: column panel.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, float *__restrict__ Ar, float *__restrict__ Ai,
+                                                int ld, const float2 *__restrict__ Linv,
+                                                const float2 *__restrict__ Uinv) {
+    extern __shared__ float2 dyn[];
+    float2(*M)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);               // the inverse
+    float2(*T)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));  // the panel tile
+    const int tid = threadIdx.x;
+    const bool rowp = blockIdx.y == 0;
+    const int off = k + kb + blockIdx.x * NB;  // first column (row panel) / row (column panel) of the tile
+    if (off >= N) return;
+    const int ext = min(NB, N - off);
+    const float2 *inv = rowp ? Linv : Uinv;
+    for (int e = tid; e < NB * NB; e += 256) M[e / NB][e % NB] = inv[e];
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int i = e / NB, j = e % NB;  // i: row within the tile, j: column within the tile
+        float2 v = make_float2(0.f, 0.f);
+        if (rowp) {
+            if (i < kb && j < ext) v = make_float2(Ar[(size_t)(k + i) * ld + off + j], Ai[(size_t)(k + i) * ld + off + j]);
+        } else {
+            if (i < ext && j < kb) v = make_float2(Ar[(size_t)(off + i) * ld + k + j], Ai[(size_t)(off + i) * ld + k + j]);
+        }
+        T[i][j] = v;
+    }
+    __syncthreads();
+    // each thread: 16 outputs (4 rows x 4 cols)
+    const int r0 = (tid >> 4) * 4, c0 = (tid & 15) * 4;
+    float2 acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
+    for (int q = 0; q < NB; q++) {
+        float2 x[4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            x[a] = rowp ? M[r0 + a][q] : T[r0 + a][q];
+            y[a] = rowp ? T[q][c0 + a] : M[q][c0 + a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                acc[a][b].x += x[a].x * y[b].x - x[a].y * y[b].y;
+                acc[a][b].y += x[a].x * y[b].y + x[a].y * y[b].x;
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = r0 + a, j = c0 + b;
+            if (rowp) {
+                if (i < kb && j < ext) {
+                    Ar[(size_t)(k + i) * ld + off + j] = acc[a][b].x;
+                    Ai[(size_t)(k + i) * ld + off + j] = acc[a][b].y;
+                }
+            } else {
+                if (i < ext && j < kb) {
+                    Ar[(size_t)(off + i) * ld + k + j] = acc[a][b].x;
+                    Ai[(size_t)(off + i) * ld + k + j] = acc[a][b].y;
+                }
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Trailing update A22 -= L21 * U12 on CUDA cores (complex FP32), 64x64 tiles,
+// K = kb <= 64.  Used for small trailing matrices and as the portable path.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float *__restrict__ Ar,
+                                                     float *__restrict__ Ai, int ld) {
+    extern __shared__ float2 dyn[];
+    float2(*Ls)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);
+    float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
+    const int tid = threadIdx.x;
+    const int s = k + kb;
+    const int row0 = s + blockIdx.y * NB, col0 = s + blockIdx.x * NB;
+    if (row0 >= N || col0 >= N) return;
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int i = e / NB, j = e % NB;
+        Ls[i][j] = (row0 + i < N && j < kb)
+                       ? make_float2(Ar[(size_t)(row0 + i) * ld + k + j], Ai[(size_t)(row0 + i) * ld + k + j])
+                       : make_float2(0.f, 0.f);
+        Us[i][j] = (i < kb && col0 + j < N)
+                       ? make_float2(Ar[(size_t)(k + i) * ld + col0 + j], Ai[(size_t)(k + i) * ld + col0 + j])
+                       : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int r0 = (tid >> 4) * 4, c0 = (tid & 15) * 4;
+    float2 acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
+    for (int q = 0; q < kb; q++) {
+        float2 x[4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            x[a] = Ls[r0 + a][q];
+            y[a] = Us[q][c0 + a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                acc[a][b].x += x[a].x * y[b].x - x[a].y * y[b].y;
+                acc[a][b].y += x[a].x * y[b].y + x[a].y * y[b].x;
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = row0 + r0 + a, j = col0 + c0 + b;
+            if (i < N && j < N) {
+                Ar[(size_t)i * ld + j] -= acc[a][b].x;
+                Ai[(size_t)i * ld + j] -= acc[a][b].y;
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Triangular solves with the factored planes.  Persistent cooperative grid;
+// block row b waits (bounded) for the flags of the blocks it depends on.
+// lower: y = L^-1 r  (unit lower, forward);  upper: d = U^-1 y (backward) and
+// x += d in FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool wait_flag(const volatile int *flag, int epoch, int *err) {
+    long long spins = 0;
+    while (*flag != epoch) {
+        if (++spins > (1ll << 24)) {  // ~ a few hundred ms: give up, record the error
+            atomicExch(err, 2);
+            return false;
+        }
+        if (*((volatile int *)err)) return false;
+        __nanosleep(64);
+    }
+    __threadfence();
+    return true;
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(256) k_trsv(int N, int nblk, const float *__restrict__ Ar,
+                                              const float *__restrict__ Ai, int ld, const float2 *__restrict__ dinv,
+                                              const float2 *__restrict__ rhs, float2 *__restrict__ out,
+                                              double2 *__restrict__ x, int *flags, int epoch, int *err,
+                                              const int *__restrict__ skip) {
+    if (skip && *skip) return;  // refinement already converged
+    __shared__ float2 acc[NB];
+    __shared__ float2 yj[NB];
+    __shared__ float2 part[4][NB];
+    __shared__ int ok;
+    const int tid = threadIdx.x;
+    const int row = tid & 63, quarter = tid >> 6;
+    for (int it = blockIdx.x; it < nblk; it += gridDim.x) {
+        const int b = LOWER ? it : nblk - 1 - it;
+        const int r0 = b * NB;
+        const int rows = min(NB, N - r0);
+        if (tid < NB) acc[tid] = (tid < rows) ? rhs[r0 + tid] : make_float2(0.f, 0.f);
+        if (tid == 0) ok = 1;
+        __syncthreads();
+        const int jbeg = LOWER ? 0 : b + 1, jend = LOWER ? b : nblk;
+        for (int jb = jbeg; jb < jend; jb++) {
+            if (tid == 0) {
+                if (!wait_flag(flags + jb, epoch, err)) ok = 0;
+            }
+            __syncthreads();
+            if (!ok) return;
+            const int c0 = jb * NB;
+            const int cols = min(NB, N - c0);
+            // written by another CTA of this grid: read through L2 only
+            if (tid < NB) yj[tid] = (tid < cols) ? __ldcg(out + c0 + tid) : make_float2(0.f, 0.f);
+            __syncthreads();
+            float2 s = make_float2(0.f, 0.f);
+            if (row < rows) {
+                const float *pr = Ar + (size_t)(r0 + row) * ld + c0;
+                const float *pi = Ai + (size_t)(r0 + row) * ld + c0;
+                for (int c = quarter * 16; c < quarter * 16 + 16 && c < cols; c++) {
+                    const float2 l = make_float2(pr[c], pi[c]);
+                    const float2 v = yj[c];
+                    s.x += l.x * v.x - l.y * v.y;
+                    s.y += l.x * v.y + l.y * v.x;
+                }
+            }
+            part[quarter][row] = s;
+            __syncthreads();
+            if (tid < NB) {
+                float2 t = acc[tid];
+                t.x -= part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
+                t.y -= part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
+                acc[tid] = t;
+            }
+            __syncthreads();
+        }
+        // y_b = inv(diag block) * acc
+        const float2 *D = dinv + (size_t)b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
+        float2 s = make_float2(0.f, 0.f);
+        for (int c = quarter * 16; c < quarter * 16 + 16; c++) {
+            const float2 m = D[row * NB + c];
+            const float2 v = acc[c];
+            s.x += m.x * v.x - m.y * v.y;
+            s.y += m.x * v.y + m.y * v.x;
+        }
+        part[quarter][row] = s;
+        __syncthreads();
+        if (tid < rows) {
+            float2 t;
+            t.x = part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
+            t.y = part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
+            out[r0 + tid] = t;
+            if (!LOWER) {
+                double2 xv = x[r0 + tid];
+                xv.x += (double)t.x;
+                xv.y += (double)t.y;
+                x[r0 + tid] = xv;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicExch(flags + b, epoch);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// r = V - Z x  (complex128 GEMV over the column-major Z), the complex64 copy
+// of r for the next correction, and ||r||^2.  Block = 32 rows x 8 column
+// groups.  The last CTA turns ||r|| into the convergence flag.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restrict__ Z, const double2 *__restrict__ x,
+                                                  const double2 *__restrict__ b, float2 *__restrict__ rf,
+                                                  double *__restrict__ red /* [0]=sum r^2, [1]=||b||, [2]=relres */,
+                                                  unsigned int *__restrict__ counter, int *__restrict__ conv,
+                                                  double tol, int *__restrict__ skip) {
+    if (*skip) return;
+    __shared__ double2 part[8][32];
+    __shared__ double sq[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int m = blockIdx.x * 32 + lane;
+    double2 s = make_double2(0.0, 0.0);
+    if (m < N) {
+        for (int n = g; n < N; n += 8) {
+            const double2 z = Z[(size_t)m + (size_t)N * n];
+            const double2 v = x[n];
+            s.x += z.x * v.x - z.y * v.y;
+            s.y += z.x * v.y + z.y * v.x;
+        }
+    }
+    part[g][lane] = s;
+    __syncthreads();
+    if (g == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int i = 0; i < 8; i++) {
+            t.x += part[i][lane].x;
+            t.y += part[i][lane].y;
+        }
+        double q = 0.0;
+        if (m < N) {
+            const double2 bb = b[m];
+            const double2 r = make_double2(bb.x - t.x, bb.y - t.y);
+            rf[m] = make_float2((float)r.x, (float)r.y);
+            q = r.x * r.x + r.y * r.y;
+        }
+        sq[lane] = q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double q = 0.0;
+        for (int i = 0; i < 32; i++) q += sq[i];
+        atomicAdd(red, q);
+        __threadfence();
+        const unsigned int done = atomicAdd(counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const double rr = sqrt(*((volatile double *)red));
+        const double rel = rr / red[1];
+        red[2] = rel;
+        red[0] = 0.0;
+        *counter = 0u;
+        if (rel <= tol) {
+            *conv = 1;
+            *skip = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Port reduction + Zin/S11 (patch_sweep_fastquad_cuda.cu:777-799 for the
+// Gaussian model; patch_sweep_cuda.cu:484-494 for the edge difference).
+// One CTA.  out[0] = Zin, out[1] = S11.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_port(int N, const double2 *__restrict__ x, const double *__restrict__ wport,
+                                               int model, int pe, int ge, double V0, double Z0,
+                                               double2 *__restrict__ out) {
+    __shared__ double sr[1024], si[1024];
+    const int tid = threadIdx.x;
+    double a = 0.0, c = 0.0;
+    if (model == EFIE_PORT_GAUSS) {
+        for (int i = tid; i < N; i += 1024) {
+            a += wport[i] * x[i].x;
+            c += wport[i] * x[i].y;
+        }
+    }
+    sr[tid] = a;
+    si[tid] = c;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1) {
+        if (tid < o) {
+            sr[tid] += sr[tid + o];
+            si[tid] += si[tid + o];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double Ipr = sr[0], Ipi = si[0];
+        if (model == EFIE_PORT_EDGE_DIFF) {
+            Ipr = x[pe].x - x[ge].x;
+            Ipi = x[pe].y - x[ge].y;
+        }
+        const double den = Ipr * Ipr + Ipi * Ipi;
+        const double Zr = V0 * (Ipr / den), Zi = -V0 * (Ipi / den);
+        const double ar = Zr - Z0, ai = Zi, br = Zr + Z0, bi = Zi;
+        const double bden = br * br + bi * bi;
+        out[0] = make_double2(Zr, Zi);
+        out[1] = make_double2((ar * br + ai * bi) / bden, (ai * br - ar * bi) / bden);
+    }
+}
+
+__global__ void k_fill_c128(int N, double2 *__restrict__ dst, double2 v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) dst[i] = v;
+}
+
+}  // namespace
+
+int efie_solve_nb() { return NB; }
+
+namespace {
+constexpr size_t kTwoTiles = sizeof(float2) * 2 * NB * (NB + 1);
+
+efie_status set_smem_attrs() {
+    static bool done = false;
+    if (done) return EFIE_OK;
+    EFIE_CUDA(cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
+    EFIE_CUDA(cudaFuncSetAttribute(k_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
+    done = true;
+    return EFIE_OK;
+}
+}  // namespace
+
+efie_status efie_mixed_workspace(SolveWork &w, int N) {
+    EFIE_TRY(set_smem_attrs());
+    w.N = N;
+    w.ld = (N + 63) / 64 * 64;
+    w.nblk = (N + NB - 1) / NB;
+    EFIE_TRY(w.planes.reserve(sizeof(float) * 2 * (size_t)w.ld * N));
+    EFIE_TRY(w.dinv.reserve(sizeof(float2) * 2 * (size_t)NB * NB * w.nblk));
+    EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.ld));
+    const size_t fbytes = sizeof(int) * 2 * (size_t)w.nblk;
+    if (fbytes > w.flags.bytes) {
+        EFIE_TRY(w.flags.reserve(fbytes));
+        EFIE_CUDA(cudaMemset(w.flags.p, 0, fbytes));  // epochs restart above any stale value
+        w.epoch = 0;
+    }
+    EFIE_TRY(w.ctl.reserve(256));
+    return EFIE_OK;
+}
+
+efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, efie_sweep_stats *st, bool timing) {
+    cudaStream_t s = ctx->stream;
+    const int N = w.N, ld = w.ld;
+    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)ld * N;
+    int *err = reinterpret_cast<int *>(w.ctl.as<char>() + 64);
+    EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 256, s));
+    dim3 tg((N + 31) / 32, (N + 31) / 32);
+    k_z_to_planes<<<tg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), Ar, Ai, ld);
+    EFIE_CUDA(cudaGetLastError());
+    float2 *dinv = w.dinv.as<float2>();
+    for (int bi = 0; bi < w.nblk; bi++) {
+        const int k = bi * NB, kb = std::min(NB, N - k);
+        float2 *Linv = dinv + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
+        k_diag_factor<<<1, 1024, kTwoTiles, s>>>(k, kb, Ar, Ai, ld, Linv, Uinv, err);
+        const int rest = N - k - kb;
+        if (rest > 0) {
+            dim3 pg((rest + NB - 1) / NB, 2);
+            k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, Ar, Ai, ld, Linv, Uinv);
+            EFIE_TRY(efie_trailing_update(ctx, w, k, kb, st, timing));
+        }
+    }
+    EFIE_CUDA(cudaGetLastError());
+    return EFIE_OK;
+}
+
+efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb) {
+    const int N = w.N, rest = N - k - kb;
+    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)w.ld * N;
+    dim3 g((rest + NB - 1) / NB, (rest + NB - 1) / NB);
+    k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, k, kb, Ar, Ai, w.ld);
+    EFIE_CUDA(cudaGetLastError());
+    return EFIE_OK;
+}
+
+efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const void *b, void *x, double bnorm,
+                              double tol, int max_iter, int *iters, double *relres, bool *converged) {
+    cudaStream_t s = ctx->stream;
+    const int N = w.N, ld = w.ld;
+    const float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)ld * N;
+    float2 *rf = w.vec.as<float2>(), *y = rf + ld, *d = y + ld;
+    char *ctl = w.ctl.as<char>();
+    double *red = reinterpret_cast<double *>(ctl);            // [0..2]
+    unsigned int *counter = reinterpret_cast<unsigned int *>(ctl + 32);
+    int *conv = reinterpret_cast<int *>(ctl + 40);
+    int *skip = reinterpret_cast<int *>(ctl + 44);
+    int *err = reinterpret_cast<int *>(ctl + 64);
+    int *flagsL = w.flags.as<int>(), *flagsU = flagsL + w.nblk;
+    // x = 0, rf = b (complex64), red = {0, ||b||, 1}
+    k_fill_c128<<<(N + 255) / 256, 256, 0, s>>>(N, static_cast<double2 *>(x), make_double2(0.0, 0.0));
+    const double init[3] = {0.0, bnorm, 1.0};
+    EFIE_CUDA(cudaMemcpyAsync(red, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    EFIE_CUDA(cudaMemsetAsync(ctl + 32, 0, 16, s));
+    int grid = std::min(w.nblk, ctx->num_sms);
+    int it = 0;
+    bool done = false;
+    int hconv = 0;
+    // initial residual r = b (x = 0) through the residual kernel keeps one code path
+    k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z), static_cast<const double2 *>(x),
+                                             static_cast<const double2 *>(b), rf, red, counter, conv, -1.0, skip);
+    EFIE_CUDA(cudaGetLastError());
+    while (!done) {
+        const int chunk = std::min(5, max_iter - it);
+        if (chunk <= 0) break;
+        for (int c = 0; c < chunk; c++) {
+            const int epoch = ++w.epoch;
+            void *argsL[] = {(void *)&N, (void *)&w.nblk, (void *)&Ar, (void *)&Ai, (void *)&ld,
+                             (void *)&w.dinv.p, (void *)&rf, (void *)&y, (void *)&x, (void *)&flagsL,
+                             (void *)&epoch, (void *)&err, (void *)&skip};
+            EFIE_CUDA(cudaLaunchCooperativeKernel((const void *)k_trsv<true>, dim3(grid), dim3(256), argsL, 0, s));
+            const float2 *yc = y;
+            void *argsU[] = {(void *)&N, (void *)&w.nblk, (void *)&Ar, (void *)&Ai, (void *)&ld,
+                             (void *)&w.dinv.p, (void *)&yc, (void *)&d, (void *)&x, (void *)&flagsU,
+                             (void *)&epoch, (void *)&err, (void *)&skip};
+            EFIE_CUDA(cudaLaunchCooperativeKernel((const void *)k_trsv<false>, dim3(grid), dim3(256), argsU, 0, s));
+            k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z),
+                                                     static_cast<const double2 *>(x),
+                                                     static_cast<const double2 *>(b), rf, red, counter, conv, tol,
+                                                     skip);
+            EFIE_CUDA(cudaGetLastError());
+        }
+        it += chunk;
+        int hctl[2] = {0, 0};
+        EFIE_CUDA(cudaMemcpyAsync(hctl, conv, sizeof(int), cudaMemcpyDeviceToHost, s));
+        EFIE_CUDA(cudaMemcpyAsync(hctl + 1, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        EFIE_CUDA(cudaStreamSynchronize(s));
+        hconv = hctl[0];
+        if (hctl[1]) break;
+        if (hconv) done = true;
+    }
+    double hred[3];
+    EFIE_CUDA(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, s));
+    EFIE_CUDA(cudaStreamSynchronize(s));
+    *relres = hred[2];
+    *iters = it;
+    *converged = hconv != 0;
+    return EFIE_OK;
+}
+
+efie_status efie_port_reduce(efie_ctx *ctx, int N, const void *x, const double *wport, int model, int pe, int ge,
+                             double V0, double Z0, void *out2) {
+    k_port<<<1, 1024, 0, ctx->stream>>>(N, static_cast<const double2 *>(x), wport, model, pe, ge, V0, Z0,
+                                         static_cast<double2 *>(out2));
+    EFIE_CUDA(cudaGetLastError());
+    return EFIE_OK;
+}
+
+efie_status efie_mixed_error_flag(efie_ctx *ctx, SolveWork &w, int *flag) {
+    EFIE_CUDA(cudaMemcpyAsync(flag, w.ctl.as<char>() + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
+    return EFIE_OK;
+}

@@ -1,0 +1,108 @@
+"""GPU parity of the frequency sweeps (assemble + solve + Zin/S11) against the
+FP64 oracle (C assembly + LAPACK solve) and the reference's own CUDA sweep.
+Tolerances: complex128 LU path |dZin|/|Zin| <= 1e-9; mixed path (complex64
+tensor-core LU + FP64 refinement to 1e-10) |dZin|/|Zin| <= 1e-6."""
+import numpy as np
+import pytest
+
+import efie_oracle as eo
+import oracle_c as oc
+from conftest import pkg, small_design, config1_design
+
+pytestmark = pytest.mark.gpu
+
+
+def _sweep(p, freqs, solver, **kw):
+    m = pkg()
+    r = p["rwg"]
+    d = p["design"]
+    st = {}
+    out = m.patch_sweep_fastquad_cuda(
+        p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"], r["rm"],
+        r["Ap"], r["Am"], r["len"], p["prepack"], np.asarray(freqs, np.float64), d.mu, d.eps, p["patchEdge"],
+        p["groundEdge"], d.V0, p["spread"], d.Z0, opts=m.sweep_opts(solver=solver, **kw), stats=st)
+    return out[0], out[1], st
+
+
+def _oracle(p, freqs):
+    return eo.solve_sweep(p, freqs, assemble=oc.assemble_z)
+
+
+@pytest.mark.parametrize("name,design", [("small", lambda: small_design("grid")),
+                                         ("reference_sweep_538", eo.reference_sweep_design),
+                                         ("config1_1074", lambda: config1_design("grid"))])
+@pytest.mark.parametrize("solver,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_sweep_matches_oracle(name, design, solver, tol):
+    d = design()
+    p = eo.build_problem(d)
+    freqs = d.freqs[[0, len(d.freqs) // 2, -1]]
+    Zin, S11, st = _sweep(p, freqs, solver)
+    Zo, So = _oracle(p, freqs)
+    err = np.abs(Zin - Zo) / np.abs(Zo)
+    assert err.max() <= tol, err
+    assert np.abs(S11 - So).max() <= 10 * tol
+    if solver == "mixed":
+        assert st["max_relres"] <= 1e-10 and st["n_fp64_fallback"] == 0
+
+
+def test_sweep_matches_reference_cuda():
+    ref_mex = pytest.importorskip("ref_mex")
+    d = eo.reference_sweep_design()
+    p = eo.build_problem(d)
+    freqs = d.freqs[::10]
+    Zr, Sr = ref_mex.patch_sweep_fastquad(p, freqs)
+    for solver, tol in (("fp64", 1e-9), ("mixed", 1e-6)):
+        Zin, S11, _ = _sweep(p, freqs, solver)
+        assert (np.abs(Zin - Zr) / np.abs(Zr)).max() <= tol
+
+
+def test_refinement_fallback_to_fp64():
+    """A refinement that cannot reach its target re-solves with the complex128 LU."""
+    d = small_design("grid")
+    p = eo.build_problem(d)
+    freqs = d.freqs
+    Zin, _, st = _sweep(p, freqs, "mixed", refine_tol=1e-30, refine_max_iter=2)
+    assert st["n_fp64_fallback"] == len(freqs)
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zin - Zo) / np.abs(Zo)).max() <= 1e-9
+
+
+def test_centroid_sweep_matches_reference():
+    m = pkg()
+    d = small_design("grid")
+    p = eo.build_problem(d)
+    r = p["rwg"]
+    Zin, S11 = m.patch_sweep_cuda(p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"],
+                                  r["minusSign"], r["rp"], r["rm"], r["Ap"], r["Am"], r["len"], d.freqs, d.mu,
+                                  d.eps, np.int32(p["patchEdge"]), np.int32(p["groundEdge"]), d.V0, p["spread"],
+                                  d.Z0)
+    # oracle: centroid Z, LAPACK solve, edge-difference port
+    Zo = []
+    for f in d.freqs:
+        omega, k, _, _ = eo.physics(f, d.mu, d.eps)
+        Z = oc.assemble_centroid(p["V"], p["F"], r, 0.2, k, omega, d.mu, d.eps)
+        x = np.linalg.solve(Z, p["b"].astype(complex))
+        Zo.append(d.V0 / (x[p["patchEdge"] - 1] - x[p["groundEdge"] - 1]))
+    Zo = np.array(Zo)
+    assert (np.abs(Zin - Zo) / np.abs(Zo)).max() <= 1e-6
+    ref_mex = pytest.importorskip("ref_mex")
+    Zr, Sr = ref_mex.patch_sweep_cuda(p, d.freqs)
+    assert (np.abs(Zin - Zr) / np.abs(Zr)).max() <= 1e-6
+
+
+def test_plan_reuse_and_currents():
+    m = pkg()
+    d = small_design("grid")
+    p = eo.build_problem(d)
+    r = p["rwg"]
+    plan = m.SweepPlan(p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"],
+                       r["rp"], r["rm"], r["Ap"], r["Am"], r["len"], p["prepack"], d.mu, d.eps, p["patchEdge"],
+                       p["groundEdge"], d.V0, p["spread"], d.Z0)
+    a = plan.run(d.freqs, return_currents=True)
+    b = plan.run(d.freqs, return_currents=True)
+    assert np.array_equal(a[0], b[0])
+    omega, k, _, _ = eo.physics(d.freqs[0], d.mu, d.eps)
+    Z = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
+    x = a[2][:, 0]
+    assert np.linalg.norm(p["b"] - Z @ x) / np.linalg.norm(p["b"]) < 1e-9
+    plan.close()
