@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Frequency-sweep throughput of the EFIE hot path on B200.
+
+One step = one pass of the hot path (assemble Z, solve Z I = V, Zin/S11) over
+a batch of frequency points of the workload; value = frequency points solved
+per second over all ranks.  Multi-GPU runs are independent replicas (each
+rank sweeps its own frequency points; no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg2] [--batch B] [--solver mixed|fp64]
+
+The reference arm (--impl reference) times the reference's CPU path --
+CPU_FAST assembly + backslash + Zin, restated in the oracle (C, OpenMP, all
+host cores) with LAPACK from numpy -- on the same workload, one frequency
+point per step; it also times the reference's own CUDA sweep (compiled from
+its sources, oracle/_ref) on a bounded sample as ``ref_gpu``.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = "matlab-cuda-efief-vs-cpu_b200"
+METRIC = "freq points/s (assemble+LU+solve) mixed vs FP64 on B200 at rel Zin err ≤1e-6"
+
+MU0 = 4.0 * math.pi * 1e-7
+C0 = 299792458.0
+EPS0 = 1.0 / (MU0 * C0 * C0)
+
+# Workloads (synthetic geometry with the documented shapes; free space).
+WORKLOADS = {
+    # patch 38x30 mm on a 32x24 grid, 1.6 mm above a 60x60 mm ground on a 40x40 grid
+    "cfg2": dict(Lp=30e-3, Wp=38e-3, Lg=60e-3, Wg=60e-3, h=1.6e-3, Np=(32, 24), Ng=(40, 40),
+                 freqs=(2.0e9, 3.0e9, 101)),
+    # same plates, patch 12x10 grid, ground 16x16 grid
+    "cfg1": dict(Lp=30e-3, Wp=38e-3, Lg=60e-3, Wg=60e-3, h=1.6e-3, Np=(12, 10), Ng=(16, 16),
+                 freqs=(2.0e9, 3.0e9, 11)),
+}
+# The reference's GPU option set (main_patch_gpu_mex_sweep_l.m:50-56).
+OPTS_REF_GPU = dict(quad_order=2, near_sing_eps=1.2, self_subdiv=2, self_alpha=0.20, near_subdiv=1,
+                    near_alpha=0.15, near_order=2)
+
+
+def _pkg():
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    return importlib.import_module(PKG)
+
+
+def build_inputs(m, wl):
+    """Mesh, RWG, ports, prepack and sweep arguments through the product's producers."""
+    w = WORKLOADS[wl]
+    V, F, _, _ = m.make_patch_with_ground_mesh(w["Lp"], w["Wp"], w["Lg"], w["Wg"], w["h"], w["Np"][0], w["Np"][1],
+                                               w["Ng"][0], w["Ng"][1], vertex_order="grid")
+    rwg = m.build_rwg_interior({"V": V, "F": F})
+    pe = m.pick_port_edge_by_point_and_layer(rwg, (0.0, -7e-3, +w["h"] / 2), +1)
+    ge = m.pick_port_edge_by_point_and_layer(rwg, (0.0, -7e-3, -w["h"] / 2), -1)
+    pre = m.efie_precompute_pack({"V": V, "F": F}, OPTS_REF_GPU)
+    spread = 1.5 * float(np.mean(rwg["len"]))
+    a, b, n = w["freqs"]
+    freqs = np.linspace(a, b, n)
+    args = [V, F, rwg["edge"], rwg["plusTri"], rwg["minusTri"], rwg["plusSign"], rwg["minusSign"], rwg["rp"],
+            rwg["rm"], rwg["Ap"], rwg["Am"], rwg["len"], pre]
+    tail = [MU0, EPS0, pe, ge, 1.0, spread, 50.0]
+    return dict(V=V, F=F, rwg=rwg, pe=pe, ge=ge, pre=pre, spread=spread, freqs=freqs, args=args, tail=tail,
+                Ne=rwg["Ne"], Nt=F.shape[0])
+
+
+def _nbytes(objs):
+    tot = 0
+    for o in objs:
+        if isinstance(o, dict):
+            tot += _nbytes(list(o.values()))
+        elif isinstance(o, np.ndarray):
+            tot += o.nbytes
+        else:
+            tot += 8
+    return tot
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def _traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def roofline(classes):
+    """Roofline entry for the dominant kernel class (largest device time)."""
+    peaks, src = _peaks()
+    cand = {k: v for k, v in classes.items() if v["launches"] > 0 and v["ms"] > 0 and k != "other"}
+    if not cand:
+        return None
+    name = max(cand, key=lambda k: cand[k]["ms"])
+    c = cand[name]
+    per_launch_ms = c["ms"] / c["launches"]
+    per_launch_work = c["work"] / c["launches"]
+    tr = _traffic().get(name)
+    if name == "gemm":
+        achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e12
+        peak = peaks["bf16_tflops_sustained"]
+        out = dict(bound="tensor", unit="TFLOP/s", peak_source=src + " bf16 sustained")
+    elif name in ("quad", "nearself"):
+        # FP64 point-pair evaluations; reported against HBM only for the schema -- see DESIGN.md
+        achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e9
+        peak = None
+        out = dict(bound="fp64", unit="Gpair/s", peak_source="none")
+    else:
+        achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e9
+        peak = peaks["hbm_gbs"]
+        out = dict(bound="hbm", unit="GB/s", peak_source=src)
+    out.update(kernel=name, achieved=achieved, peak=peak, frac=(achieved / peak) if peak else None,
+               traffic=tr, launches=c["launches"], ms_per_launch=per_launch_ms)
+    return out
+
+
+def cpu_baseline_sample(inp, n_points=1):
+    """Oracle port of the reference CPU path on all host cores, one frequency point."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_c  # noqa: E402  (CPU-baseline leg only)
+    oracle_c.build()
+    rwg = dict(inp["rwg"])
+    pre = inp["pre"]
+    cores = os.cpu_count() or 1
+    b = None
+    t0 = time.perf_counter()
+    for f in inp["freqs"][:n_points]:
+        omega = 2 * math.pi * f
+        k = omega * np.sqrt(MU0 * EPS0 + 0j)
+        Z = oracle_c.assemble_z(rwg, pre, k, omega, MU0, EPS0, nthreads=cores)
+        if b is None:
+            m = _pkg()
+            # RHS is O(Ne): reuse the product's host RHS through a tiny ggassemble-free path
+            b = _rhs(inp)
+        x = np.linalg.solve(Z, b)
+        _ = np.sum(x)
+    dt = time.perf_counter() - t0
+    return n_points / dt, cores, dt
+
+
+def _rhs(inp):
+    V = inp["V"]
+    E = inp["rwg"]["edge"].astype(np.int64) - 1
+    c = 0.5 * (V[E[:, 0]] + V[E[:, 1]])
+    zmid = 0.5 * (c[:, 2].min() + c[:, 2].max())
+    lay = np.where(c[:, 2] > zmid, 1, -1)
+
+    def w(e0):
+        d = np.sqrt(((c - c[e0]) ** 2).sum(1))
+        v = np.exp(-(d / inp["spread"]) ** 2) * (lay == lay[e0])
+        return v / v.sum()
+    return (0.5 * w(inp["pe"] - 1) - 0.5 * w(inp["ge"] - 1)).astype(np.complex128)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    m = _pkg()
+    inp = build_inputs(m, args.workload)
+    cores = os.cpu_count() or 1
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline_sample(inp, 1)
+    times = []
+    for _ in range(args.steps):
+        v, cores, dt = cpu_baseline_sample(inp, 1)
+        times.append(dt)
+    value = args.steps / sum(times)
+    line = dict(metric=METRIC, value=value, unit="freq points/s", impl="reference", n_gpus=args.gpus,
+                steps=args.steps, warmup=min(args.warmup, 1), ms_per_step=1e3 * sum(times) / args.steps,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="c128", data="synthetic",
+                config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=1,
+                            scheme="reference cached subdivision + softening (GPU option set)"),
+                cpu_baseline=dict(value=value, unit="freq points/s", cores=cores, kind="port",
+                                  sample="1 frequency point of %s per step: C restatement of CPU_FAST "
+                                         "(OpenMP, %d threads) + numpy LAPACK solve" % (args.workload, cores)),
+                e2e=dict(value=value, unit="freq points/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    # the reference's own CUDA sweep (compiled from its sources) on a bounded sample
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref_mex  # noqa: E402
+        import torch
+        if torch.cuda.is_available():
+            n = max(2, min(args.batch, 4))
+            fr = inp["freqs"][:n]
+            r = inp["rwg"]
+            mex = ref_mex.RefMex("patch_sweep_fastquad_ref")
+            call = lambda ff: mex.call(2, inp["V"], inp["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"],
+                                       r["minusSign"], r["rp"], r["rm"], r["Ap"], r["Am"], r["len"], inp["pre"],
+                                       np.asarray(ff, np.float64), MU0, complex(EPS0), float(inp["pe"]),
+                                       float(inp["ge"]), 1.0, inp["spread"], 50.0)
+            call(fr[:1])
+            t0 = time.perf_counter()
+            call(fr)
+            dt = time.perf_counter() - t0
+            line["ref_gpu"] = dict(value=n / dt, unit="freq points/s",
+                                   sample="%d frequency points through the reference patch_sweep_fastquad_cuda "
+                                          "(compiled for sm_100a against a fake mex shim)" % n)
+    except Exception as e:  # noqa: BLE001
+        line["ref_gpu"] = dict(unavailable=str(e)[:200])
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    m = _pkg()
+    nat = importlib.import_module(PKG + "._native")
+    nat.context(local)
+    stream = torch.cuda.current_stream()
+    nat.check(nat.lib().efie_ctx_set_stream(nat.context(local), stream.cuda_stream))
+    inp = build_inputs(m, args.workload)
+    freqs = inp["freqs"]
+    B = args.batch or len(freqs)
+    opts = m.sweep_opts(solver=args.solver, timing=True)
+    plan = m.SweepPlan(*inp["args"], *inp["tail"], opts=opts)
+
+    def batch(step):
+        # each rank sweeps its own frequency points (replicas)
+        i0 = ((step * world + rank) * B) % len(freqs)
+        idx = (np.arange(B) + i0) % len(freqs)
+        return freqs[idx]
+
+    for s in range(args.warmup):
+        plan.run(batch(s))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    classes = {k: dict(launches=0, ms=0.0, work=0.0) for k in nat.KERNEL_CLASSES}
+    launches = 0
+    fallback = 0
+    relres = 0.0
+    iters = 0
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for s in range(args.steps):
+            plan.run(batch(args.warmup + s))
+            st = plan.stats
+            launches += st["n_launches"]
+            fallback += st["n_fp64_fallback"]
+            relres = max(relres, st["max_relres"])
+            iters = max(iters, st["refine_iters_max"])
+            for k, v in st["classes"].items():
+                for f in ("launches", "ms", "work"):
+                    classes[k][f] += v[f]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_points = args.steps * B * world
+    value = total_points / (ms * 1e-3)
+    plan.close()
+
+    # e2e: the public API call with host arrays (upload + sweep + results) per step
+    e2e_ms = []
+    h2d = _nbytes(inp["args"]) + B * 8
+    for s in range(max(1, args.steps)):
+        fr = batch(args.warmup + s)
+        t0 = time.perf_counter()
+        m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver))
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    e2e_value = (max(1, args.steps) * B * world) / (e2e * 1e-3)
+
+    line = None
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit="freq points/s", n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=ms / args.steps, higher_is_better=True, scaling="weak",
+                    vs_baseline=None, dtype="c128 (assembly, residual) / c64 (LU)" if args.solver == "mixed"
+                    else "c128", data="synthetic",
+                    config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=B,
+                                solver=args.solver, parallelism="replicas x%d" % world,
+                                scheme="reference cached subdivision + softening (GPU option set)",
+                                l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
+                    e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
+                             d2h_bytes_per_step=2 * 16 * B),
+                    gpu_launches=launches, clocks=clk.summary(),
+                    accuracy=dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback),
+                    roofline=roofline(classes),
+                    phases_ms_per_point={k: v["ms"] / (args.steps * B) for k, v in classes.items()})
+        if world == 1 and not args.no_cpu_baseline:
+            v, cores, dt = cpu_baseline_sample(inp, 1)
+            line["cpu_baseline"] = dict(value=v, unit="freq points/s", cores=cores, kind="port",
+                                        sample="1 frequency point of %s: C restatement of CPU_FAST (OpenMP, %d "
+                                               "threads) + numpy LAPACK solve, %.1f s" % (args.workload, cores, dt))
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="cfg2")
+    ap.add_argument("--batch", type=int, default=0, help="frequency points per step (0 = the whole sweep)")
+    ap.add_argument("--solver", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -161,6 +161,19 @@ typedef struct efie_sweep_opts {
 /* Fill `o` with the defaults listed above. */
 void efie_sweep_opts_default(efie_sweep_opts *o);
 
+/* Kernel classes of the per-launch accounting in efie_sweep_stats. */
+typedef enum efie_kernel_class {
+    EFIE_K_QUAD = 0,      /* regular-pair quadrature (work: point-pair evaluations) */
+    EFIE_K_NEARSELF = 1,  /* near / self / singular pairs (work: point-pair evaluations) */
+    EFIE_K_GATHER = 2,    /* moments -> Z entries (work: bytes of Z written) */
+    EFIE_K_GEMM = 3,      /* LU trailing update (work: algorithmic real flops, 8 m n k) */
+    EFIE_K_PANEL = 4,     /* LU diagonal blocks, panels, format conversion */
+    EFIE_K_TRSV = 5,      /* triangular solves (work: bytes of L/U read) */
+    EFIE_K_RESIDUAL = 6,  /* FP64 residual r = V - Z x (work: bytes of Z read) */
+    EFIE_K_OTHER = 7,     /* port reduction, fills, complex128 LU of the FP64 path */
+    EFIE_NUM_KERNEL_CLASSES = 8
+} efie_kernel_class;
+
 typedef struct efie_sweep_stats {
     int32_t n_freq;
     int32_t refine_iters_max;   /* worst-case refinement iterations over the sweep */
@@ -169,12 +182,10 @@ typedef struct efie_sweep_stats {
     double ms_assemble;         /* summed device time per phase (timing = 1)       */
     double ms_factor;
     double ms_solve;            /* triangular solves + residuals + reduction       */
-    int32_t n_gemm_launches;    /* tensor-core trailing-update launches            */
-    double ms_gemm;             /* summed device time of those launches            */
-    double gemm_flop;           /* their algorithmic real flops (8 m n k each)     */
-    int32_t n_qpe_launches;     /* regular-pair quadrature launches                */
-    double ms_qpe;
-    double qpe_count;           /* point-pair evaluations in those launches        */
+    int32_t n_launches;         /* kernels this library launched (always counted)  */
+    int32_t class_launches[EFIE_NUM_KERNEL_CLASSES];
+    double class_ms[EFIE_NUM_KERNEL_CLASSES];   /* summed CUDA-event time (timing = 1) */
+    double class_work[EFIE_NUM_KERNEL_CLASSES]; /* summed algorithmic work, units above */
 } efie_sweep_stats;
 
 /* Replaces patch_sweep_fastquad_cuda.cu:461-844 (mexFunction):
@@ -263,6 +274,20 @@ typedef struct efie_precompute_opts {
  * and caller-allocated arrays of those sizes. */
 efie_status efie_precompute_pack(int32_t Nv, const double *V, int32_t Nt, const int32_t *F,
                                  const efie_precompute_opts *opts, efie_prepack *out);
+
+/* ---------------------------------------------------------------------- */
+/* Self-tests                                                              */
+/* ---------------------------------------------------------------------- */
+
+/* Factors the column-major complex128 matrix A [N x N] with the complex64
+ * LU of EFIE_SOLVER_MIXED (no pivoting) and returns L (unit lower, below the
+ * diagonal) and U (on and above it) packed in LU [N x N], column-major.
+ * tensor_cores = 0 forces the CUDA-core trailing update.  No counterpart in
+ * the reference (it calls cusolverDnZgetrf). */
+efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores, efie_c128 *LU);
+
+/* 1 disables the tensor-core trailing update process-wide (CUDA-core path). */
+void efie_debug_disable_tensor_cores(int disable);
 
 #ifdef __cplusplus
 }

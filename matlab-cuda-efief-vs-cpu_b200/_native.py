@@ -8,6 +8,7 @@ from __future__ import annotations
 import atexit
 import ctypes as C
 import os
+import weakref
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libefie_b200.so")
@@ -45,15 +46,21 @@ class EfieSweepOpts(C.Structure):
                 ("lu_nb", C.c_int32), ("timing", C.c_int32)]
 
 
+KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
+
+
 class EfieSweepStats(C.Structure):
     _fields_ = [("n_freq", C.c_int32), ("refine_iters_max", C.c_int32),
                 ("n_fp64_fallback", C.c_int32), ("max_relres", C.c_double),
                 ("ms_assemble", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
-                ("n_gemm_launches", C.c_int32), ("ms_gemm", C.c_double), ("gemm_flop", C.c_double),
-                ("n_qpe_launches", C.c_int32), ("ms_qpe", C.c_double), ("qpe_count", C.c_double)]
+                ("n_launches", C.c_int32),
+                ("class_launches", C.c_int32 * 8), ("class_ms", C.c_double * 8), ("class_work", C.c_double * 8)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("class_")}
+        d["classes"] = {name: dict(launches=self.class_launches[i], ms=self.class_ms[i], work=self.class_work[i])
+                        for i, name in enumerate(KERNEL_CLASSES)}
+        return d
 
 
 class EfiePrecomputeOpts(C.Structure):
@@ -102,6 +109,8 @@ SIGNATURES = {
     "efie_quad_rule_size": (C.c_int32, [C.c_int32]),
     "efie_precompute_pack": (C.c_int, [C.c_int32, c_double_p, C.c_int32, c_int32_p,
                                        C.POINTER(EfiePrecomputeOpts), C.POINTER(EfiePrepack)]),
+    "efie_lu_selftest": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P]),
+    "efie_debug_disable_tensor_cores": (None, [C.c_int]),
 }
 
 _lib = None
@@ -139,6 +148,7 @@ def check(status):
 
 
 _ctx = None
+_plans = weakref.WeakSet()   # live plans: destroyed before their context
 
 
 def context(device=0):
@@ -152,8 +162,14 @@ def context(device=0):
     return _ctx
 
 
+def register_plan(plan):
+    _plans.add(plan)
+
+
 def _destroy_ctx():
     global _ctx
+    for p in list(_plans):
+        p.close()
     if _ctx is not None and _lib is not None:
         _lib.efie_ctx_destroy(_ctx)
     _ctx = None

@@ -394,6 +394,7 @@ class SweepPlan:
             float(_scalar(mu)), _cscalar(eps), int(_scalar(pe)), int(_scalar(ge)), float(_scalar(V0)),
             float(_scalar(spread)), float(_scalar(Z0)), C.byref(self.opts), int(rule_order), C.byref(h)))
         self._h = h
+        nat.register_plan(self)
 
     def run(self, freqs, return_currents=False):
         fr = _f64(freqs)

@@ -480,20 +480,18 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     return EFIE_OK;
 }
 
-efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z, efie_sweep_stats *st,
-                                 bool timing) {
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z) {
     cudaStream_t s = ctx->stream;
+    KernelLog &log = ctx->log;
     const int Nt = g.Nt, Ne = g.Ne;
     double *mom = g.moments.as<double>();
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (timing) {
-        EFIE_CUDA(cudaEventCreate(&e0));
-        EFIE_CUDA(cudaEventCreate(&e1));
-        EFIE_CUDA(cudaEventRecord(e0, s));
-    }
     dim3 grid((Nt + 31) / 32, (Nt + 7) / 8);
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
+    // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
+    const double all = g.symmetric ? 0.5 * (double)Nt * (Nt + 1) : (double)Nt * Nt;
+    const double n_regular = all - (double)g.n_near - (double)Nt;
+    size_t tok = log.begin(s);
     switch (g.Nq) {
     case 1: k_regular_moments<1><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
     case 3: k_regular_moments<3><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
@@ -503,39 +501,34 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
         k_regular_moments_any<<<grid, 256, 0, s>>>(Nt, g.Nq, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom);
     }
     EFIE_CUDA(cudaGetLastError());
-    if (timing) EFIE_CUDA(cudaEventRecord(e1, s));
+    log.end(EFIE_K_QUAD, s, tok, n_regular * (double)g.Nq * g.Nq);
+    tok = log.begin(s);
+    int nl = 0;
+    double qpe = 0;
     if (g.n_near > 0) {
         const int P = g.NsN * g.Nq2;
         k_near_moments<<<(g.n_near + 7) / 8, 256, 0, s>>>(Nt, g.symmetric, g.n_near, g.near_list.as<int2>(), P, org,
                                                         g.near_pts.as<double4>(), g.aeq.as<double>(), g.near_alpha,
                                                         ph.kr, ph.ki, mom);
         EFIE_CUDA(cudaGetLastError());
+        nl++;
+        qpe += (double)g.n_near * P * P;
     }
     {
         const int P = g.NsS * g.Nq2;
         k_self_moments<<<(Nt + 7) / 8, 256, 0, s>>>(Nt, g.symmetric, P, g.Nq2, g.self_pts.as<double4>(),
                                                    g.self_a.as<double>(), g.NsS, ph.kr, ph.ki, mom);
         EFIE_CUDA(cudaGetLastError());
+        nl++;
+        qpe += (double)Nt * P * P;
     }
+    log.end(EFIE_K_NEARSELF, s, tok, qpe, nl);
+    tok = log.begin(s);
     dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
     k_gather_z<<<gg, 256, 0, s>>>(Ne, Nt, g.symmetric, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr,
                                   ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
     EFIE_CUDA(cudaGetLastError());
-    if (timing) {
-        float ms = 0.f;
-        EFIE_CUDA(cudaEventSynchronize(e1));
-        EFIE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (st) {
-            st->n_qpe_launches += 1;
-            st->ms_qpe += ms;
-            // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
-            const double all = g.symmetric ? 0.5 * (double)Nt * (Nt + 1) : (double)Nt * Nt;
-            const double regular = all - (double)g.n_near - (double)Nt;
-            st->qpe_count += regular * (double)g.Nq * g.Nq;
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-    }
+    log.end(EFIE_K_GATHER, s, tok, 16.0 * (double)Ne * Ne);
     return EFIE_OK;
 }
 
@@ -598,8 +591,10 @@ efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, 
     double *d_asoft = reinterpret_cast<double *>(base + ((side_bytes + 255) / 256) * 256);
     EFIE_CUDA(cudaMemcpyAsync(d_asoft, asoft.data(), sizeof(double) * Nt, cudaMemcpyHostToDevice, ctx->stream));
     dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
+    size_t tok = ctx->log.begin(ctx->stream);
     k_centroid_z<<<gg, 256, 0, ctx->stream>>>(Ne, reinterpret_cast<const Side *>(base), d_asoft, ph.kr, ph.ki, ph.alr,
                                               ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
     EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_QUAD, ctx->stream, tok, 4.0 * (double)Ne * Ne);
     return EFIE_OK;
 }

@@ -256,7 +256,7 @@ extern "C" efie_status efie_ggassemble_zv(efie_ctx *ctx, const efie_mesh *mesh, 
     EFIE_TRY(efie_geom_upload(ctx, mesh, pre, EFIE_SCHEME_REF, 0, g));
     DevBuf dZ;
     EFIE_TRY(dZ.reserve(sizeof(efie_c128) * (size_t)Ne * Ne));
-    EFIE_TRY(efie_assemble_device(ctx, g, ph, dZ.p, nullptr, false));
+    EFIE_TRY(efie_assemble_device(ctx, g, ph, dZ.p));
     EFIE_CUDA(cudaMemcpyAsync(Z, dZ.p, sizeof(efie_c128) * (size_t)Ne * Ne, cudaMemcpyDeviceToHost, ctx->stream));
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     for (int e = 0; e < Ne; e++) Vrhs[e] = efie_c128{rhs[e], 0.0};
@@ -412,10 +412,14 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                                      efie_c128 *I, efie_sweep_stats *st) {
     if (!p) return efie_fail(EFIE_ERR_ARGS, "null plan");
     if (Nf < 0 || (Nf > 0 && (!freqs || !Zin || !S11))) return efie_fail(EFIE_ERR_FREQS, "freqs must be double vector.");
+    for (int fi = 0; fi < Nf; fi++)
+        if (!(freqs[fi] > 0.0) || !std::isfinite(freqs[fi]))
+            return efie_fail(EFIE_ERR_FREQS, "frequencies must be positive and finite.");
     efie_ctx *ctx = p->ctx;
     DeviceGuard dg(ctx->device);
     const int N = p->Ne;
-    const bool timing = p->opts.timing != 0;
+    KernelLog &log = ctx->log;
+    log.reset(p->opts.timing != 0);
     efie_sweep_stats local{};
     efie_sweep_stats *S = st ? st : &local;
     std::memset(S, 0, sizeof(*S));
@@ -423,32 +427,17 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     EFIE_TRY(p->out.reserve(sizeof(efie_c128) * 2 * std::max(Nf, 1)));
     EFIE_TRY(p->info.reserve(sizeof(int) * std::max(Nf, 1)));
     EFIE_CUDA(cudaMemsetAsync(p->info.p, 0, sizeof(int) * std::max(Nf, 1), ctx->stream));
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    if (timing)
-        for (auto &e : ev) EFIE_CUDA(cudaEventCreate(&e));
-    auto elapsed = [&](cudaEvent_t a, cudaEvent_t b) -> double {
-        float ms = 0.f;
-        cudaEventSynchronize(b);
-        cudaEventElapsedTime(&ms, a, b);
-        return ms;
-    };
+    double ms_fp64 = 0.0;
     efie_status rc = EFIE_OK;
     for (int fi = 0; fi < Nf && rc == EFIE_OK; fi++) {
-        if (!(freqs[fi] > 0.0) || !std::isfinite(freqs[fi])) {
-            rc = efie_fail(EFIE_ERR_FREQS, "frequencies must be positive and finite.");
-            break;
-        }
         const Physics ph = efie_physics(freqs[fi], p->mu, p->eps);
-        if (timing) cudaEventRecord(ev[0], ctx->stream);
         if (p->centroid) rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph, p->Z.p, p->scratch);
-        else rc = efie_assemble_device(ctx, p->g, ph, p->Z.p, S, timing);
+        else rc = efie_assemble_device(ctx, p->g, ph, p->Z.p);
         if (rc != EFIE_OK) break;
-        if (timing) cudaEventRecord(ev[1], ctx->stream);
         bool use_fp64 = p->opts.solver == EFIE_SOLVER_FP64;
         if (!use_fp64) {
-            rc = efie_mixed_factor(ctx, p->sw, p->Z.p, S, timing);
+            rc = efie_mixed_factor(ctx, p->sw, p->Z.p);
             if (rc != EFIE_OK) break;
-            if (timing) cudaEventRecord(ev[2], ctx->stream);
             int iters = 0;
             double rel = 0;
             bool conv = false;
@@ -458,12 +447,6 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             int err = 0;
             rc = efie_mixed_error_flag(ctx, p->sw, &err);
             if (rc != EFIE_OK) break;
-            if (timing) {
-                cudaEventRecord(ev[3], ctx->stream);
-                S->ms_assemble += elapsed(ev[0], ev[1]);
-                S->ms_factor += elapsed(ev[1], ev[2]);
-                S->ms_solve += elapsed(ev[2], ev[3]);
-            }
             S->refine_iters_max = std::max(S->refine_iters_max, iters);
             if (!conv || err) {
                 // zero pivot or stalled refinement: complex128 LU for this frequency
@@ -474,14 +457,11 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             }
         }
         if (use_fp64) {
-            if (timing) cudaEventRecord(ev[2], ctx->stream);
+            // cuSOLVER Zgetrf/Zgetrs: timed in class OTHER, not counted as our launches
+            size_t tok = log.begin(ctx->stream);
             rc = plan_solve_fp64(p, fi, nullptr);
             if (rc != EFIE_OK) break;
-            if (timing && p->opts.solver == EFIE_SOLVER_FP64) {
-                cudaEventRecord(ev[3], ctx->stream);
-                S->ms_assemble += elapsed(ev[0], ev[1]);
-                S->ms_factor += elapsed(ev[2], ev[3]);
-            }
+            log.end(EFIE_K_OTHER, ctx->stream, tok, 8.0 / 3.0 * (double)N * N * N, 0);
         }
         rc = efie_port_reduce(ctx, N, p->x.p, p->wport.as<double>(), p->centroid ? EFIE_PORT_EDGE_DIFF : p->opts.port_model,
                               p->pe - 1, p->ge - 1, p->V0, p->Z0, p->out.as<efie_c128>() + 2 * fi);
@@ -492,6 +472,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
         }
     }
+    (void)ms_fp64;
     if (rc == EFIE_OK && Nf > 0) {
         std::vector<efie_c128> res(2 * (size_t)Nf);
         std::vector<int> info(Nf);
@@ -516,9 +497,16 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     } else {
         cudaStreamSynchronize(ctx->stream);
     }
-    if (timing)
-        for (auto &e : ev)
-            if (e) cudaEventDestroy(e);
+    log.resolve();
+    for (int c = 0; c < EFIE_NUM_KERNEL_CLASSES; c++) {
+        S->class_launches[c] = log.launches[c];
+        S->class_ms[c] = log.ms[c];
+        S->class_work[c] = log.work[c];
+        S->n_launches += log.launches[c];
+    }
+    S->ms_assemble = log.ms[EFIE_K_QUAD] + log.ms[EFIE_K_NEARSELF] + log.ms[EFIE_K_GATHER];
+    S->ms_factor = log.ms[EFIE_K_PANEL] + log.ms[EFIE_K_GEMM];
+    S->ms_solve = log.ms[EFIE_K_TRSV] + log.ms[EFIE_K_RESIDUAL] + log.ms[EFIE_K_OTHER];
     return rc;
 }
 
@@ -578,4 +566,35 @@ extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh 
     }
     efie_plan_destroy(p);
     return s;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test of the complex64 LU (no pivoting) used by the mixed solver.
+// ---------------------------------------------------------------------------
+extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores,
+                                        efie_c128 *LU) {
+    if (!ctx || N < 1 || !A || !LU) return efie_fail(EFIE_ERR_ARGS, "efie_lu_selftest: bad arguments");
+    DeviceGuard dg(ctx->device);
+    ctx->log.reset(false);
+    SolveWork w;
+    EFIE_TRY(efie_mixed_workspace(w, N));
+    DevBuf dA;
+    EFIE_TRY(dA.reserve(sizeof(efie_c128) * (size_t)N * N));
+    EFIE_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(efie_c128) * (size_t)N * N, cudaMemcpyHostToDevice, ctx->stream));
+    efie_debug_disable_tensor_cores(tensor_cores ? 0 : 1);
+    efie_status s = efie_mixed_factor(ctx, w, dA.p);
+    efie_debug_disable_tensor_cores(0);
+    EFIE_TRY(s);
+    std::vector<float> pl(2 * (size_t)w.ld * N);
+    EFIE_CUDA(cudaMemcpyAsync(pl.data(), w.planes.p, sizeof(float) * pl.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    int err = 0;
+    EFIE_CUDA(cudaMemcpyAsync(&err, w.ctl.as<char>() + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
+    const float *Ar = pl.data(), *Ai = Ar + (size_t)w.ld * N;
+    for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++)
+            LU[(size_t)i + (size_t)N * j] = efie_c128{Ar[(size_t)i * w.ld + j], Ai[(size_t)i * w.ld + j]};
+    ctx->log.resolve();
+    if (err) return efie_fail(err == 1 ? EFIE_ERR_SINGULAR : EFIE_ERR_TIMEOUT, "LU self-test: device error flag " + std::to_string(err));
+    return EFIE_OK;
 }

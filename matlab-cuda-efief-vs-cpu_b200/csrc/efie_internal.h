@@ -56,6 +56,63 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+#include <vector>
+
+// Per-launch accounting: every launch is counted per kernel class; with
+// timing on, a pair of CUDA events brackets it on the launching stream and
+// the durations are resolved once, after the sweep's final synchronisation.
+struct KernelLog {
+    bool timing = false;
+    int launches[EFIE_NUM_KERNEL_CLASSES] = {0};
+    double work[EFIE_NUM_KERNEL_CLASSES] = {0};
+    double ms[EFIE_NUM_KERNEL_CLASSES] = {0};
+    struct Ent { int cls; size_t a, b; };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Ent> ents;
+    size_t used = 0;
+    cudaEvent_t next() {
+        if (used == pool.size()) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+    // Call before a launch; returns a token for end().
+    size_t begin(cudaStream_t s) {
+        if (!timing) return 0;
+        size_t i = used;
+        cudaEventRecord(next(), s);
+        return i;
+    }
+    void end(int cls, cudaStream_t s, size_t tok, double w, int nlaunch = 1) {
+        launches[cls] += nlaunch;
+        work[cls] += w;
+        if (!timing) return;
+        size_t i = used;
+        cudaEventRecord(next(), s);
+        ents.push_back(Ent{cls, tok, i});
+    }
+    void reset(bool t) {
+        timing = t;
+        for (int c = 0; c < EFIE_NUM_KERNEL_CLASSES; c++) launches[c] = 0, work[c] = 0, ms[c] = 0;
+        ents.clear();
+        used = 0;
+    }
+    // After the stream has been synchronised.
+    void resolve() {
+        for (const Ent &e : ents) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, pool[e.a], pool[e.b]) == cudaSuccess) ms[e.cls] += t;
+        }
+        ents.clear();
+        used = 0;
+    }
+    ~KernelLog() {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+};
+
 struct efie_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -64,6 +121,7 @@ struct efie_ctx {
     int num_sms = 0;
     int cc_major = 0;
     DevBuf status;   // device-side error flags of bounded waits (int32[8])
+    KernelLog log;
 };
 
 // Device geometry of one sweep/assembly problem (uploaded once per plan).
@@ -101,8 +159,7 @@ Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
 // assemble.cu
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
                              int rule_order, GeomDev &g);
-efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/,
-                                 efie_sweep_stats *st, bool timing);
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/);
 efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, double selfAlpha,
                                           const Physics &ph, void *Z, DevBuf &scratch);
 #endif

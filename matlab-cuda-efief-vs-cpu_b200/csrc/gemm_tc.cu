@@ -1,8 +1,355 @@
-// Trailing-matrix update of the complex64 LU: A22 -= L21 * U12.
+// Trailing-matrix update of the complex64 LU on the 5th-generation tensor
+// cores: A22 -= L21 * U12.
+//
+// The complex product is realified into one real GEMM per 64-row block:
+//     [ Re ]   [ Lr  -Li ]   [ Ur ]
+//     [ Im ] = [ Li   Lr ] * [ Ui ]        (M' = 128 rows, K' = 2 kb)
+// and every operand is split into two TF32 terms, x = hi + lo with
+// hi = tf32(x), lo = tf32(x - hi); the three products hi*hi + hi*lo + lo*hi
+// accumulate in FP32 in tensor memory (TMEM), which keeps the update close to
+// FP32 accuracy (the LU is then refined in FP64).
+//
+// Operands are packed per LU step into 128B-swizzled K-major tiles that sit
+// contiguously in global memory, so each CTA fetches them with plain bulk
+// copies (cp.async.bulk, the TMA engine; no multicast, local memory only).
+// One CTA computes a 128 x 256 accumulator tile (64 complex rows x 256
+// complex columns): one elected thread issues tcgen05.mma, two shared-memory
+// stages double-buffer the K' chunks, and all four warps drain TMEM with
+// tcgen05.ld for the read-modify-write epilogue on the row-major planes.
+// Every mbarrier wait is bounded; a timeout sets the device error flag.
+#include <cstdint>
+
 #include "solve.h"
 
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, efie_sweep_stats *st, bool timing) {
-    (void)st;
-    (void)timing;
-    return efie_trailing_update_simt(ctx, w, k, kb);
+namespace {
+
+constexpr int NB = 64;           // LU panel width (kb <= NB)
+constexpr int TM = 128;          // accumulator rows (64 complex rows)
+constexpr int TN = 256;          // accumulator columns (complex columns)
+constexpr int KC = 32;           // fp32 elements per 128-byte swizzle row (one K' chunk)
+constexpr int NCHUNK = 2 * NB / KC;   // K' = 2*NB = 128 -> 4 chunks
+constexpr int A_TILE = TM * KC;       // floats per A tile (16 KB)
+constexpr int B_TILE = TN * KC;       // floats per B tile (32 KB)
+constexpr int STAGE_FLOATS = 2 * A_TILE + 2 * B_TILE;   // hi/lo of A and B: 96 KB
+constexpr int NSTAGE = 2;
+constexpr size_t GEMM_SMEM = sizeof(float) * NSTAGE * STAGE_FLOATS + 1024 + 64;
+
+// byte offset of element (row r, k) inside a K-major 128B-swizzled tile
+__host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) {
+    return r * 128u + ((((k >> 2) ^ (r & 7u)) & 7u) << 4) + ((k & 3u) << 2);
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ---------------------------------------------------------------------------
+// Packing.  A: per 64-row block of L21 and K' chunk, a 128 x 32 tile (hi, lo).
+// B: per 256-column block of U12 and K' chunk, a 256 x 32 tile (hi, lo).
+// Tiles are built in shared memory in their final swizzled byte layout and
+// written out with coalesced 16-byte stores.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const float *__restrict__ Ar,
+                                                const float *__restrict__ Ai, int ld, float *__restrict__ out) {
+    __shared__ __align__(1024) float hi[A_TILE];
+    __shared__ __align__(1024) float lo[A_TILE];
+    const int tile = blockIdx.x, chunk = blockIdx.y;
+    const int s = k + kb;
+    for (int e = threadIdx.x; e < A_TILE; e += 256) {
+        const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
+        const int kp = chunk * KC + kq;              // K' index
+        const int kk = kp & 63;                      // column within the panel
+        const bool second = kp >= 64;
+        const int row = s + tile * 64 + (r & 63);
+        float v = 0.f;
+        if (row < N && kk < kb) {
+            const size_t o = (size_t)row * ld + k + kk;
+            if (r < 64) v = second ? -Ai[o] : Ar[o];     // [ Lr  -Li ]
+            else v = second ? Ar[o] : Ai[o];            // [ Li   Lr ]
+        }
+        const float h = tf32_rna(v);
+        const uint32_t off = swz(r, kq) >> 2;
+        hi[off] = h;
+        lo[off] = tf32_rna(v - h);
+    }
+    __syncthreads();
+    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * NCHUNK + chunk) * 2) * A_TILE);
+    const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
+    for (int e = threadIdx.x; e < A_TILE / 4; e += 256) {
+        dst[e] = h4[e];
+        dst[A_TILE / 4 + e] = l4[e];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const float *__restrict__ Ar,
+                                                const float *__restrict__ Ai, int ld, float *__restrict__ out) {
+    extern __shared__ __align__(1024) float dynb[];
+    float *hi = dynb, *lo = dynb + B_TILE;
+    const int tile = blockIdx.x, chunk = blockIdx.y;
+    const int s = k + kb;
+    for (int e = threadIdx.x; e < B_TILE; e += 256) {
+        const int kq = e >> 8, n = e & 255;          // consecutive threads: consecutive columns
+        const int kp = chunk * KC + kq;
+        const int kk = kp & 63;
+        const int col = s + tile * TN + n;
+        float v = 0.f;
+        if (col < N && kk < kb) {
+            const size_t o = (size_t)(k + kk) * ld + col;
+            v = kp >= 64 ? Ai[o] : Ar[o];               // [ Ur ; Ui ]
+        }
+        const float h = tf32_rna(v);
+        const uint32_t off = swz(n, kq) >> 2;
+        hi[off] = h;
+        lo[off] = tf32_rna(v - h);
+    }
+    __syncthreads();
+    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * NCHUNK + chunk) * 2) * B_TILE);
+    const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
+    for (int e = threadIdx.x; e < B_TILE / 4; e += 256) {
+        dst[e] = h4[e];
+        dst[B_TILE / 4 + e] = l4[e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 / mbarrier / bulk-copy primitives (inline PTX)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false (and the error flag set) after ~1 s of polling.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+    for (long long i = 0; i < (1ll << 22); i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    atomicExch(err, 3);
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t desc_sw128(const void *smem_tile) {
+    const uint32_t a = smem_u32(smem_tile);
+    uint64_t d = 0;
+    d |= (uint64_t)((a & 0x3FFFFu) >> 4);      // start address
+    d |= (uint64_t)1 << 16;                    // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                    // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+    return d;
+}
+
+// kind::tf32, D = F32, A = B = TF32, both K-major, N = 256, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                           ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float *__restrict__ Apack,
+                                                      const float *__restrict__ Bpack, float *__restrict__ Ar,
+                                                      float *__restrict__ Ai, int ld, int *__restrict__ err) {
+    extern __shared__ uint8_t dyn_raw[];
+    // 1024-byte alignment for the swizzled tiles
+    float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_FLOATS);  // full[2], empty[2], done
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 5);
+    int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile_n = blockIdx.x, tile_m = blockIdx.y;
+
+    if (tid == 0) {
+        for (int i = 0; i < 5; i++) mbar_init(&bars[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    bool ok = true;
+    if (tid == 0) *ok_sh = 1;
+    if (tid == 0) {
+        const float *ga = Apack + (size_t)tile_m * NCHUNK * 2 * A_TILE;
+        const float *gb = Bpack + (size_t)tile_n * NCHUNK * 2 * B_TILE;
+        const uint32_t bytes = sizeof(float) * (2 * A_TILE + 2 * B_TILE);
+        auto load = [&](int c) {
+            float *st = stage + (c % NSTAGE) * STAGE_FLOATS;
+            mbar_expect_tx(&bars[c % NSTAGE], bytes);
+            bulk_g2s(st, ga + (size_t)c * 2 * A_TILE, sizeof(float) * 2 * A_TILE, &bars[c % NSTAGE]);
+            bulk_g2s(st + 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, sizeof(float) * 2 * B_TILE, &bars[c % NSTAGE]);
+        };
+        load(0);
+        load(1);
+        for (int c = 0; c < NCHUNK && ok; c++) {
+            const int sidx = c % NSTAGE;
+            const uint32_t phase = (c / NSTAGE) & 1;
+            if (!mbar_wait(&bars[sidx], phase, err)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const float *st = stage + sidx * STAGE_FLOATS;
+            const uint64_t ahi = desc_sw128(st), alo = desc_sw128(st + A_TILE);
+            const uint64_t bhi = desc_sw128(st + 2 * A_TILE), blo = desc_sw128(st + 2 * A_TILE + B_TILE);
+#pragma unroll
+            for (int kk = 0; kk < KC / 8; kk++) {
+                const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+                // small terms first, then the leading product
+                mma_tf32(tmem, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
+                mma_tf32(tmem, ahi + adv, blo + adv, 1u);
+                mma_tf32(tmem, ahi + adv, bhi + adv, 1u);
+            }
+            mma_commit(&bars[2 + sidx]);   // stage sidx free once these MMAs have read it
+            if (c + NSTAGE < NCHUNK) {
+                if (!mbar_wait(&bars[2 + sidx], phase, err)) { ok = false; break; }
+                load(c + NSTAGE);
+            }
+        }
+        mma_commit(&bars[4]);              // all MMAs of this tile done
+        if (!ok) *ok_sh = 0;
+    }
+    __syncthreads();
+    // every thread waits for the accumulator (bounded); the decision is made
+    // uniform per warp because tcgen05.ld is a warp-collective instruction
+    bool have = mbar_wait(&bars[4], 0, err);
+    have = __all_sync(0xffffffffu, have) && (*ok_sh != 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (have) {
+        const int half = warp & 1;                  // rows 0-31 or 32-63 of the complex block
+        float *plane = (warp < 2) ? Ar : Ai;        // warps 0,1: real part; 2,3: imaginary part
+        const int row = s + tile_m * 64 + half * 32 + lane;
+        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int j = 0; j < TN / 32; j++) {
+            uint32_t v[32];
+            tmem_ld32(tbase + j * 32, v);
+            const int col0 = s + tile_n * TN + j * 32;
+            if (row < N && col0 < N) {
+                float *p = plane + (size_t)row * ld + col0;
+                if (col0 + 32 <= N) {
+                    float4 *p4 = reinterpret_cast<float4 *>(p);
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        float4 a = p4[q];
+                        a.x -= __uint_as_float(v[4 * q]);
+                        a.y -= __uint_as_float(v[4 * q + 1]);
+                        a.z -= __uint_as_float(v[4 * q + 2]);
+                        a.w -= __uint_as_float(v[4 * q + 3]);
+                        p4[q] = a;
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 32; q++)
+                        if (col0 + q < N) p[q] -= __uint_as_float(v[q]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+    }
+}
+
+}  // namespace
+
+static bool g_tc_disabled = false;
+
+efie_status efie_tc_attrs() {
+    static bool done = false;
+    if (done) return EFIE_OK;
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_pack_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(float) * 2 * B_TILE)));
+    done = true;
+    return EFIE_OK;
+}
+
+// Tensor cores pay off once the trailing matrix spans a few tiles.
+static bool use_tc(int rest) { return !g_tc_disabled && rest >= 256; }
+
+extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
+
+efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb) {
+    const int N = w.N, s = k + kb, rest = N - s;
+    if (!use_tc(rest) || kb > NB) return efie_trailing_update_simt(ctx, w, k, kb);
+    EFIE_TRY(efie_tc_attrs());
+    cudaStream_t st = ctx->stream;
+    const int mt = (rest + 63) / 64, nt = (rest + TN - 1) / TN;
+    EFIE_TRY(w.packA.reserve(sizeof(float) * (size_t)mt * NCHUNK * 2 * A_TILE));
+    EFIE_TRY(w.packB.reserve(sizeof(float) * (size_t)nt * NCHUNK * 2 * B_TILE));
+    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)w.ld * N;
+    int *err = reinterpret_cast<int *>(w.ctl.as<char>() + 64);
+    KernelLog &log = ctx->log;
+    size_t tok = log.begin(st);
+    k_pack_a<<<dim3(mt, NCHUNK), 256, 0, st>>>(N, k, kb, Ar, Ai, w.ld, w.packA.as<float>());
+    k_pack_b<<<dim3(nt, NCHUNK), 256, sizeof(float) * 2 * B_TILE, st>>>(N, k, kb, Ar, Ai, w.ld, w.packB.as<float>());
+    EFIE_CUDA(cudaGetLastError());
+    log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
+    tok = log.begin(st);
+    k_update_tc<<<dim3(nt, mt), 128, GEMM_SMEM, st>>>(N, s, w.packA.as<float>(), w.packB.as<float>(), Ar, Ai, w.ld,
+                                                      err);
+    EFIE_CUDA(cudaGetLastError());
+    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rest * rest * kb);
+    return EFIE_OK;
 }

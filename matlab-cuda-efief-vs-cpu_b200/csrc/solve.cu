@@ -275,109 +275,6 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float
 }
 
 // ---------------------------------------------------------------------------
-// Triangular solves with the factored planes.  Persistent cooperative grid;
-// block row b waits (bounded) for the flags of the blocks it depends on.
-// lower: y = L^-1 r  (unit lower, forward);  upper: d = U^-1 y (backward) and
-// x += d in FP64.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool wait_flag(const volatile int *flag, int epoch, int *err) {
-    long long spins = 0;
-    while (*flag != epoch) {
-        if (++spins > (1ll << 24)) {  // ~ a few hundred ms: give up, record the error
-            atomicExch(err, 2);
-            return false;
-        }
-        if (*((volatile int *)err)) return false;
-        __nanosleep(64);
-    }
-    __threadfence();
-    return true;
-}
-
-template <bool LOWER>
-__global__ void __launch_bounds__(256) k_trsv(int N, int nblk, const float *__restrict__ Ar,
-                                              const float *__restrict__ Ai, int ld, const float2 *__restrict__ dinv,
-                                              const float2 *__restrict__ rhs, float2 *__restrict__ out,
-                                              double2 *__restrict__ x, int *flags, int epoch, int *err,
-                                              const int *__restrict__ skip) {
-    if (skip && *skip) return;  // refinement already converged
-    __shared__ float2 acc[NB];
-    __shared__ float2 yj[NB];
-    __shared__ float2 part[4][NB];
-    __shared__ int ok;
-    const int tid = threadIdx.x;
-    const int row = tid & 63, quarter = tid >> 6;
-    for (int it = blockIdx.x; it < nblk; it += gridDim.x) {
-        const int b = LOWER ? it : nblk - 1 - it;
-        const int r0 = b * NB;
-        const int rows = min(NB, N - r0);
-        if (tid < NB) acc[tid] = (tid < rows) ? rhs[r0 + tid] : make_float2(0.f, 0.f);
-        if (tid == 0) ok = 1;
-        __syncthreads();
-        const int jbeg = LOWER ? 0 : b + 1, jend = LOWER ? b : nblk;
-        for (int jb = jbeg; jb < jend; jb++) {
-            if (tid == 0) {
-                if (!wait_flag(flags + jb, epoch, err)) ok = 0;
-            }
-            __syncthreads();
-            if (!ok) return;
-            const int c0 = jb * NB;
-            const int cols = min(NB, N - c0);
-            // written by another CTA of this grid: read through L2 only
-            if (tid < NB) yj[tid] = (tid < cols) ? __ldcg(out + c0 + tid) : make_float2(0.f, 0.f);
-            __syncthreads();
-            float2 s = make_float2(0.f, 0.f);
-            if (row < rows) {
-                const float *pr = Ar + (size_t)(r0 + row) * ld + c0;
-                const float *pi = Ai + (size_t)(r0 + row) * ld + c0;
-                for (int c = quarter * 16; c < quarter * 16 + 16 && c < cols; c++) {
-                    const float2 l = make_float2(pr[c], pi[c]);
-                    const float2 v = yj[c];
-                    s.x += l.x * v.x - l.y * v.y;
-                    s.y += l.x * v.y + l.y * v.x;
-                }
-            }
-            part[quarter][row] = s;
-            __syncthreads();
-            if (tid < NB) {
-                float2 t = acc[tid];
-                t.x -= part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
-                t.y -= part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
-                acc[tid] = t;
-            }
-            __syncthreads();
-        }
-        // y_b = inv(diag block) * acc
-        const float2 *D = dinv + (size_t)b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
-        float2 s = make_float2(0.f, 0.f);
-        for (int c = quarter * 16; c < quarter * 16 + 16; c++) {
-            const float2 m = D[row * NB + c];
-            const float2 v = acc[c];
-            s.x += m.x * v.x - m.y * v.y;
-            s.y += m.x * v.y + m.y * v.x;
-        }
-        part[quarter][row] = s;
-        __syncthreads();
-        if (tid < rows) {
-            float2 t;
-            t.x = part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
-            t.y = part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
-            out[r0 + tid] = t;
-            if (!LOWER) {
-                double2 xv = x[r0 + tid];
-                xv.x += (double)t.x;
-                xv.y += (double)t.y;
-                x[r0 + tid] = xv;
-            }
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) atomicExch(flags + b, epoch);
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
 // r = V - Z x  (complex128 GEMV over the column-major Z), the complex64 copy
 // of r for the next correction, and ||r||^2.  Block = 32 rows x 8 column
 // groups.  The last CTA turns ||r|| into the convergence flag.
@@ -513,7 +410,11 @@ efie_status efie_mixed_workspace(SolveWork &w, int N) {
     w.N = N;
     w.ld = (N + 63) / 64 * 64;
     w.nblk = (N + NB - 1) / NB;
-    EFIE_TRY(w.planes.reserve(sizeof(float) * 2 * (size_t)w.ld * N));
+    const size_t pbytes = sizeof(float) * 2 * (size_t)w.ld * N;
+    if (pbytes > w.planes.bytes) {
+        EFIE_TRY(w.planes.reserve(pbytes));
+        EFIE_CUDA(cudaMemset(w.planes.p, 0, pbytes));  // padding columns stay zero
+    }
     EFIE_TRY(w.dinv.reserve(sizeof(float2) * 2 * (size_t)NB * NB * w.nblk));
     EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.ld));
     const size_t fbytes = sizeof(int) * 2 * (size_t)w.nblk;
@@ -526,26 +427,32 @@ efie_status efie_mixed_workspace(SolveWork &w, int N) {
     return EFIE_OK;
 }
 
-efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, efie_sweep_stats *st, bool timing) {
+efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z) {
     cudaStream_t s = ctx->stream;
+    KernelLog &log = ctx->log;
     const int N = w.N, ld = w.ld;
     float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)ld * N;
     int *err = reinterpret_cast<int *>(w.ctl.as<char>() + 64);
     EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 256, s));
     dim3 tg((N + 31) / 32, (N + 31) / 32);
+    size_t tok = log.begin(s);
     k_z_to_planes<<<tg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), Ar, Ai, ld);
     EFIE_CUDA(cudaGetLastError());
+    log.end(EFIE_K_PANEL, s, tok, 24.0 * (double)N * N);
     float2 *dinv = w.dinv.as<float2>();
     for (int bi = 0; bi < w.nblk; bi++) {
         const int k = bi * NB, kb = std::min(NB, N - k);
         float2 *Linv = dinv + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
-        k_diag_factor<<<1, 1024, kTwoTiles, s>>>(k, kb, Ar, Ai, ld, Linv, Uinv, err);
         const int rest = N - k - kb;
+        tok = log.begin(s);
+        k_diag_factor<<<1, 1024, kTwoTiles, s>>>(k, kb, Ar, Ai, ld, Linv, Uinv, err);
         if (rest > 0) {
             dim3 pg((rest + NB - 1) / NB, 2);
             k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, Ar, Ai, ld, Linv, Uinv);
-            EFIE_TRY(efie_trailing_update(ctx, w, k, kb, st, timing));
         }
+        EFIE_CUDA(cudaGetLastError());
+        log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
+        if (rest > 0) EFIE_TRY(efie_trailing_update(ctx, w, k, kb));
     }
     EFIE_CUDA(cudaGetLastError());
     return EFIE_OK;
@@ -555,8 +462,10 @@ efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb
     const int N = w.N, rest = N - k - kb;
     float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)w.ld * N;
     dim3 g((rest + NB - 1) / NB, (rest + NB - 1) / NB);
+    size_t tok = ctx->log.begin(ctx->stream);
     k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, k, kb, Ar, Ai, w.ld);
     EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_GEMM, ctx->stream, tok, 8.0 * (double)rest * rest * kb);
     return EFIE_OK;
 }
 
@@ -574,37 +483,39 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const 
     int *err = reinterpret_cast<int *>(ctl + 64);
     int *flagsL = w.flags.as<int>(), *flagsU = flagsL + w.nblk;
     // x = 0, rf = b (complex64), red = {0, ||b||, 1}
+    KernelLog &log = ctx->log;
+    size_t tok = log.begin(s);
     k_fill_c128<<<(N + 255) / 256, 256, 0, s>>>(N, static_cast<double2 *>(x), make_double2(0.0, 0.0));
+    log.end(EFIE_K_OTHER, s, tok, 0.0);
     const double init[3] = {0.0, bnorm, 1.0};
     EFIE_CUDA(cudaMemcpyAsync(red, init, sizeof(init), cudaMemcpyHostToDevice, s));
     EFIE_CUDA(cudaMemsetAsync(ctl + 32, 0, 16, s));
-    int grid = std::min(w.nblk, ctx->num_sms);
     int it = 0;
     bool done = false;
     int hconv = 0;
     // initial residual r = b (x = 0) through the residual kernel keeps one code path
+    const double zbytes = 16.0 * (double)N * N, lubytes = 8.0 * (double)N * N;
+    tok = log.begin(s);
     k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z), static_cast<const double2 *>(x),
                                              static_cast<const double2 *>(b), rf, red, counter, conv, -1.0, skip);
     EFIE_CUDA(cudaGetLastError());
+    log.end(EFIE_K_RESIDUAL, s, tok, zbytes);
     while (!done) {
         const int chunk = std::min(5, max_iter - it);
         if (chunk <= 0) break;
         for (int c = 0; c < chunk; c++) {
             const int epoch = ++w.epoch;
-            void *argsL[] = {(void *)&N, (void *)&w.nblk, (void *)&Ar, (void *)&Ai, (void *)&ld,
-                             (void *)&w.dinv.p, (void *)&rf, (void *)&y, (void *)&x, (void *)&flagsL,
-                             (void *)&epoch, (void *)&err, (void *)&skip};
-            EFIE_CUDA(cudaLaunchCooperativeKernel((const void *)k_trsv<true>, dim3(grid), dim3(256), argsL, 0, s));
-            const float2 *yc = y;
-            void *argsU[] = {(void *)&N, (void *)&w.nblk, (void *)&Ar, (void *)&Ai, (void *)&ld,
-                             (void *)&w.dinv.p, (void *)&yc, (void *)&d, (void *)&x, (void *)&flagsU,
-                             (void *)&epoch, (void *)&err, (void *)&skip};
-            EFIE_CUDA(cudaLaunchCooperativeKernel((const void *)k_trsv<false>, dim3(grid), dim3(256), argsU, 0, s));
+            tok = log.begin(s);
+            EFIE_TRY(efie_trsv(ctx, w, true, rf, y, x, flagsL, epoch, err, skip));
+            EFIE_TRY(efie_trsv(ctx, w, false, y, d, x, flagsU, epoch, err, skip));
+            log.end(EFIE_K_TRSV, s, tok, lubytes, 2);
+            tok = log.begin(s);
             k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z),
                                                      static_cast<const double2 *>(x),
                                                      static_cast<const double2 *>(b), rf, red, counter, conv, tol,
                                                      skip);
             EFIE_CUDA(cudaGetLastError());
+            log.end(EFIE_K_RESIDUAL, s, tok, zbytes);
         }
         it += chunk;
         int hctl[2] = {0, 0};
@@ -626,9 +537,11 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const 
 
 efie_status efie_port_reduce(efie_ctx *ctx, int N, const void *x, const double *wport, int model, int pe, int ge,
                              double V0, double Z0, void *out2) {
+    size_t tok = ctx->log.begin(ctx->stream);
     k_port<<<1, 1024, 0, ctx->stream>>>(N, static_cast<const double2 *>(x), wport, model, pe, ge, V0, Z0,
                                          static_cast<double2 *>(out2));
     EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_OTHER, ctx->stream, tok, 0.0);
     return EFIE_OK;
 }
 

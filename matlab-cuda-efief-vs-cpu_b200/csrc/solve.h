@@ -16,14 +16,17 @@ struct SolveWork {
 
 int efie_solve_nb();
 efie_status efie_mixed_workspace(SolveWork &w, int N);
-efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, efie_sweep_stats *st, bool timing);
+efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z);
 efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const void *b, void *x, double bnorm,
                               double tol, int max_iter, int *iters, double *relres, bool *converged);
+efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int *flags,
+                      int epoch, int *err, const int *skip);
 efie_status efie_mixed_error_flag(efie_ctx *ctx, SolveWork &w, int *flag);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, const void *x, const double *wport, int model, int pe, int ge,
                              double V0, double Z0, void *out2);
 
 // A22 -= L21 * U12 for the block at (k, kb): tensor cores when the trailing
 // matrix is large enough, CUDA cores otherwise.
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, efie_sweep_stats *st, bool timing);
+efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb);
 efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb);
+extern "C" void efie_debug_disable_tensor_cores(int disable);
