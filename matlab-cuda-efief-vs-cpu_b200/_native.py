@@ -43,7 +43,7 @@ class EfiePrepack(C.Structure):
 class EfieSweepOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("port_model", C.c_int32), ("scheme", C.c_int32),
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
-                ("lu_nb", C.c_int32), ("timing", C.c_int32)]
+                ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")

@@ -63,6 +63,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->refine_max_iter = 30;
     o->lu_nb = 0;
     o->timing = 0;
+    o->batch = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -296,6 +297,7 @@ struct efie_plan {
     bool centroid = false;       // patch_sweep_cuda model
     double self_alpha = 0.20;
     int Ne = 0;
+    int B = 1;                   // frequencies per batch
     double mu = 0, V0 = 0, Z0 = 0;
     efie_c128 eps{0, 0};
     int pe = 0, ge = 0;
@@ -312,10 +314,12 @@ struct efie_plan {
 
 namespace {
 
-efie_status plan_solve_fp64(efie_plan *p, int fi, int *info_host) {
+// complex128 LU (cuSOLVER) of Z_f in place and x_f = Z_f^-1 V
+efie_status plan_solve_fp64(efie_plan *p, int slot, int fi) {
     efie_ctx *ctx = p->ctx;
     const int N = p->Ne;
-    cuDoubleComplex *A = p->Z.as<cuDoubleComplex>();
+    cuDoubleComplex *A = p->Z.as<cuDoubleComplex>() + (size_t)N * N * slot;
+    cuDoubleComplex *x = p->x.as<cuDoubleComplex>() + (size_t)N * slot;
     if (p->lwork_elems < 0) {
         int lw = 0;
         if (cusolverDnZgetrf_bufferSize(ctx->solver, N, N, A, N, &lw) != CUSOLVER_STATUS_SUCCESS)
@@ -323,16 +327,27 @@ efie_status plan_solve_fp64(efie_plan *p, int fi, int *info_host) {
         EFIE_TRY(p->lwork.reserve(sizeof(cuDoubleComplex) * (size_t)std::max(lw, 1)));
         p->lwork_elems = lw;
     }
-    EFIE_CUDA(cudaMemcpyAsync(p->x.p, p->b.p, sizeof(cuDoubleComplex) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    EFIE_CUDA(cudaMemcpyAsync(x, p->b.p, sizeof(cuDoubleComplex) * N, cudaMemcpyDeviceToDevice, ctx->stream));
     int *dinfo = p->info.as<int>() + fi;
     if (cusolverDnZgetrf(ctx->solver, N, N, A, N, p->lwork.as<cuDoubleComplex>(), p->ipiv.as<int>(), dinfo) !=
         CUSOLVER_STATUS_SUCCESS)
         return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
-    if (cusolverDnZgetrs(ctx->solver, CUBLAS_OP_N, N, 1, A, N, p->ipiv.as<int>(), p->x.as<cuDoubleComplex>(), N,
-                         dinfo) != CUSOLVER_STATUS_SUCCESS)
+    if (cusolverDnZgetrs(ctx->solver, CUBLAS_OP_N, N, 1, A, N, p->ipiv.as<int>(), x, N, dinfo) !=
+        CUSOLVER_STATUS_SUCCESS)
         return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
-    (void)info_host;
     return EFIE_OK;
+}
+
+// Frequencies per batch: everything a frequency needs on the device (Z in
+// complex128, its complex64 planes, staging) within a fraction of free HBM.
+int choose_batch(int N, int requested, int solver) {
+    if (solver == EFIE_SOLVER_FP64) return 1;
+    if (requested > 0) return std::min(requested, EFIE_MAX_BATCH);
+    size_t freeb = 0, total = 0;
+    if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
+    const double per = 26.0 * (double)N * N + 1e6;
+    int B = (int)std::floor(0.35 * (double)freeb / per);
+    return std::max(1, std::min(B, 8));
 }
 
 efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c128 eps, int pe, int ge, double V0,
@@ -362,14 +377,15 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         bn += rhs[e] * rhs[e];
     }
     p->bnorm = std::sqrt(bn);
-    EFIE_TRY(p->Z.reserve(sizeof(efie_c128) * (size_t)N * N));
+    p->B = choose_batch(N, p->opts.batch, p->opts.solver);
+    EFIE_TRY(p->Z.reserve(sizeof(efie_c128) * (size_t)N * N * p->B));
     EFIE_TRY(p->b.reserve(sizeof(efie_c128) * N));
-    EFIE_TRY(p->x.reserve(sizeof(efie_c128) * N));
+    EFIE_TRY(p->x.reserve(sizeof(efie_c128) * (size_t)N * p->B));
     EFIE_TRY(p->wport.reserve(sizeof(double) * N));
     EFIE_TRY(p->ipiv.reserve(sizeof(int) * N));
     EFIE_CUDA(cudaMemcpyAsync(p->b.p, bc.data(), sizeof(efie_c128) * N, cudaMemcpyHostToDevice, ctx->stream));
     EFIE_CUDA(cudaMemcpyAsync(p->wport.p, wport.data(), sizeof(double) * N, cudaMemcpyHostToDevice, ctx->stream));
-    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N));
+    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B));
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
 }
@@ -418,6 +434,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     efie_ctx *ctx = p->ctx;
     DeviceGuard dg(ctx->device);
     const int N = p->Ne;
+    const size_t NN = (size_t)N * N;
     KernelLog &log = ctx->log;
     log.reset(p->opts.timing != 0);
     efie_sweep_stats local{};
@@ -427,52 +444,57 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     EFIE_TRY(p->out.reserve(sizeof(efie_c128) * 2 * std::max(Nf, 1)));
     EFIE_TRY(p->info.reserve(sizeof(int) * std::max(Nf, 1)));
     EFIE_CUDA(cudaMemsetAsync(p->info.p, 0, sizeof(int) * std::max(Nf, 1), ctx->stream));
-    double ms_fp64 = 0.0;
+    const bool mixed = p->opts.solver == EFIE_SOLVER_MIXED;
+    const int B = p->B;
     efie_status rc = EFIE_OK;
-    for (int fi = 0; fi < Nf && rc == EFIE_OK; fi++) {
-        const Physics ph = efie_physics(freqs[fi], p->mu, p->eps);
-        if (p->centroid) rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph, p->Z.p, p->scratch);
-        else rc = efie_assemble_device(ctx, p->g, ph, p->Z.p);
+    for (int f0 = 0; f0 < Nf && rc == EFIE_OK; f0 += B) {
+        const int nb = std::min(B, Nf - f0);
+        int active[EFIE_MAX_BATCH] = {0};
+        for (int f = 0; f < nb; f++) active[f] = 1;
+        for (int f = 0; f < nb && rc == EFIE_OK; f++) {
+            const Physics ph = efie_physics(freqs[f0 + f], p->mu, p->eps);
+            void *Zf = p->Z.as<efie_c128>() + NN * f;
+            if (p->centroid) rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph, Zf, p->scratch);
+            else rc = efie_assemble_device(ctx, p->g, ph, Zf);
+        }
         if (rc != EFIE_OK) break;
-        bool use_fp64 = p->opts.solver == EFIE_SOLVER_FP64;
-        if (!use_fp64) {
-            rc = efie_mixed_factor(ctx, p->sw, p->Z.p);
+        bool fallback[EFIE_MAX_BATCH] = {false};
+        if (mixed) {
+            rc = efie_mixed_factor(ctx, p->sw, p->Z.p, NN, active);
             if (rc != EFIE_OK) break;
-            int iters = 0;
-            double rel = 0;
-            bool conv = false;
-            rc = efie_mixed_refine(ctx, p->sw, p->Z.p, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
-                                   p->opts.refine_max_iter, &iters, &rel, &conv);
+            RefineResult rr;
+            rc = efie_mixed_refine(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
+                                   p->opts.refine_max_iter, active, &rr);
             if (rc != EFIE_OK) break;
-            int err = 0;
-            rc = efie_mixed_error_flag(ctx, p->sw, &err);
-            if (rc != EFIE_OK) break;
-            S->refine_iters_max = std::max(S->refine_iters_max, iters);
-            if (!conv || err) {
-                // zero pivot or stalled refinement: complex128 LU for this frequency
-                S->n_fp64_fallback++;
-                use_fp64 = true;
-            } else {
-                S->max_relres = std::max(S->max_relres, rel);
+            S->refine_iters_max = std::max(S->refine_iters_max, rr.iters);
+            for (int f = 0; f < nb; f++) {
+                if (!rr.converged[f] || rr.err[f]) {
+                    // zero pivot, timeout or stalled refinement: complex128 LU for this frequency
+                    fallback[f] = true;
+                    S->n_fp64_fallback++;
+                } else {
+                    S->max_relres = std::max(S->max_relres, rr.relres[f]);
+                }
             }
         }
-        if (use_fp64) {
+        for (int f = 0; f < nb && rc == EFIE_OK; f++) {
+            if (mixed && !fallback[f]) continue;
             // cuSOLVER Zgetrf/Zgetrs: timed in class OTHER, not counted as our launches
             size_t tok = log.begin(ctx->stream);
-            rc = plan_solve_fp64(p, fi, nullptr);
-            if (rc != EFIE_OK) break;
-            log.end(EFIE_K_OTHER, ctx->stream, tok, 8.0 / 3.0 * (double)N * N * N, 0);
+            rc = plan_solve_fp64(p, f, f0 + f);
+            if (rc == EFIE_OK) log.end(EFIE_K_OTHER, ctx->stream, tok, 8.0 / 3.0 * (double)N * N * N, 0);
         }
-        rc = efie_port_reduce(ctx, N, p->x.p, p->wport.as<double>(), p->centroid ? EFIE_PORT_EDGE_DIFF : p->opts.port_model,
-                              p->pe - 1, p->ge - 1, p->V0, p->Z0, p->out.as<efie_c128>() + 2 * fi);
+        if (rc != EFIE_OK) break;
+        rc = efie_port_reduce(ctx, N, nb, p->x.p, p->wport.as<double>(),
+                              p->centroid ? EFIE_PORT_EDGE_DIFF : p->opts.port_model, p->pe - 1, p->ge - 1, p->V0,
+                              p->Z0, p->out.as<efie_c128>() + 2 * f0);
         if (rc != EFIE_OK) break;
         if (I) {
-            cudaError_t e = cudaMemcpyAsync(I + (size_t)fi * N, p->x.p, sizeof(efie_c128) * N, cudaMemcpyDeviceToHost,
-                                            ctx->stream);
+            cudaError_t e = cudaMemcpyAsync(I + (size_t)f0 * N, p->x.p, sizeof(efie_c128) * N * nb,
+                                            cudaMemcpyDeviceToHost, ctx->stream);
             if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
         }
     }
-    (void)ms_fp64;
     if (rc == EFIE_OK && Nf > 0) {
         std::vector<efie_c128> res(2 * (size_t)Nf);
         std::vector<int> info(Nf);
@@ -577,24 +599,27 @@ extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c12
     DeviceGuard dg(ctx->device);
     ctx->log.reset(false);
     SolveWork w;
-    EFIE_TRY(efie_mixed_workspace(w, N));
+    EFIE_TRY(efie_mixed_workspace(w, N, 1));
     DevBuf dA;
     EFIE_TRY(dA.reserve(sizeof(efie_c128) * (size_t)N * N));
     EFIE_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(efie_c128) * (size_t)N * N, cudaMemcpyHostToDevice, ctx->stream));
+    const int active[1] = {1};
     efie_debug_disable_tensor_cores(tensor_cores ? 0 : 1);
-    efie_status s = efie_mixed_factor(ctx, w, dA.p);
+    efie_status s = efie_mixed_factor(ctx, w, dA.p, (size_t)N * N, active);
     efie_debug_disable_tensor_cores(0);
     EFIE_TRY(s);
     std::vector<float> pl(2 * (size_t)w.ld * N);
     EFIE_CUDA(cudaMemcpyAsync(pl.data(), w.planes.p, sizeof(float) * pl.size(), cudaMemcpyDeviceToHost, ctx->stream));
     int err = 0;
-    EFIE_CUDA(cudaMemcpyAsync(&err, w.ctl.as<char>() + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    EFIE_CUDA(cudaMemcpyAsync(&err, w.ctl.as<char>() + 36, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     const float *Ar = pl.data(), *Ai = Ar + (size_t)w.ld * N;
     for (int j = 0; j < N; j++)
         for (int i = 0; i < N; i++)
             LU[(size_t)i + (size_t)N * j] = efie_c128{Ar[(size_t)i * w.ld + j], Ai[(size_t)i * w.ld + j]};
     ctx->log.resolve();
-    if (err) return efie_fail(err == 1 ? EFIE_ERR_SINGULAR : EFIE_ERR_TIMEOUT, "LU self-test: device error flag " + std::to_string(err));
+    if (err)
+        return efie_fail(err == 1 ? EFIE_ERR_SINGULAR : EFIE_ERR_TIMEOUT,
+                         "LU self-test: device error flag " + std::to_string(err));
     return EFIE_OK;
 }

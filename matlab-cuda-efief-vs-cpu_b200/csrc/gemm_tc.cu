@@ -55,10 +55,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 // Tiles are built in shared memory in their final swizzled byte layout and
 // written out with coalesced 16-byte stores.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const float *__restrict__ Ar,
-                                                const float *__restrict__ Ai, int ld, float *__restrict__ out) {
+__global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const float *__restrict__ planes,
+                                                size_t pstride, int ld, float *__restrict__ outb, size_t ostride,
+                                                const int *__restrict__ active) {
     __shared__ __align__(1024) float hi[A_TILE];
     __shared__ __align__(1024) float lo[A_TILE];
+    const int f = blockIdx.z;
+    if (!active[f]) return;
+    const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    float *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
     const int s = k + kb;
     for (int e = threadIdx.x; e < A_TILE; e += 256) {
@@ -87,10 +92,15 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const floa
     }
 }
 
-__global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const float *__restrict__ Ar,
-                                                const float *__restrict__ Ai, int ld, float *__restrict__ out) {
+__global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const float *__restrict__ planes,
+                                                size_t pstride, int ld, float *__restrict__ outb, size_t ostride,
+                                                const int *__restrict__ active) {
     extern __shared__ __align__(1024) float dynb[];
     float *hi = dynb, *lo = dynb + B_TILE;
+    const int f = blockIdx.z;
+    if (!active[f]) return;
+    const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    float *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
     const int s = k + kb;
     for (int e = threadIdx.x; e < B_TILE; e += 256) {
@@ -202,9 +212,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // ---------------------------------------------------------------------------
 // The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float *__restrict__ Apack,
-                                                      const float *__restrict__ Bpack, float *__restrict__ Ar,
-                                                      float *__restrict__ Ai, int ld, int *__restrict__ err) {
+__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float *__restrict__ Apackb,
+                                                      size_t astride, const float *__restrict__ Bpackb,
+                                                      size_t bstride, float *__restrict__ planes, size_t pstride,
+                                                      int ld, char *__restrict__ ctl,
+                                                      const int *__restrict__ active) {
+    const int f = blockIdx.z;
+    if (!active[f]) return;
+    const float *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
+    float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
     extern __shared__ uint8_t dyn_raw[];
     // 1024-byte alignment for the swizzled tiles
     float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
@@ -330,26 +347,31 @@ static bool use_tc(int rest) { return !g_tc_disabled && rest >= 256; }
 
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
 
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb) {
-    const int N = w.N, s = k + kb, rest = N - s;
-    if (!use_tc(rest) || kb > NB) return efie_trailing_update_simt(ctx, w, k, kb);
+efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact) {
+    const int N = w.N, s = k + kb, rest = N - s, B = w.B;
+    if (!use_tc(rest) || kb > NB) return efie_trailing_update_simt(ctx, w, k, kb, nact);
     EFIE_TRY(efie_tc_attrs());
     cudaStream_t st = ctx->stream;
     const int mt = (rest + 63) / 64, nt = (rest + TN - 1) / TN;
-    EFIE_TRY(w.packA.reserve(sizeof(float) * (size_t)mt * NCHUNK * 2 * A_TILE));
-    EFIE_TRY(w.packB.reserve(sizeof(float) * (size_t)nt * NCHUNK * 2 * B_TILE));
-    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)w.ld * N;
-    int *err = reinterpret_cast<int *>(w.ctl.as<char>() + 64);
+    // per-frequency staging sized for the first (largest) trailing matrix of an N x N LU
+    const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
+    const size_t astride = (size_t)mt0 * NCHUNK * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK * 2 * B_TILE;
+    EFIE_TRY(w.packA.reserve(sizeof(float) * astride * B));
+    EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * B));
+    float *planes = w.planes.as<float>();
+    const int *active = w.active.as<int>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
-    k_pack_a<<<dim3(mt, NCHUNK), 256, 0, st>>>(N, k, kb, Ar, Ai, w.ld, w.packA.as<float>());
-    k_pack_b<<<dim3(nt, NCHUNK), 256, sizeof(float) * 2 * B_TILE, st>>>(N, k, kb, Ar, Ai, w.ld, w.packB.as<float>());
+    k_pack_a<<<dim3(mt, NCHUNK, B), 256, 0, st>>>(N, k, kb, planes, w.pstride, w.ld, w.packA.as<float>(), astride,
+                                                  active);
+    k_pack_b<<<dim3(nt, NCHUNK, B), 256, sizeof(float) * 2 * B_TILE, st>>>(N, k, kb, planes, w.pstride, w.ld,
+                                                                          w.packB.as<float>(), bstride, active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
-    k_update_tc<<<dim3(nt, mt), 128, GEMM_SMEM, st>>>(N, s, w.packA.as<float>(), w.packB.as<float>(), Ar, Ai, w.ld,
-                                                      err);
+    k_update_tc<<<dim3(nt, mt, B), 128, GEMM_SMEM, st>>>(N, s, w.packA.as<float>(), astride, w.packB.as<float>(),
+                                                         bstride, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rest * rest * kb);
+    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rest * rest * kb * nact);
     return EFIE_OK;
 }

@@ -1,19 +1,23 @@
-// Mixed-precision dense solve of Z x = V on sm_100a.
+// Mixed-precision dense solve of Z x = V on sm_100a, batched over frequencies.
 //
 // The reference factors Z in complex128 with cusolverDnZgetrf/Zgetrs
-// (patch_sweep_fastquad_cuda.cu:765-771).  Here Z (complex128, column-major,
-// as assembled) is kept for the residual, and a complex64 copy is factored
-// without pivoting (Z is complex symmetric and, for these EFIE matrices,
-// strongly diagonal: element growth stays near 1); FP64 iterative
+// (patch_sweep_fastquad_cuda.cu:765-771), one frequency at a time.  Here a
+// batch of B frequencies is solved together: Z_f (complex128, column-major,
+// as assembled) is kept for the residual, and a complex64 copy of each Z_f is
+// factored without pivoting (Z is complex symmetric and, for these EFIE
+// matrices, strongly diagonal: element growth stays near 1); FP64 iterative
 // refinement then recovers the complex128 solution:
 //     x = 0, r = V;  repeat { d = U^-1 L^-1 r (complex64);  x += d;
 //                            r = V - Z x (complex128) }  until ||r|| <= tol ||V||.
-// A zero pivot or a refinement that stalls makes the caller re-solve that
-// frequency with the complex128 LU.
+// Every kernel carries the frequency in its grid (blockIdx.z or blockIdx.x),
+// so the latency-bound parts of B problems (diagonal blocks, triangular-solve
+// chains, small trailing updates) overlap instead of serialising.  A zero
+// pivot or a refinement that stalls makes the caller re-solve that frequency
+// with the complex128 LU.
 //
-// Layout of the complex64 working matrix: two FP32 planes (re, im),
-// row-major, leading dimension ld (multiple of 4).  Z is symmetric, so the
-// row-major planes are filled from the column-major Z by a tiled transpose.
+// Working matrix of frequency f: two FP32 planes (re, im), row-major,
+// leading dimension ld (multiple of 64), at planes + f * pstride.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -23,28 +27,32 @@
 namespace {
 
 constexpr int NB = 64;  // diagonal block size of the LU and the triangular solves
+constexpr size_t kTwoTiles = sizeof(float2) * 2 * NB * (NB + 1);
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
 // ---------------------------------------------------------------------------
-// Z (c128, column-major Ne x Ne) -> planes (row-major, ld).  32x32 tiles.
+// Z_f (c128, column-major) -> planes_f (row-major).  32x32 tiles, grid z = f.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__restrict__ Z, float *__restrict__ Ar,
-                                                     float *__restrict__ Ai, int ld) {
+__global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__restrict__ Z, size_t zstride,
+                                                     float *__restrict__ planes, size_t pstride, int ld) {
     __shared__ float tr[32][33], ti[32][33];
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // bx: column block of Z, by: row block of Z
+    const int f = blockIdx.z;
+    Z += zstride * f;
+    float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // bx: column block, by: row block
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int r = ty; r < 32; r += 8) {
-        const int row = by + tx, col = bx + r;  // coalesced along rows of the column-major Z
+        const int row = by + tx, col = bx + r;  // coalesced along the columns of Z
         double2 v = (row < N && col < N) ? Z[(size_t)row + (size_t)N * col] : make_double2(0, 0);
         tr[r][tx] = (float)v.x;
         ti[r][tx] = (float)v.y;
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
-        const int row = by + r, col = bx + tx;  // row-major plane, coalesced along columns
+        const int row = by + r, col = bx + tx;  // coalesced along the rows of the planes
         if (row < N && col < N) {
             Ar[(size_t)row * ld + col] = tr[tx][r];
             Ai[(size_t)row * ld + col] = ti[tx][r];
@@ -53,16 +61,22 @@ __global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__res
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block: unblocked LU (no pivoting) of A[k:k+kb, k:k+kb] and the
-// inverses of its unit-lower L and upper U factors (kept for the panel
-// products and the triangular solves).  One CTA of 1024 threads.
+// Diagonal block bi of every frequency (blockIdx.x = f): unblocked LU without
+// pivoting of A[k:k+kb, k:k+kb] and the inverses of its unit-lower L and upper
+// U factors (kept for the panel products and the triangular solves).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__restrict__ Ar, float *__restrict__ Ai,
-                                                      int ld, float2 *__restrict__ Linv, float2 *__restrict__ Uinv,
-                                                      int *__restrict__ err) {
+__global__ void __launch_bounds__(1024) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
+                                                      size_t pstride, int ld, float2 *__restrict__ dinv,
+                                                      size_t dstride, char *__restrict__ ctl,
+                                                      const int *__restrict__ active) {
+    const int f = blockIdx.x;
+    if (!active[f]) return;
     extern __shared__ float2 dyn[];
     float2(*a)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);
     float2(*w)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
+    float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
+    int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
     const int tid = threadIdx.x;
     for (int e = tid; e < NB * NB; e += 1024) {
         const int i = e / NB, j = e % NB;
@@ -93,7 +107,6 @@ __global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__re
         const float2 p = a[NB - 1][NB - 1];
         if (!(p.x * p.x + p.y * p.y > 0.f)) atomicExch(err, 1);
     }
-    // write the factors back
     for (int e = tid; e < NB * NB; e += 1024) {
         const int i = e / NB, j = e % NB;
         if (i < kb && j < kb) {
@@ -101,7 +114,7 @@ __global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__re
             Ai[(size_t)(k + i) * ld + k + j] = a[i][j].y;
         }
     }
-    // Linv: unit lower; column c by forward substitution.  16 threads per column.
+    // Linv: unit lower; column c by forward substitution, 16 threads per column
     const int c = tid >> 4, sub = tid & 15;
     for (int i = 0; i < NB; i++) {
         float2 s = make_float2(0.f, 0.f);
@@ -120,7 +133,7 @@ __global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__re
     }
     for (int e = tid; e < NB * NB; e += 1024) Linv[e] = w[e / NB][e % NB];
     __syncthreads();
-    // Uinv: upper; column c by backward substitution.
+    // Uinv: upper; column c by backward substitution
     for (int i = NB - 1; i >= 0; i--) {
         float2 s = make_float2(0.f, 0.f);
         for (int j = i + 1 + sub; j <= c; j += 16) {
@@ -149,25 +162,29 @@ __global__ void __launch_bounds__(1024) k_diag_factor(int k, int kb, float *__re
 }
 
 // ---------------------------------------------------------------------------
-// Panels: U12 = Linv * A12 (rows k..k+kb, columns right of the block) and
-// L21 = A21 * Uinv (columns k..k+kb, rows below).  One 64x64 tile per CTA,
-// in place.  blockIdx.y = 0: row panel, 1: column panel.
+// Panels: U12 = Linv * A12 (row panel) and L21 = A21 * Uinv (column panel).
+// One 64x64 tile per CTA, in place.  blockIdx.y: 0 row panel, 1 column panel;
+// blockIdx.z: frequency.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, float *__restrict__ Ar, float *__restrict__ Ai,
-                                                int ld, const float2 *__restrict__ Linv,
-                                                const float2 *__restrict__ Uinv) {
+__global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, float *__restrict__ planes,
+                                                size_t pstride, int ld, const float2 *__restrict__ dinv,
+                                                size_t dstride, const int *__restrict__ active) {
+    const int f = blockIdx.z;
+    if (!active[f]) return;
     extern __shared__ float2 dyn[];
     float2(*M)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);               // the inverse
     float2(*T)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));  // the panel tile
+    float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    const float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
     const int tid = threadIdx.x;
     const bool rowp = blockIdx.y == 0;
-    const int off = k + kb + blockIdx.x * NB;  // first column (row panel) / row (column panel) of the tile
+    const int off = k + kb + blockIdx.x * NB;
     if (off >= N) return;
     const int ext = min(NB, N - off);
     const float2 *inv = rowp ? Linv : Uinv;
     for (int e = tid; e < NB * NB; e += 256) M[e / NB][e % NB] = inv[e];
     for (int e = tid; e < NB * NB; e += 256) {
-        const int i = e / NB, j = e % NB;  // i: row within the tile, j: column within the tile
+        const int i = e / NB, j = e % NB;
         float2 v = make_float2(0.f, 0.f);
         if (rowp) {
             if (i < kb && j < ext) v = make_float2(Ar[(size_t)(k + i) * ld + off + j], Ai[(size_t)(k + i) * ld + off + j]);
@@ -177,7 +194,6 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, float *__r
         T[i][j] = v;
     }
     __syncthreads();
-    // each thread: 16 outputs (4 rows x 4 cols)
     const int r0 = (tid >> 4) * 4, c0 = (tid & 15) * 4;
     float2 acc[4][4];
 #pragma unroll
@@ -220,13 +236,16 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, float *__r
 
 // ---------------------------------------------------------------------------
 // Trailing update A22 -= L21 * U12 on CUDA cores (complex FP32), 64x64 tiles,
-// K = kb <= 64.  Used for small trailing matrices and as the portable path.
+// K = kb <= 64: small trailing matrices and the portable path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float *__restrict__ Ar,
-                                                     float *__restrict__ Ai, int ld) {
+__global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float *__restrict__ planes, size_t pstride,
+                                                     int ld, const int *__restrict__ active) {
+    const int f = blockIdx.z;
+    if (!active[f]) return;
     extern __shared__ float2 dyn[];
     float2(*Ls)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);
     float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
+    float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     const int tid = threadIdx.x;
     const int s = k + kb;
     const int row0 = s + blockIdx.y * NB, col0 = s + blockIdx.x * NB;
@@ -275,16 +294,25 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float
 }
 
 // ---------------------------------------------------------------------------
-// r = V - Z x  (complex128 GEMV over the column-major Z), the complex64 copy
-// of r for the next correction, and ||r||^2.  Block = 32 rows x 8 column
-// groups.  The last CTA turns ||r|| into the convergence flag.
+// r_f = V - Z_f x_f (complex128 GEMV over the column-major Z_f), the complex64
+// copy of r_f for the next correction, and ||r_f||.  Block = 32 rows x 8
+// column groups, grid y = f.  The last CTA of frequency f turns ||r_f|| into
+// its convergence flag (ctl_f: red[3] @0, counter @24, conv @28, skip @32).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restrict__ Z, const double2 *__restrict__ x,
-                                                  const double2 *__restrict__ b, float2 *__restrict__ rf,
-                                                  double *__restrict__ red /* [0]=sum r^2, [1]=||b||, [2]=relres */,
-                                                  unsigned int *__restrict__ counter, int *__restrict__ conv,
-                                                  double tol, int *__restrict__ skip) {
+__global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restrict__ Zb, size_t zstride,
+                                                  const double2 *__restrict__ xb, const double2 *__restrict__ b,
+                                                  float2 *__restrict__ rfb, int vstride, char *__restrict__ ctl,
+                                                  double tol) {
+    const int f = blockIdx.y;
+    char *c = ctl + 64 * f;
+    double *red = reinterpret_cast<double *>(c);
+    unsigned int *counter = reinterpret_cast<unsigned int *>(c + 24);
+    int *conv = reinterpret_cast<int *>(c + 28);
+    int *skip = reinterpret_cast<int *>(c + 32);
     if (*skip) return;
+    const double2 *Z = Zb + zstride * f;
+    const double2 *x = xb + (size_t)N * f;
+    float2 *rf = rfb + (size_t)vstride * f;
     __shared__ double2 part[8][32];
     __shared__ double sq[32];
     __shared__ bool last;
@@ -343,12 +371,14 @@ __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restri
 // ---------------------------------------------------------------------------
 // Port reduction + Zin/S11 (patch_sweep_fastquad_cuda.cu:777-799 for the
 // Gaussian model; patch_sweep_cuda.cu:484-494 for the edge difference).
-// One CTA.  out[0] = Zin, out[1] = S11.
+// One CTA per frequency.  out_f = {Zin, S11}.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_port(int N, const double2 *__restrict__ x, const double *__restrict__ wport,
+__global__ void __launch_bounds__(1024) k_port(int N, const double2 *__restrict__ xb, const double *__restrict__ wport,
                                                int model, int pe, int ge, double V0, double Z0,
                                                double2 *__restrict__ out) {
     __shared__ double sr[1024], si[1024];
+    const int f = blockIdx.x;
+    const double2 *x = xb + (size_t)N * f;
     const int tid = threadIdx.x;
     double a = 0.0, c = 0.0;
     if (model == EFIE_PORT_GAUSS) {
@@ -377,22 +407,28 @@ __global__ void __launch_bounds__(1024) k_port(int N, const double2 *__restrict_
         const double Zr = V0 * (Ipr / den), Zi = -V0 * (Ipi / den);
         const double ar = Zr - Z0, ai = Zi, br = Zr + Z0, bi = Zi;
         const double bden = br * br + bi * bi;
-        out[0] = make_double2(Zr, Zi);
-        out[1] = make_double2((ar * br + ai * bi) / bden, (ai * br - ar * bi) / bden);
+        out[2 * f] = make_double2(Zr, Zi);
+        out[2 * f + 1] = make_double2((ar * br + ai * bi) / bden, (ai * br - ar * bi) / bden);
     }
 }
 
-__global__ void k_fill_c128(int N, double2 *__restrict__ dst, double2 v) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) dst[i] = v;
+__global__ void k_fill_c128(size_t n, double2 *__restrict__ dst, double2 v) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = v;
 }
 
-}  // namespace
-
-int efie_solve_nb() { return NB; }
-
-namespace {
-constexpr size_t kTwoTiles = sizeof(float2) * 2 * NB * (NB + 1);
+__global__ void k_init_ctl(int B, char *__restrict__ ctl, double bnorm, const int *__restrict__ active) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= B) return;
+    char *c = ctl + 64 * f;
+    double *red = reinterpret_cast<double *>(c);
+    red[0] = 0.0;
+    red[1] = bnorm;
+    red[2] = 1.0;
+    *reinterpret_cast<unsigned int *>(c + 24) = 0u;
+    *reinterpret_cast<int *>(c + 28) = 0;
+    *reinterpret_cast<int *>(c + 32) = active[f] ? 0 : 1;  // inactive slots count as converged
+}
 
 efie_status set_smem_attrs() {
     static bool done = false;
@@ -403,150 +439,149 @@ efie_status set_smem_attrs() {
     done = true;
     return EFIE_OK;
 }
+
 }  // namespace
 
-efie_status efie_mixed_workspace(SolveWork &w, int N) {
+int efie_solve_nb() { return NB; }
+
+efie_status efie_mixed_workspace(SolveWork &w, int N, int B) {
     EFIE_TRY(set_smem_attrs());
     w.N = N;
+    w.B = B;
     w.ld = (N + 63) / 64 * 64;
     w.nblk = (N + NB - 1) / NB;
-    const size_t pbytes = sizeof(float) * 2 * (size_t)w.ld * N;
+    w.pstride = 2 * (size_t)w.ld * N;
+    w.dstride = 2 * (size_t)NB * NB * w.nblk;
+    w.vstride = w.ld;
+    const size_t pbytes = sizeof(float) * w.pstride * B;
     if (pbytes > w.planes.bytes) {
         EFIE_TRY(w.planes.reserve(pbytes));
         EFIE_CUDA(cudaMemset(w.planes.p, 0, pbytes));  // padding columns stay zero
     }
-    EFIE_TRY(w.dinv.reserve(sizeof(float2) * 2 * (size_t)NB * NB * w.nblk));
-    EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.ld));
-    const size_t fbytes = sizeof(int) * 2 * (size_t)w.nblk;
-    if (fbytes > w.flags.bytes) {
-        EFIE_TRY(w.flags.reserve(fbytes));
-        EFIE_CUDA(cudaMemset(w.flags.p, 0, fbytes));  // epochs restart above any stale value
-        w.epoch = 0;
-    }
-    EFIE_TRY(w.ctl.reserve(256));
+    EFIE_TRY(w.dinv.reserve(sizeof(float2) * w.dstride * B));
+    EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.vstride * B));
+    EFIE_TRY(w.ctl.reserve(64 * (size_t)B + 64));
+    EFIE_TRY(w.active.reserve(sizeof(int) * B));
+    EFIE_TRY(efie_trsv_workspace(w));
     return EFIE_OK;
 }
 
-efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z) {
+efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
-    const int N = w.N, ld = w.ld;
-    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)ld * N;
-    int *err = reinterpret_cast<int *>(w.ctl.as<char>() + 64);
-    EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 256, s));
-    dim3 tg((N + 31) / 32, (N + 31) / 32);
+    const int N = w.N, ld = w.ld, B = w.B;
+    float *planes = w.planes.as<float>();
+    char *ctl = w.ctl.as<char>();
+    int nact = 0;
+    for (int f = 0; f < B; f++) nact += active_host[f] ? 1 : 0;
+    EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 64 * (size_t)B, s));
+    EFIE_CUDA(cudaMemcpyAsync(w.active.p, active_host, sizeof(int) * B, cudaMemcpyHostToDevice, s));
+    const int *active = w.active.as<int>();
+    dim3 tg((N + 31) / 32, (N + 31) / 32, B);
     size_t tok = log.begin(s);
-    k_z_to_planes<<<tg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), Ar, Ai, ld);
+    k_z_to_planes<<<tg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, s, tok, 24.0 * (double)N * N);
+    log.end(EFIE_K_PANEL, s, tok, 24.0 * (double)N * N * nact);
     float2 *dinv = w.dinv.as<float2>();
     for (int bi = 0; bi < w.nblk; bi++) {
         const int k = bi * NB, kb = std::min(NB, N - k);
-        float2 *Linv = dinv + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
         const int rest = N - k - kb;
         tok = log.begin(s);
-        k_diag_factor<<<1, 1024, kTwoTiles, s>>>(k, kb, Ar, Ai, ld, Linv, Uinv, err);
+        k_diag_factor<<<B, 1024, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
         if (rest > 0) {
-            dim3 pg((rest + NB - 1) / NB, 2);
-            k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, Ar, Ai, ld, Linv, Uinv);
+            dim3 pg((rest + NB - 1) / NB, 2, B);
+            k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, active);
         }
         EFIE_CUDA(cudaGetLastError());
         log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
-        if (rest > 0) EFIE_TRY(efie_trailing_update(ctx, w, k, kb));
+        if (rest > 0) EFIE_TRY(efie_trailing_update(ctx, w, k, kb, nact));
     }
-    EFIE_CUDA(cudaGetLastError());
     return EFIE_OK;
 }
 
-efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb) {
+efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact) {
     const int N = w.N, rest = N - k - kb;
-    float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)w.ld * N;
-    dim3 g((rest + NB - 1) / NB, (rest + NB - 1) / NB);
+    dim3 g((rest + NB - 1) / NB, (rest + NB - 1) / NB, w.B);
     size_t tok = ctx->log.begin(ctx->stream);
-    k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, k, kb, Ar, Ai, w.ld);
+    k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, k, kb, w.planes.as<float>(), w.pstride, w.ld,
+                                                      w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
-    ctx->log.end(EFIE_K_GEMM, ctx->stream, tok, 8.0 * (double)rest * rest * kb);
+    ctx->log.end(EFIE_K_GEMM, ctx->stream, tok, 8.0 * (double)rest * rest * kb * nact);
     return EFIE_OK;
 }
 
-efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const void *b, void *x, double bnorm,
-                              double tol, int max_iter, int *iters, double *relres, bool *converged) {
+efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
+                              double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res) {
     cudaStream_t s = ctx->stream;
-    const int N = w.N, ld = w.ld;
-    const float *Ar = w.planes.as<float>(), *Ai = Ar + (size_t)ld * N;
-    float2 *rf = w.vec.as<float2>(), *y = rf + ld, *d = y + ld;
-    char *ctl = w.ctl.as<char>();
-    double *red = reinterpret_cast<double *>(ctl);            // [0..2]
-    unsigned int *counter = reinterpret_cast<unsigned int *>(ctl + 32);
-    int *conv = reinterpret_cast<int *>(ctl + 40);
-    int *skip = reinterpret_cast<int *>(ctl + 44);
-    int *err = reinterpret_cast<int *>(ctl + 64);
-    int *flagsL = w.flags.as<int>(), *flagsU = flagsL + w.nblk;
-    // x = 0, rf = b (complex64), red = {0, ||b||, 1}
     KernelLog &log = ctx->log;
-    size_t tok = log.begin(s);
-    k_fill_c128<<<(N + 255) / 256, 256, 0, s>>>(N, static_cast<double2 *>(x), make_double2(0.0, 0.0));
-    log.end(EFIE_K_OTHER, s, tok, 0.0);
-    const double init[3] = {0.0, bnorm, 1.0};
-    EFIE_CUDA(cudaMemcpyAsync(red, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    EFIE_CUDA(cudaMemsetAsync(ctl + 32, 0, 16, s));
-    int it = 0;
-    bool done = false;
-    int hconv = 0;
-    // initial residual r = b (x = 0) through the residual kernel keeps one code path
+    const int N = w.N, B = w.B;
+    char *ctl = w.ctl.as<char>();
+    float2 *vec = w.vec.as<float2>();
+    float2 *rf = vec, *y = vec + (size_t)w.vstride * B, *d = y + (size_t)w.vstride * B;
+    int nact = 0;
+    for (int f = 0; f < B; f++) nact += active_host[f] ? 1 : 0;
     const double zbytes = 16.0 * (double)N * N, lubytes = 8.0 * (double)N * N;
-    tok = log.begin(s);
-    k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z), static_cast<const double2 *>(x),
-                                             static_cast<const double2 *>(b), rf, red, counter, conv, -1.0, skip);
+    size_t tok = log.begin(s);
+    k_fill_c128<<<(unsigned)(((size_t)N * B + 255) / 256), 256, 0, s>>>((size_t)N * B, static_cast<double2 *>(x),
+                                                                        make_double2(0.0, 0.0));
+    k_init_ctl<<<(B + 63) / 64, 64, 0, s>>>(B, ctl, bnorm, w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_RESIDUAL, s, tok, zbytes);
-    while (!done) {
+    log.end(EFIE_K_OTHER, s, tok, 0.0, 2);
+    // initial residual r = V (x = 0) through the residual kernel keeps one code path
+    dim3 rg((N + 31) / 32, B);
+    tok = log.begin(s);
+    k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, static_cast<const double2 *>(x),
+                                  static_cast<const double2 *>(b), rf, w.vstride, ctl, -1.0);
+    EFIE_CUDA(cudaGetLastError());
+    log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
+    int it = 0;
+    std::vector<char> hctl(64 * (size_t)B);
+    bool all_done = false, failed = false;
+    while (!all_done && !failed) {
         const int chunk = std::min(5, max_iter - it);
         if (chunk <= 0) break;
         for (int c = 0; c < chunk; c++) {
             const int epoch = ++w.epoch;
             tok = log.begin(s);
-            EFIE_TRY(efie_trsv(ctx, w, true, rf, y, x, flagsL, epoch, err, skip));
-            EFIE_TRY(efie_trsv(ctx, w, false, y, d, x, flagsU, epoch, err, skip));
-            log.end(EFIE_K_TRSV, s, tok, lubytes, 2);
+            EFIE_TRY(efie_trsv(ctx, w, true, rf, y, x, epoch));
+            EFIE_TRY(efie_trsv(ctx, w, false, y, d, x, epoch));
+            log.end(EFIE_K_TRSV, s, tok, lubytes * nact, 2);
             tok = log.begin(s);
-            k_residual<<<(N + 31) / 32, 256, 0, s>>>(N, static_cast<const double2 *>(Z),
-                                                     static_cast<const double2 *>(x),
-                                                     static_cast<const double2 *>(b), rf, red, counter, conv, tol,
-                                                     skip);
+            k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride,
+                                          static_cast<const double2 *>(x), static_cast<const double2 *>(b), rf,
+                                          w.vstride, ctl, tol);
             EFIE_CUDA(cudaGetLastError());
-            log.end(EFIE_K_RESIDUAL, s, tok, zbytes);
+            log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
         }
         it += chunk;
-        int hctl[2] = {0, 0};
-        EFIE_CUDA(cudaMemcpyAsync(hctl, conv, sizeof(int), cudaMemcpyDeviceToHost, s));
-        EFIE_CUDA(cudaMemcpyAsync(hctl + 1, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        EFIE_CUDA(cudaMemcpyAsync(hctl.data(), ctl, 64 * (size_t)B, cudaMemcpyDeviceToHost, s));
         EFIE_CUDA(cudaStreamSynchronize(s));
-        hconv = hctl[0];
-        if (hctl[1]) break;
-        if (hconv) done = true;
+        all_done = true;
+        for (int f = 0; f < B; f++) {
+            const char *c = hctl.data() + 64 * f;
+            if (!active_host[f]) continue;
+            if (*reinterpret_cast<const int *>(c + 36)) failed = true;
+            if (!*reinterpret_cast<const int *>(c + 28)) all_done = false;
+        }
     }
-    double hred[3];
-    EFIE_CUDA(cudaMemcpyAsync(hred, red, sizeof(hred), cudaMemcpyDeviceToHost, s));
+    EFIE_CUDA(cudaMemcpyAsync(hctl.data(), ctl, 64 * (size_t)B, cudaMemcpyDeviceToHost, s));
     EFIE_CUDA(cudaStreamSynchronize(s));
-    *relres = hred[2];
-    *iters = it;
-    *converged = hconv != 0;
+    res->iters = it;
+    for (int f = 0; f < B; f++) {
+        const char *c = hctl.data() + 64 * f;
+        res->relres[f] = reinterpret_cast<const double *>(c)[2];
+        res->converged[f] = *reinterpret_cast<const int *>(c + 28) != 0;
+        res->err[f] = *reinterpret_cast<const int *>(c + 36);
+    }
     return EFIE_OK;
 }
 
-efie_status efie_port_reduce(efie_ctx *ctx, int N, const void *x, const double *wport, int model, int pe, int ge,
-                             double V0, double Z0, void *out2) {
+efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
+                             int ge, double V0, double Z0, void *out) {
     size_t tok = ctx->log.begin(ctx->stream);
-    k_port<<<1, 1024, 0, ctx->stream>>>(N, static_cast<const double2 *>(x), wport, model, pe, ge, V0, Z0,
-                                         static_cast<double2 *>(out2));
+    k_port<<<B, 1024, 0, ctx->stream>>>(N, static_cast<const double2 *>(x), wport, model, pe, ge, V0, Z0,
+                                         static_cast<double2 *>(out));
     EFIE_CUDA(cudaGetLastError());
     ctx->log.end(EFIE_K_OTHER, ctx->stream, tok, 0.0);
-    return EFIE_OK;
-}
-
-efie_status efie_mixed_error_flag(efie_ctx *ctx, SolveWork &w, int *flag) {
-    EFIE_CUDA(cudaMemcpyAsync(flag, w.ctl.as<char>() + 64, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
 }

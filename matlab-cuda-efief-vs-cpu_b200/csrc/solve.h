@@ -1,32 +1,48 @@
-// Mixed-precision solver workspace and entry points (solve.cu, gemm_tc.cu).
+// Mixed-precision solver, batched over frequencies (solve.cu, trsv.cu, gemm_tc.cu).
 #pragma once
 
 #include "efie_internal.h"
 
+constexpr int EFIE_MAX_BATCH = 16;
+
 struct SolveWork {
     int N = 0, ld = 0, nblk = 0;
-    int epoch = 0;
-    DevBuf planes;   // float re[N][ld], im[N][ld]  (row-major)
-    DevBuf dinv;     // float2 [nblk][2][NB*NB]  (L^-1, U^-1 of each diagonal block)
-    DevBuf vec;      // float2 rf[ld], y[ld], d[ld]
-    DevBuf flags;    // int [2*nblk]
-    DevBuf ctl;      // reductions, counters, flags (256 B)
+    int B = 0;                // batch slots (frequencies solved together)
+    int epoch = 0;            // triangular-solve epoch (tags the progress counters)
+    size_t pstride = 0;       // floats per frequency in `planes` (2 * ld * N)
+    size_t dstride = 0;       // float2 per frequency in `dinv`
+    int vstride = 0;          // float2 per frequency in each vector of `vec`
+    int grid = 0;             // CTAs of the triangular-solve grid
+    DevBuf planes;   // per f: float re[N][ld], im[N][ld]  (row-major)
+    DevBuf dinv;     // per f: float2 [nblk][2][NB*NB] (L^-1, U^-1 of each diagonal block)
+    DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]
+    DevBuf prog;     // triangular-solve progress counters: u64 [2][B][grid] on 64-byte lines
+    DevBuf ctl;      // per f 64 bytes: red[3] @0, counter @24, conv @28, skip @32, err @36
+    DevBuf active;   // int[B]: slot holds a frequency of this batch
     DevBuf packA, packB;  // tensor-core operand staging
 };
 
-int efie_solve_nb();
-efie_status efie_mixed_workspace(SolveWork &w, int N);
-efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z);
-efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, const void *b, void *x, double bnorm,
-                              double tol, int max_iter, int *iters, double *relres, bool *converged);
-efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int *flags,
-                      int epoch, int *err, const int *skip);
-efie_status efie_mixed_error_flag(efie_ctx *ctx, SolveWork &w, int *flag);
-efie_status efie_port_reduce(efie_ctx *ctx, int N, const void *x, const double *wport, int model, int pe, int ge,
-                             double V0, double Z0, void *out2);
+struct RefineResult {
+    int iters = 0;
+    double relres[EFIE_MAX_BATCH];
+    bool converged[EFIE_MAX_BATCH];
+    int err[EFIE_MAX_BATCH];
+};
 
-// A22 -= L21 * U12 for the block at (k, kb): tensor cores when the trailing
-// matrix is large enough, CUDA cores otherwise.
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb);
-efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb);
+int efie_solve_nb();
+efie_status efie_mixed_workspace(SolveWork &w, int N, int B);
+efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host);
+efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
+                              double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
+efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
+                             int ge, double V0, double Z0, void *out);
+
+// Triangular solves of every active frequency in one cooperative launch.
+efie_status efie_trsv_workspace(SolveWork &w);
+efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int epoch);
+
+// A22 -= L21 * U12 for the block at (k, kb) of every active frequency:
+// tensor cores when the trailing matrix is large enough, CUDA cores otherwise.
+efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact);
+efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact);
 extern "C" void efie_debug_disable_tensor_cores(int disable);

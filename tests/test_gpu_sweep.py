@@ -106,3 +106,15 @@ def test_plan_reuse_and_currents():
     x = a[2][:, 0]
     assert np.linalg.norm(p["b"] - Z @ x) / np.linalg.norm(p["b"]) < 1e-9
     plan.close()
+
+
+@pytest.mark.parametrize("batch", [1, 2, 4])
+def test_batched_sweep_matches_unbatched(batch):
+    """Frequencies solved together (ragged last batch) give the same Zin."""
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    freqs = d.freqs[:5]
+    Zb, Sb, st = _sweep(p, freqs, "mixed", batch=batch)
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zb - Zo) / np.abs(Zo)).max() <= 1e-6
+    assert st["n_fp64_fallback"] == 0 and st["max_relres"] <= 1e-10
