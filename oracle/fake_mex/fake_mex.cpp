@@ -134,7 +134,7 @@ void fm_read(const mxArray *a, double *re, double *im) {
 }
 }
 
-void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]);
+int mexAtExit(void (*)(void)) { return 0; }
 
 // Calls mexFunction; returns 0 on success, 1 with the error id/message copied out.
 extern "C" int fm_call(int nlhs, mxArray **plhs, int nrhs, const mxArray **prhs, char *id, char *msg, int cap) {

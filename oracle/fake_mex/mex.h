@@ -7,6 +7,10 @@ extern "C" {
 #endif
 /* Throws fake_mex::MexError (C++): the caller of mexFunction catches it. */
 void mexErrMsgIdAndTxt(const char *id, const char *fmt, ...);
+/* Runs fn when the library is unloaded (here: never; kept for the API). */
+int mexAtExit(void (*fn)(void));
+/* The gateway every MEX file defines (C linkage, as in MATLAB's mex.h). */
+void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]);
 #ifdef __cplusplus
 }
 #endif
