@@ -290,6 +290,34 @@ efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32
 /* 1 disables the tensor-core trailing update process-wide (CUDA-core path). */
 void efie_debug_disable_tensor_cores(int disable);
 
+/* ---------------------------------------------------------------------- */
+/* Centroid assembly without device allocation                             */
+/* ---------------------------------------------------------------------- */
+#define EFIE_NOALLOC_MAX_NE 16384
+#define EFIE_NOALLOC_MAX_NT 16384
+
+/* No counterpart in the reference.  The same result as efie_gassemble_zv
+ * (Z and Vrhs of the one-point centroid assembly) for callers that cannot
+ * call cudaMalloc -- code running while a CUDA graph is captured, processes
+ * held to a memory budget fixed at start-up, hosts that own every device
+ * buffer.  Every array argument (V ... len, Z, Vrhs) is a DEVICE pointer in
+ * the MEX layout; exc (host) = [patchEdge, groundEdge, V0, spreadRadius,
+ * selfAlpha].  The function allocates nothing: its scratch is one fixed
+ * __device__ array (about 3.2 MB) that every GPU loading this library keeps
+ * until exit, which limits Ne <= EFIE_NOALLOC_MAX_NE and Nt <=
+ * EFIE_NOALLOC_MAX_NT (larger sizes are rejected with EFIE_ERR_ARGS).  All
+ * calls share that array: calls that overlap on the GPU race, so serialise
+ * them.  The first call on a device looks up the array's address with that
+ * device current; make it before any stream capture.  Runs on `stream` (a
+ * cudaStream_t) and returns after synchronising it. */
+efie_status efie_gassemble_zv_noalloc(int device, void *stream, int32_t Nv, int32_t Nt, int32_t Ne,
+                                      const double *V, const int32_t *F, const int32_t *E,
+                                      const int32_t *plusTri, const int32_t *minusTri,
+                                      const int32_t *plusSign, const int32_t *minusSign,
+                                      const double *rp, const double *rm, const double *Ap, const double *Am,
+                                      const double *len, efie_c128 k, double omega, double mu, efie_c128 eps,
+                                      const double exc[5], efie_c128 *Z, efie_c128 *Vrhs);
+
 #ifdef __cplusplus
 }
 #endif
