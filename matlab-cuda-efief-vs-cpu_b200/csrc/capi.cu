@@ -350,6 +350,14 @@ int choose_batch(int N, int requested, int solver) {
     return std::max(1, std::min(B, 8));
 }
 
+// Outer LU panel width: the caller's choice, else the tuned table (wider
+// panels cut trailing-matrix traffic; narrower ones keep fewer terms per
+// tensor-core accumulation).
+int choose_panel(int N, int requested) {
+    if (requested == 64 || requested == 128 || requested == 256) return requested;
+    return N >= 4096 ? 256 : 128;
+}
+
 efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c128 eps, int pe, int ge, double V0,
                         double spread, double Z0, const efie_sweep_opts *opts) {
     efie_ctx *ctx = p->ctx;
@@ -385,7 +393,7 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
     EFIE_TRY(p->ipiv.reserve(sizeof(int) * N));
     EFIE_CUDA(cudaMemcpyAsync(p->b.p, bc.data(), sizeof(efie_c128) * N, cudaMemcpyHostToDevice, ctx->stream));
     EFIE_CUDA(cudaMemcpyAsync(p->wport.p, wport.data(), sizeof(double) * N, cudaMemcpyHostToDevice, ctx->stream));
-    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B));
+    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B, choose_panel(N, p->opts.lu_nb)));
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
 }
@@ -599,7 +607,7 @@ extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c12
     DeviceGuard dg(ctx->device);
     ctx->log.reset(false);
     SolveWork w;
-    EFIE_TRY(efie_mixed_workspace(w, N, 1));
+    EFIE_TRY(efie_mixed_workspace(w, N, 1, 256));
     DevBuf dA;
     EFIE_TRY(dA.reserve(sizeof(efie_c128) * (size_t)N * N));
     EFIE_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(efie_c128) * (size_t)N * N, cudaMemcpyHostToDevice, ctx->stream));

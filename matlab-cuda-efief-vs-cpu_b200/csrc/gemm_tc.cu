@@ -23,11 +23,11 @@
 
 namespace {
 
-constexpr int NB = 64;           // LU panel width (kb <= NB)
+constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
 constexpr int TM = 128;          // accumulator rows (64 complex rows)
 constexpr int TN = 256;          // accumulator columns (complex columns)
 constexpr int KC = 32;           // fp32 elements per 128-byte swizzle row (one K' chunk)
-constexpr int NCHUNK = 2 * NB / KC;   // K' = 2*NB = 128 -> 4 chunks
+constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 16 chunks
 constexpr int A_TILE = TM * KC;       // floats per A tile (16 KB)
 constexpr int B_TILE = TN * KC;       // floats per B tile (32 KB)
 constexpr int STAGE_FLOATS = 2 * A_TILE + 2 * B_TILE;   // hi/lo of A and B: 96 KB
@@ -55,8 +55,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 // Tiles are built in shared memory in their final swizzled byte layout and
 // written out with coalesced 16-byte stores.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const float *__restrict__ planes,
-                                                size_t pstride, int ld, float *__restrict__ outb, size_t ostride,
+__global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol, int K, int nchunk,
+                                                const float *__restrict__ planes, size_t pstride, int ld,
+                                                float *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
     __shared__ __align__(1024) float hi[A_TILE];
     __shared__ __align__(1024) float lo[A_TILE];
@@ -65,16 +66,15 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const floa
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     float *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
-    const int s = k + kb;
     for (int e = threadIdx.x; e < A_TILE; e += 256) {
         const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
         const int kp = chunk * KC + kq;              // K' index
-        const int kk = kp & 63;                      // column within the panel
-        const bool second = kp >= 64;
-        const int row = s + tile * 64 + (r & 63);
+        const bool second = kp >= K;
+        const int kk = second ? kp - K : kp;         // column within the L block
+        const int row = r0 + tile * 64 + (r & 63);
         float v = 0.f;
-        if (row < N && kk < kb) {
-            const size_t o = (size_t)row * ld + k + kk;
+        if (row < r1 && kk < K) {
+            const size_t o = (size_t)row * ld + kcol + kk;
             if (r < 64) v = second ? -Ai[o] : Ar[o];     // [ Lr  -Li ]
             else v = second ? Ar[o] : Ai[o];            // [ Li   Lr ]
         }
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const floa
         lo[off] = tf32_rna(v - h);
     }
     __syncthreads();
-    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * NCHUNK + chunk) * 2) * A_TILE);
+    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * A_TILE);
     const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
     for (int e = threadIdx.x; e < A_TILE / 4; e += 256) {
         dst[e] = h4[e];
@@ -92,8 +92,9 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int k, int kb, const floa
     }
 }
 
-__global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const float *__restrict__ planes,
-                                                size_t pstride, int ld, float *__restrict__ outb, size_t ostride,
+__global__ void __launch_bounds__(256) k_pack_b(int N, int c0, int c1, int krow, int K, int nchunk,
+                                                const float *__restrict__ planes, size_t pstride, int ld,
+                                                float *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
     extern __shared__ __align__(1024) float dynb[];
     float *hi = dynb, *lo = dynb + B_TILE;
@@ -102,16 +103,16 @@ __global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const floa
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     float *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
-    const int s = k + kb;
     for (int e = threadIdx.x; e < B_TILE; e += 256) {
         const int kq = e >> 8, n = e & 255;          // consecutive threads: consecutive columns
         const int kp = chunk * KC + kq;
-        const int kk = kp & 63;
-        const int col = s + tile * TN + n;
+        const bool second = kp >= K;
+        const int kk = second ? kp - K : kp;
+        const int col = c0 + tile * TN + n;
         float v = 0.f;
-        if (col < N && kk < kb) {
-            const size_t o = (size_t)(k + kk) * ld + col;
-            v = kp >= 64 ? Ai[o] : Ar[o];               // [ Ur ; Ui ]
+        if (col < c1 && kk < K) {
+            const size_t o = (size_t)(krow + kk) * ld + col;
+            v = second ? Ai[o] : Ar[o];                  // [ Ur ; Ui ]
         }
         const float h = tf32_rna(v);
         const uint32_t off = swz(n, kq) >> 2;
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(256) k_pack_b(int N, int k, int kb, const floa
         lo[off] = tf32_rna(v - h);
     }
     __syncthreads();
-    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * NCHUNK + chunk) * 2) * B_TILE);
+    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * B_TILE);
     const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
     for (int e = threadIdx.x; e < B_TILE / 4; e += 256) {
         dst[e] = h4[e];
@@ -212,11 +213,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // ---------------------------------------------------------------------------
 // The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float *__restrict__ Apackb,
-                                                      size_t astride, const float *__restrict__ Bpackb,
-                                                      size_t bstride, float *__restrict__ planes, size_t pstride,
-                                                      int ld, char *__restrict__ ctl,
-                                                      const int *__restrict__ active) {
+__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk,
+                                                      const float *__restrict__ Apackb, size_t astride,
+                                                      const float *__restrict__ Bpackb, size_t bstride,
+                                                      float *__restrict__ planes, size_t pstride, int ld,
+                                                      char *__restrict__ ctl, const int *__restrict__ active) {
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
@@ -248,8 +249,8 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float 
     bool ok = true;
     if (tid == 0) *ok_sh = 1;
     if (tid == 0) {
-        const float *ga = Apack + (size_t)tile_m * NCHUNK * 2 * A_TILE;
-        const float *gb = Bpack + (size_t)tile_n * NCHUNK * 2 * B_TILE;
+        const float *ga = Apack + (size_t)tile_m * nchunk * 2 * A_TILE;
+        const float *gb = Bpack + (size_t)tile_n * nchunk * 2 * B_TILE;
         const uint32_t bytes = sizeof(float) * (2 * A_TILE + 2 * B_TILE);
         auto load = [&](int c) {
             float *st = stage + (c % NSTAGE) * STAGE_FLOATS;
@@ -258,8 +259,8 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float 
             bulk_g2s(st + 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, sizeof(float) * 2 * B_TILE, &bars[c % NSTAGE]);
         };
         load(0);
-        load(1);
-        for (int c = 0; c < NCHUNK && ok; c++) {
+        if (nchunk > 1) load(1);
+        for (int c = 0; c < nchunk && ok; c++) {
             const int sidx = c % NSTAGE;
             const uint32_t phase = (c / NSTAGE) & 1;
             if (!mbar_wait(&bars[sidx], phase, err)) { ok = false; break; }
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float 
                 mma_tf32(tmem, ahi + adv, bhi + adv, 1u);
             }
             mma_commit(&bars[2 + sidx]);   // stage sidx free once these MMAs have read it
-            if (c + NSTAGE < NCHUNK) {
+            if (c + NSTAGE < nchunk) {
                 if (!mbar_wait(&bars[2 + sidx], phase, err)) { ok = false; break; }
                 load(c + NSTAGE);
             }
@@ -293,16 +294,16 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float 
     if (have) {
         const int half = warp & 1;                  // rows 0-31 or 32-63 of the complex block
         float *plane = (warp < 2) ? Ar : Ai;        // warps 0,1: real part; 2,3: imaginary part
-        const int row = s + tile_m * 64 + half * 32 + lane;
+        const int row = r0 + tile_m * 64 + half * 32 + lane;
         const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
         for (int j = 0; j < TN / 32; j++) {
             uint32_t v[32];
             tmem_ld32(tbase + j * 32, v);
-            const int col0 = s + tile_n * TN + j * 32;
-            if (row < N && col0 < N) {
+            const int col0 = c0 + tile_n * TN + j * 32;
+            if (row < r1 && col0 < c1) {
                 float *p = plane + (size_t)row * ld + col0;
-                if (col0 + 32 <= N) {
+                if (col0 + 32 <= c1) {
                     float4 *p4 = reinterpret_cast<float4 *>(p);
 #pragma unroll
                     for (int q = 0; q < 8; q++) {
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int s, const float 
                 } else {
 #pragma unroll
                     for (int q = 0; q < 32; q++)
-                        if (col0 + q < N) p[q] -= __uint_as_float(v[q]);
+                        if (col0 + q < c1) p[q] -= __uint_as_float(v[q]);
                 }
             }
         }
@@ -342,36 +343,47 @@ efie_status efie_tc_attrs() {
     return EFIE_OK;
 }
 
-// Tensor cores pay off once the trailing matrix spans a few tiles.
-static bool use_tc(int rest) { return !g_tc_disabled && rest >= 256; }
-
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
 
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact) {
-    const int N = w.N, s = k + kb, rest = N - s, B = w.B;
-    if (!use_tc(rest) || kb > NB) return efie_trailing_update_simt(ctx, w, k, kb, nact);
+// C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] for every
+// active frequency: tensor cores when the block spans enough work, CUDA cores
+// otherwise.
+efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
+                             int nact) {
+    const int rows = r1 - r0, cols = c1 - c0;
+    if (rows <= 0 || cols <= 0 || K <= 0) return EFIE_OK;
+    const bool tc = !g_tc_disabled && K <= KMAX && (double)rows * cols >= 64.0 * 256.0 && cols >= 96;
+    if (!tc) {
+        for (int k0 = 0; k0 < K; k0 += 64)
+            EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
+        return EFIE_OK;
+    }
     EFIE_TRY(efie_tc_attrs());
+    const int N = w.N, B = w.B;
     cudaStream_t st = ctx->stream;
-    const int mt = (rest + 63) / 64, nt = (rest + TN - 1) / TN;
-    // per-frequency staging sized for the first (largest) trailing matrix of an N x N LU
+    const int mt = (rows + 63) / 64, nt = (cols + TN - 1) / TN;
+    const int nchunk = (2 * K + KC - 1) / KC;
+    // per-frequency staging sized for the largest update of an N x N LU
     const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
-    const size_t astride = (size_t)mt0 * NCHUNK * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK * 2 * B_TILE;
+    const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
     EFIE_TRY(w.packA.reserve(sizeof(float) * astride * B));
     EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * B));
     float *planes = w.planes.as<float>();
     const int *active = w.active.as<int>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
-    k_pack_a<<<dim3(mt, NCHUNK, B), 256, 0, st>>>(N, k, kb, planes, w.pstride, w.ld, w.packA.as<float>(), astride,
-                                                  active);
-    k_pack_b<<<dim3(nt, NCHUNK, B), 256, sizeof(float) * 2 * B_TILE, st>>>(N, k, kb, planes, w.pstride, w.ld,
-                                                                          w.packB.as<float>(), bstride, active);
+    k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld,
+                                                  w.packA.as<float>(), astride, active);
+    k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(float) * 2 * B_TILE, st>>>(N, c0, c1, krow, K, nchunk, planes,
+                                                                          w.pstride, w.ld, w.packB.as<float>(),
+                                                                          bstride, active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
-    k_update_tc<<<dim3(nt, mt, B), 128, GEMM_SMEM, st>>>(N, s, w.packA.as<float>(), astride, w.packB.as<float>(),
-                                                         bstride, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
+    k_update_tc<<<dim3(nt, mt, B), 128, GEMM_SMEM, st>>>(N, r0, r1, c0, c1, nchunk, w.packA.as<float>(), astride,
+                                                         w.packB.as<float>(), bstride, planes, w.pstride, w.ld,
+                                                         w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rest * rest * kb * nact);
+    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;
 }

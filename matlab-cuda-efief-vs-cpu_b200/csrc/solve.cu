@@ -26,7 +26,7 @@
 
 namespace {
 
-constexpr int NB = 64;  // diagonal block size of the LU and the triangular solves
+constexpr int NB = 64;   // diagonal block size of the LU and the triangular solves
 constexpr size_t kTwoTiles = sizeof(float2) * 2 * NB * (NB + 1);
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
@@ -235,11 +235,12 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
 }
 
 // ---------------------------------------------------------------------------
-// Trailing update A22 -= L21 * U12 on CUDA cores (complex FP32), 64x64 tiles,
-// K = kb <= 64: small trailing matrices and the portable path.
+// C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] on CUDA
+// cores (complex FP32), 64x64 tiles, K <= 64: small blocks and the portable path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float *__restrict__ planes, size_t pstride,
-                                                     int ld, const int *__restrict__ active) {
+__global__ void __launch_bounds__(256) k_update_simt(int N, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
+                                                     float *__restrict__ planes, size_t pstride, int ld,
+                                                     const int *__restrict__ active) {
     const int f = blockIdx.z;
     if (!active[f]) return;
     extern __shared__ float2 dyn[];
@@ -247,31 +248,30 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float
     float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     const int tid = threadIdx.x;
-    const int s = k + kb;
-    const int row0 = s + blockIdx.y * NB, col0 = s + blockIdx.x * NB;
-    if (row0 >= N || col0 >= N) return;
+    const int row0 = r0 + blockIdx.y * NB, col0 = c0 + blockIdx.x * NB;
+    if (row0 >= r1 || col0 >= c1) return;
     for (int e = tid; e < NB * NB; e += 256) {
         const int i = e / NB, j = e % NB;
-        Ls[i][j] = (row0 + i < N && j < kb)
-                       ? make_float2(Ar[(size_t)(row0 + i) * ld + k + j], Ai[(size_t)(row0 + i) * ld + k + j])
+        Ls[i][j] = (row0 + i < r1 && j < K)
+                       ? make_float2(Ar[(size_t)(row0 + i) * ld + kcol + j], Ai[(size_t)(row0 + i) * ld + kcol + j])
                        : make_float2(0.f, 0.f);
-        Us[i][j] = (i < kb && col0 + j < N)
-                       ? make_float2(Ar[(size_t)(k + i) * ld + col0 + j], Ai[(size_t)(k + i) * ld + col0 + j])
+        Us[i][j] = (i < K && col0 + j < c1)
+                       ? make_float2(Ar[(size_t)(krow + i) * ld + col0 + j], Ai[(size_t)(krow + i) * ld + col0 + j])
                        : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    const int r0 = (tid >> 4) * 4, c0 = (tid & 15) * 4;
+    const int rr = (tid >> 4) * 4, cc = (tid & 15) * 4;
     float2 acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
-    for (int q = 0; q < kb; q++) {
+    for (int q = 0; q < K; q++) {
         float2 x[4], y[4];
 #pragma unroll
         for (int a = 0; a < 4; a++) {
-            x[a] = Ls[r0 + a][q];
-            y[a] = Us[q][c0 + a];
+            x[a] = Ls[rr + a][q];
+            y[a] = Us[q][cc + a];
         }
 #pragma unroll
         for (int a = 0; a < 4; a++)
@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int k, int kb, float
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-            const int i = row0 + r0 + a, j = col0 + c0 + b;
-            if (i < N && j < N) {
+            const int i = row0 + rr + a, j = col0 + cc + b;
+            if (i < r1 && j < c1) {
                 Ar[(size_t)i * ld + j] -= acc[a][b].x;
                 Ai[(size_t)i * ld + j] -= acc[a][b].y;
             }
@@ -444,8 +444,11 @@ efie_status set_smem_attrs() {
 
 int efie_solve_nb() { return NB; }
 
-efie_status efie_mixed_workspace(SolveWork &w, int N, int B) {
+efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(set_smem_attrs());
+    if (kb_outer != 64 && kb_outer != 128 && kb_outer != 256)
+        return efie_fail(EFIE_ERR_ARGS, "LU panel width must be 64, 128 or 256");
+    w.kb_outer = kb_outer;
     w.N = N;
     w.B = B;
     w.ld = (N + 63) / 64 * 64;
@@ -483,30 +486,47 @@ efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, s, tok, 24.0 * (double)N * N * nact);
     float2 *dinv = w.dinv.as<float2>();
-    for (int bi = 0; bi < w.nblk; bi++) {
-        const int k = bi * NB, kb = std::min(NB, N - k);
-        const int rest = N - k - kb;
-        tok = log.begin(s);
-        k_diag_factor<<<B, 1024, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
-        if (rest > 0) {
-            dim3 pg((rest + NB - 1) / NB, 2, B);
-            k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, active);
+    // Two-level blocking: outer panels of KB columns are factored with 64-wide
+    // diagonal blocks whose updates stay inside the panel's L-shaped region;
+    // the rest of the trailing matrix gets one update with K = KB.
+    const int KB = w.kb_outer;
+    for (int K0 = 0; K0 < N; K0 += KB) {
+        const int Kend = std::min(N, K0 + KB);
+        for (int k = K0; k < Kend; k += NB) {
+            const int bi = k / NB, kb = std::min(NB, N - k);
+            const int s1 = k + kb, rest = N - s1;
+            tok = log.begin(s);
+            k_diag_factor<<<B, 1024, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl,
+                                                     active);
+            if (rest > 0) {
+                dim3 pg((rest + NB - 1) / NB, 2, B);
+                k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, active);
+            }
+            EFIE_CUDA(cudaGetLastError());
+            log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
+            if (s1 < Kend) {
+                // rows of this panel below the block, every column to the right
+                EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact));
+                // rows below the panel, the panel's remaining columns
+                EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, s1, Kend, k, k, kb, nact));
+            }
         }
-        EFIE_CUDA(cudaGetLastError());
-        log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
-        if (rest > 0) EFIE_TRY(efie_trailing_update(ctx, w, k, kb, nact));
+        // the deferred trailing update with the whole panel
+        EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, Kend, N, K0, K0, Kend - K0, nact));
     }
     return EFIE_OK;
 }
 
-efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact) {
-    const int N = w.N, rest = N - k - kb;
-    dim3 g((rest + NB - 1) / NB, (rest + NB - 1) / NB, w.B);
+efie_status efie_update_simt(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
+                             int nact) {
+    const int N = w.N;
+    if (r1 <= r0 || c1 <= c0) return EFIE_OK;
+    dim3 g((c1 - c0 + NB - 1) / NB, (r1 - r0 + NB - 1) / NB, w.B);
     size_t tok = ctx->log.begin(ctx->stream);
-    k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, k, kb, w.planes.as<float>(), w.pstride, w.ld,
-                                                      w.active.as<int>());
+    k_update_simt<<<g, 256, kTwoTiles, ctx->stream>>>(N, r0, r1, c0, c1, kcol, krow, K, w.planes.as<float>(),
+                                                      w.pstride, w.ld, w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
-    ctx->log.end(EFIE_K_GEMM, ctx->stream, tok, 8.0 * (double)rest * rest * kb * nact);
+    ctx->log.end(EFIE_K_GEMM, ctx->stream, tok, 8.0 * (double)(r1 - r0) * (c1 - c0) * K * nact);
     return EFIE_OK;
 }
 

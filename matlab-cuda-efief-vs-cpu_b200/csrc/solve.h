@@ -13,6 +13,7 @@ struct SolveWork {
     size_t dstride = 0;       // float2 per frequency in `dinv`
     int vstride = 0;          // float2 per frequency in each vector of `vec`
     int grid = 0;             // CTAs of the triangular-solve grid
+    int kb_outer = 256;       // outer panel width of the two-level LU (K of the big updates)
     DevBuf planes;   // per f: float re[N][ld], im[N][ld]  (row-major)
     DevBuf dinv;     // per f: float2 [nblk][2][NB*NB] (L^-1, U^-1 of each diagonal block)
     DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]
@@ -30,7 +31,7 @@ struct RefineResult {
 };
 
 int efie_solve_nb();
-efie_status efie_mixed_workspace(SolveWork &w, int N, int B);
+efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer);
 efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host);
 efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
                               double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
@@ -41,8 +42,11 @@ efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const d
 efie_status efie_trsv_workspace(SolveWork &w);
 efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int epoch);
 
-// A22 -= L21 * U12 for the block at (k, kb) of every active frequency:
-// tensor cores when the trailing matrix is large enough, CUDA cores otherwise.
-efie_status efie_trailing_update(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact);
-efie_status efie_trailing_update_simt(efie_ctx *ctx, SolveWork &w, int k, int kb, int nact);
+// C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] for every
+// active frequency: tensor cores when the block is large enough (K <= 256),
+// CUDA cores otherwise (efie_update_simt, K <= 64 per call).
+efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
+                             int nact);
+efie_status efie_update_simt(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
+                             int nact);
 extern "C" void efie_debug_disable_tensor_cores(int disable);
