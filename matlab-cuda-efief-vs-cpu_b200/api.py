@@ -389,7 +389,11 @@ class SweepPlan:
         self._m = _Marshal()
         self._mesh = self._m.mesh(V, F, E, pt, mt, ps, ms, rp, rm, Ap, Am, ln)
         self._pp = self._m.prepack(pre, Nt) if pre is not None else None
-        self.opts = opts if opts is not None else sweep_opts()
+        if opts is None:
+            from .autotune import tuned_opts
+            t = tuned_opts(Ne)
+            opts = sweep_opts(batch=t[0], lu_nb=t[1]) if t else sweep_opts()
+        self.opts = opts
         h = C.c_void_p()
         nat.check(nat.lib().efie_plan_create(
             nat.context(), C.byref(self._mesh), C.byref(self._pp) if self._pp is not None else None,

@@ -253,14 +253,10 @@ __global__ void __launch_bounds__(256) k_self_moments(
 // ---------------------------------------------------------------------------
 // Gather: Z(m,n) = sum over the 4 triangle pairs of alpha Ivec + beta Isca,
 // in the reference's (im, in) order (kernel_Z_fastquad, fastquad.cu:373-409).
-// Thread per entry, m fastest (column-major Z, coalesced stores).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_gather_z(
-    int Ne, int Nt, bool sym, const int *__restrict__ etri, const double4 *__restrict__ ecd,
-    const double *__restrict__ mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
-    const int m = blockIdx.x * 64 + (threadIdx.x & 63);
-    const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
-    if (m >= Ne || n >= Ne) return;
+__device__ __forceinline__ double2 z_entry(int m, int n, int Ne, int Nt, bool sym, const int *__restrict__ etri,
+                                           const double4 *__restrict__ ecd, const double *__restrict__ mom,
+                                           double alr, double ali, double ber, double bei) {
     double zr = 0.0, zi = 0.0;
 #pragma unroll
     for (int a = 0; a < 2; a++) {
@@ -292,7 +288,45 @@ __global__ void __launch_bounds__(256) k_gather_z(
             zi += (alr * Ivi + ali * Ivr) + (ber * Isi + bei * Isr);
         }
     }
-    Z[(size_t)m + (size_t)Ne * n] = make_double2(zr, zi);
+    return make_double2(zr, zi);
+}
+
+// Thread per entry, m fastest (column-major Z, coalesced stores).
+__global__ void __launch_bounds__(256) k_gather_z(
+    int Ne, int Nt, bool sym, const int *__restrict__ etri, const double4 *__restrict__ ecd,
+    const double *__restrict__ mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+    const int m = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
+    if (m >= Ne || n >= Ne) return;
+    Z[(size_t)m + (size_t)Ne * n] = z_entry(m, n, Ne, Nt, sym, etri, ecd, mom, alr, ali, ber, bei);
+}
+
+// Symmetric Z (symmetric pair regimes): only 32x32 tiles with bm <= bn are
+// evaluated; an off-diagonal tile is also stored transposed through shared
+// memory, so Z(n,m) is a bit-exact copy of Z(m,n).
+__global__ void __launch_bounds__(256) k_gather_z_sym(
+    int Ne, int Nt, const int *__restrict__ etri, const double4 *__restrict__ ecd, const double *__restrict__ mom,
+    double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+    const int bm = blockIdx.x, bn = blockIdx.y;
+    if (bm > bn) return;
+    __shared__ double2 tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int m = bm * 32 + tx;
+    for (int j = ty; j < 32; j += 8) {
+        const int n = bn * 32 + j;
+        double2 z = make_double2(0.0, 0.0);
+        if (m < Ne && n < Ne) {
+            z = z_entry(m, n, Ne, Nt, true, etri, ecd, mom, alr, ali, ber, bei);
+            Z[(size_t)m + (size_t)Ne * n] = z;
+        }
+        tile[j][tx] = z;
+    }
+    if (bm == bn) return;
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        const int mm = bm * 32 + j, nn = bn * 32 + tx;
+        if (mm < Ne && nn < Ne) Z[(size_t)nn + (size_t)Ne * mm] = tile[tx][j];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -524,9 +558,15 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     }
     log.end(EFIE_K_NEARSELF, s, tok, qpe, nl);
     tok = log.begin(s);
-    dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
-    k_gather_z<<<gg, 256, 0, s>>>(Ne, Nt, g.symmetric, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr,
-                                  ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
+    if (g.symmetric) {
+        dim3 gs((Ne + 31) / 32, (Ne + 31) / 32);
+        k_gather_z_sym<<<gs, 256, 0, s>>>(Ne, Nt, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr, ph.ali,
+                                          ph.ber, ph.bei, static_cast<double2 *>(Z));
+    } else {
+        dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
+        k_gather_z<<<gg, 256, 0, s>>>(Ne, Nt, false, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr,
+                                      ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
+    }
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GATHER, s, tok, 16.0 * (double)Ne * Ne);
     return EFIE_OK;
