@@ -251,6 +251,130 @@ __global__ void __launch_bounds__(256) k_self_moments(
 }
 
 // ---------------------------------------------------------------------------
+// Extraction scheme (no reference counterpart): on self and vertex-adjacent
+// pairs G = 1/(4 pi R) + (exp(-jkR) - 1)/(4 pi R).  The static part is
+// integrated analytically over the inner triangle (potential integrals of
+// Wilton et al. 1984 / Graglia 1993) at every outer rule point, the smooth
+// part with the rule on both triangles.  One warp per pair (t1 <= t2).
+// ---------------------------------------------------------------------------
+// I0 = int_T 1/R dS', J = int_T (r' - r)/R dS' for triangle (a0, a1, a2).
+__device__ void potential_integrals(const double3 a0, const double3 a1, const double3 a2, const double3 r,
+                                    double &I0, double3 &J) {
+    const double3 A[3] = {a0, a1, a2};
+    double3 n = make_double3((a1.y - a0.y) * (a2.z - a0.z) - (a1.z - a0.z) * (a2.y - a0.y),
+                             (a1.z - a0.z) * (a2.x - a0.x) - (a1.x - a0.x) * (a2.z - a0.z),
+                             (a1.x - a0.x) * (a2.y - a0.y) - (a1.y - a0.y) * (a2.x - a0.x));
+    const double nn = sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+    n.x /= nn; n.y /= nn; n.z /= nn;
+    const double d = n.x * (r.x - a0.x) + n.y * (r.y - a0.y) + n.z * (r.z - a0.z);
+    const double ad = fabs(d);
+    const double3 rho = make_double3(r.x - d * n.x, r.y - d * n.y, r.z - d * n.z);
+    double s0 = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const double3 p = A[i], q = A[(i + 1) % 3];
+        double3 l = make_double3(q.x - p.x, q.y - p.y, q.z - p.z);
+        const double ll = sqrt(l.x * l.x + l.y * l.y + l.z * l.z);
+        l.x /= ll; l.y /= ll; l.z /= ll;
+        const double3 u = make_double3(l.y * n.z - l.z * n.y, l.z * n.x - l.x * n.z, l.x * n.y - l.y * n.x);
+        const double P0 = (p.x - rho.x) * u.x + (p.y - rho.y) * u.y + (p.z - rho.z) * u.z;
+        const double lp = (q.x - rho.x) * l.x + (q.y - rho.y) * l.y + (q.z - rho.z) * l.z;
+        const double lm = (p.x - rho.x) * l.x + (p.y - rho.y) * l.y + (p.z - rho.z) * l.z;
+        const double R02 = P0 * P0 + d * d;
+        const double Rp = sqrt(R02 + lp * lp), Rm = sqrt(R02 + lm * lm);
+        double f;
+        if (R02 < 1e-30 * (lp * lp + lm * lm)) {
+            f = 0.0;   // point on the edge line: the terms vanish
+        } else {
+            // f = log((Rp + lp)/(Rm + lm)); R + l = R02/(R - l) where l < 0 avoids the cancellation
+            const double np_ = lp >= 0.0 ? Rp + lp : R02 / (Rp - lp);
+            const double nm_ = lm >= 0.0 ? Rm + lm : R02 / (Rm - lm);
+            f = log(np_ / nm_);
+        }
+        double beta = 0.0;
+        if (ad > 0.0) beta = atan(P0 * lp / (R02 + ad * Rp)) - atan(P0 * lm / (R02 + ad * Rm));
+        s0 += P0 * f - ad * beta;
+        const double t = 0.5 * (R02 * f + lp * Rp - lm * Rm);
+        vx += u.x * t; vy += u.y * t; vz += u.z * t;
+    }
+    I0 = s0;
+    J = make_double3(vx - d * n.x * s0, vy - d * n.y * s0, vz - d * n.z * s0);
+}
+
+// (exp(-jkR) - 1)/(4 pi R) without cancellation; -jk/(4 pi) at R = 0
+__device__ __forceinline__ void smooth_green(double kr, double ki, double R, double &gr, double &gi) {
+    if (R == 0.0) {
+        gr = ki / (4.0 * kPi);
+        gi = -kr / (4.0 * kPi);
+        return;
+    }
+    double s, c, sh, ch;
+    sincos(kr * R, &s, &c);
+    sincos(0.5 * kr * R, &sh, &ch);
+    const double em = expm1(ki * R);
+    const double inv = 1.0 / (4.0 * kPi * R);
+    gr = (em * c - 2.0 * sh * sh) * inv;
+    gi = -(1.0 + em) * s * inv;
+}
+
+__global__ void __launch_bounds__(256) k_singular_moments(
+    int Nt, int n_pairs, const int2 *__restrict__ list, int NQ, const double4 *__restrict__ origin,
+    const double4 *__restrict__ pts, const double4 *__restrict__ vtx, double kr, double ki,
+    double *__restrict__ mom) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_pairs) return;
+    const int2 pr = list[warp];
+    const int t1 = pr.x, t2 = pr.y;   // t1 <= t2: outer t1, inner t2
+    const double4 o1 = origin[t1], o2 = origin[t2];
+    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
+    double m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = 0.0;
+    // static part: outer point p on t1, analytic over t2 (coordinates relative to o2)
+    if (lane < NQ) {
+        const double4 pp = pts[(size_t)t1 * NQ + lane];
+        const double3 r = make_double3(pp.x + dox, pp.y + doy, pp.z + doz);
+        const double4 v0 = vtx[3 * (size_t)t2], v1 = vtx[3 * (size_t)t2 + 1], v2 = vtx[3 * (size_t)t2 + 2];
+        double I0;
+        double3 J;
+        potential_integrals(make_double3(v0.x, v0.y, v0.z), make_double3(v1.x, v1.y, v1.z),
+                            make_double3(v2.x, v2.y, v2.z), r, I0, J);
+        // int rho' / R = J + (r - o2) I0   (rho' = r' - o2)
+        const double sx = J.x + r.x * I0, sy = J.y + r.y * I0, sz = J.z + r.z * I0;
+        const double w = pp.w / (4.0 * kPi);
+        m[0] += w * I0;
+        m[2] += w * I0 * pp.x; m[4] += w * I0 * pp.y; m[6] += w * I0 * pp.z;
+        m[8] += w * sx; m[10] += w * sy; m[12] += w * sz;
+        m[14] += w * (pp.x * sx + pp.y * sy + pp.z * sz);
+    }
+    // smooth part with the rule on both triangles
+    for (int e = lane; e < NQ * NQ; e += 32) {
+        const int p = e / NQ, q = e - p * NQ;
+        const double4 pp = pts[(size_t)t1 * NQ + p];
+        const double4 pq = pts[(size_t)t2 * NQ + q];
+        const double dx = dox + pp.x - pq.x, dy = doy + pp.y - pq.y, dz = doz + pp.z - pq.z;
+        const double R = sqrt(dx * dx + dy * dy + dz * dz);
+        double gr, gi;
+        smooth_green(kr, ki, R, gr, gi);
+        acc_qpe(m, pp, pq, gr, gi);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
+    if (t1 == t2) {
+        // self pair: numeric-outer / analytic-inner is not symmetric in the two
+        // sides; the mean of both orders (S1, S2 -> their average) keeps Z symmetric
+#pragma unroll
+        for (int i = 2; i < 8; i++) {
+            const double s = 0.5 * (m[i] + m[i + 6]);
+            m[i] = s;
+            m[i + 6] = s;
+        }
+    }
+    if (lane == 0) store_mom(mom + 16 * pair_slot(t1, t2, Nt, true), m);
+}
+
+// ---------------------------------------------------------------------------
 // Gather: Z(m,n) = sum over the 4 triangle pairs of alpha Ivec + beta Isca,
 // in the reference's (im, in) order (kernel_Z_fastquad, fastquad.cu:373-409).
 // ---------------------------------------------------------------------------
@@ -504,10 +628,56 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
             }
         g.n_near = (int)list.size();
         EFIE_TRY(up(g.near_list, list.data(), sizeof(int2) * (list.empty() ? 1 : list.size())));
+    } else if (scheme == EFIE_SCHEME_EXTRACT) {
+        // rule points of every triangle from V/F (map_ref_to_vertices.m form), weights times 2A
+        const int order = rule_order ? rule_order : EFIE_QUAD_DUNAVANT7;
+        double qu[7], qv[7], qw[7];
+        const int Nq = efie_quad_rule(order, qu, qv, qw);
+        g.Nq = Nq;
+        std::vector<double4> reg((size_t)Nt * Nq), vtx(3 * (size_t)Nt);
+        for (int t = 0; t < Nt; t++) {
+            double a[3][3];
+            for (int j = 0; j < 3; j++) {
+                const int v = mesh->F[t + (size_t)j * Nt] - 1;
+                for (int k = 0; k < 3; k++) a[j][k] = mesh->V[v + (size_t)k * Nv];
+            }
+            const double4 o = origin[t];
+            const double e1[3] = {a[1][0] - a[0][0], a[1][1] - a[0][1], a[1][2] - a[0][2]};
+            const double e2[3] = {a[2][0] - a[0][0], a[2][1] - a[0][1], a[2][2] - a[0][2]};
+            const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                         cz = e1[0] * e2[1] - e1[1] * e2[0];
+            const double a2 = std::sqrt(cx * cx + cy * cy + cz * cz);
+            for (int i = 0; i < Nq; i++)
+                reg[(size_t)t * Nq + i] = make_double4(a[0][0] + qu[i] * e1[0] + qv[i] * e2[0] - o.x,
+                                                       a[0][1] + qu[i] * e1[1] + qv[i] * e2[1] - o.y,
+                                                       a[0][2] + qu[i] * e1[2] + qv[i] * e2[2] - o.z, qw[i] * a2);
+            for (int j = 0; j < 3; j++) vtx[3 * (size_t)t + j] = make_double4(a[j][0] - o.x, a[j][1] - o.y, a[j][2] - o.z, 0.0);
+        }
+        EFIE_TRY(up(g.reg_pts, reg.data(), sizeof(double4) * reg.size()));
+        EFIE_TRY(up(g.tri_vtx, vtx.data(), sizeof(double4) * vtx.size()));
+        // self and vertex-adjacent pairs (t1 <= t2) through a vertex -> triangles map
+        std::vector<std::vector<int>> vt(Nv);
+        for (int t = 0; t < Nt; t++)
+            for (int j = 0; j < 3; j++) vt[mesh->F[t + (size_t)j * Nt] - 1].push_back(t);
+        std::vector<int2> list;
+        std::vector<int> seen(Nt, -1);
+        for (int t1 = 0; t1 < Nt; t1++) {
+            for (int j = 0; j < 3; j++)
+                for (int t2 : vt[mesh->F[t1 + (size_t)j * Nt] - 1])
+                    if (t2 >= t1 && seen[t2] != t1) {
+                        seen[t2] = t1;
+                        list.push_back(make_int2(t1, t2));
+                        mask[(size_t)t1 + (size_t)Nt * t2] = 1;
+                        mask[(size_t)t2 + (size_t)Nt * t1] = 1;
+                    }
+        }
+        g.symmetric = true;
+        g.n_adj = (int)list.size();
+        g.n_near = 0;
+        EFIE_TRY(up(g.adj_list, list.data(), sizeof(int2) * (list.empty() ? 1 : list.size())));
     } else {
-        return efie_fail(EFIE_ERR_ARGS, "scheme not available in this build");
+        return efie_fail(EFIE_ERR_ARGS, "unknown scheme");
     }
-    (void)rule_order;
     EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
     EFIE_TRY(g.moments.reserve(sizeof(double) * 16 * g.npairs));
@@ -524,7 +694,8 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     const uint8_t *skip = g.near_mask.as<uint8_t>();
     // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
     const double all = g.symmetric ? 0.5 * (double)Nt * (Nt + 1) : (double)Nt * Nt;
-    const double n_regular = all - (double)g.n_near - (double)Nt;
+    const double n_regular = g.scheme == EFIE_SCHEME_EXTRACT ? all - (double)g.n_adj
+                                                             : all - (double)g.n_near - (double)Nt;
     size_t tok = log.begin(s);
     switch (g.Nq) {
     case 1: k_regular_moments<1><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
@@ -539,6 +710,13 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     tok = log.begin(s);
     int nl = 0;
     double qpe = 0;
+    if (g.scheme == EFIE_SCHEME_EXTRACT) {
+        k_singular_moments<<<(g.n_adj + 7) / 8, 256, 0, s>>>(Nt, g.n_adj, g.adj_list.as<int2>(), g.Nq, org,
+                                                            g.reg_pts.as<double4>(), g.tri_vtx.as<double4>(), ph.kr,
+                                                            ph.ki, mom);
+        EFIE_CUDA(cudaGetLastError());
+        log.end(EFIE_K_NEARSELF, s, tok, (double)g.n_adj * g.Nq * (g.Nq + 1), 1);
+    } else {
     if (g.n_near > 0) {
         const int P = g.NsN * g.Nq2;
         k_near_moments<<<(g.n_near + 7) / 8, 256, 0, s>>>(Nt, g.symmetric, g.n_near, g.near_list.as<int2>(), P, org,
@@ -557,6 +735,7 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
         qpe += (double)Nt * P * P;
     }
     log.end(EFIE_K_NEARSELF, s, tok, qpe, nl);
+    }
     tok = log.begin(s);
     if (g.symmetric) {
         dim3 gs((Ne + 31) / 32, (Ne + 31) / 32);

@@ -294,3 +294,209 @@ int oracle_assemble_centroid(int Nv, int Nt, int Ne, const double *V, const int3
     free(side);
     return 0;
 }
+
+/* ====================================================================== */
+/* Extraction scheme (no reference counterpart): Dunavant 7-point rule on   */
+/* every triangle; on self and vertex-adjacent pairs the kernel is split as */
+/* G = 1/(4 pi R) + (exp(-jkR) - 1)/(4 pi R): the first term integrated     */
+/* analytically over the inner triangle (Wilton et al. 1984; Graglia 1993), */
+/* the second (smooth) term by the 7x7 rule.  For a pair the outer triangle */
+/* is the lower index, the inner the higher, so Z is symmetric.             */
+/* ====================================================================== */
+
+/* I0 = int_T 1/R dS', J = int_T (r' - r)/R dS' for the triangle a[0..2]. */
+void oracle_potential_integrals(const double a[3][3], const double r[3], double *I0, double J[3]) {
+    double e1[3], e2[3], n[3];
+    for (int c = 0; c < 3; c++) { e1[c] = a[1][c] - a[0][c]; e2[c] = a[2][c] - a[0][c]; }
+    n[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    n[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    n[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    for (int c = 0; c < 3; c++) n[c] /= nn;
+    double d = n[0] * (r[0] - a[0][0]) + n[1] * (r[1] - a[0][1]) + n[2] * (r[2] - a[0][2]);
+    double ad = fabs(d);
+    double rho[3] = { r[0] - d * n[0], r[1] - d * n[1], r[2] - d * n[2] };
+    double s0 = 0.0, v[3] = { 0.0, 0.0, 0.0 };
+    for (int i = 0; i < 3; i++) {
+        const double *p = a[i], *q = a[(i + 1) % 3];
+        double l[3] = { q[0] - p[0], q[1] - p[1], q[2] - p[2] };
+        double ll = sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
+        for (int c = 0; c < 3; c++) l[c] /= ll;
+        double u[3] = { l[1] * n[2] - l[2] * n[1], l[2] * n[0] - l[0] * n[2], l[0] * n[1] - l[1] * n[0] };
+        double P0 = (p[0] - rho[0]) * u[0] + (p[1] - rho[1]) * u[1] + (p[2] - rho[2]) * u[2];
+        double lp = (q[0] - rho[0]) * l[0] + (q[1] - rho[1]) * l[1] + (q[2] - rho[2]) * l[2];
+        double lm = (p[0] - rho[0]) * l[0] + (p[1] - rho[1]) * l[1] + (p[2] - rho[2]) * l[2];
+        double R02 = P0 * P0 + d * d;
+        double Rp = sqrt(R02 + lp * lp), Rm = sqrt(R02 + lm * lm);
+        double f;
+        if (R02 < 1e-30 * (lp * lp + lm * lm)) f = 0.0;            /* r on the edge line: terms vanish */
+        else {
+            /* f = log((Rp + lp)/(Rm + lm)); R + l = R02/(R - l) where l < 0 avoids the cancellation */
+            double np_ = lp >= 0.0 ? Rp + lp : R02 / (Rp - lp);
+            double nm_ = lm >= 0.0 ? Rm + lm : R02 / (Rm - lm);
+            f = log(np_ / nm_);
+        }
+        double beta = 0.0;
+        if (ad > 0.0) beta = atan(P0 * lp / (R02 + ad * Rp)) - atan(P0 * lm / (R02 + ad * Rm));
+        s0 += P0 * f - ad * beta;
+        double t = R02 * f + lp * Rp - lm * Rm;
+        for (int c = 0; c < 3; c++) v[c] += 0.5 * u[c] * t;
+    }
+    *I0 = s0;
+    for (int c = 0; c < 3; c++) J[c] = v[c] - d * n[c] * s0;
+}
+
+/* (exp(-jkR) - 1)/(4 pi R) without cancellation; its limit -jk/(4 pi) at R = 0 */
+static inline cplx smooth_green(double kr, double ki, double R) {
+    cplx g;
+    if (R == 0.0) { g.re = ki / (4.0 * PI_D); g.im = -kr / (4.0 * PI_D); return g; }
+    double ph = kr * R, s = sin(ph), h = sin(0.5 * ph);
+    double em = expm1(ki * R), e = 1.0 + em;
+    /* e^{kiR}(cos - j sin) - 1 = em*cos + (cos - 1) - j e sin, cos - 1 = -2 sin^2(ph/2) */
+    double c = cos(ph);
+    g.re = (em * c - 2.0 * h * h) / (4.0 * PI_D * R);
+    g.im = (-e * s) / (4.0 * PI_D * R);
+    return g;
+}
+
+typedef struct {
+    int Nv, Nt, Ne;
+    const double *V; const int32_t *F;
+    const int32_t *plusTri, *minusTri, *plusSign, *minusSign;
+    const double *rp, *rm, *Ap, *Am, *len;
+    double qu[7], qv[7], qw[7];
+    int nq;
+} ext_in;
+
+static void tri_vertices(const ext_in *in, int t, double a[3][3]) {
+    for (int j = 0; j < 3; j++) {
+        int v = in->F[t + (size_t)j * in->Nt] - 1;
+        for (int c = 0; c < 3; c++) a[j][c] = in->V[v + (size_t)c * in->Nv];
+    }
+}
+
+/* rule points of triangle t (map_ref_to_vertices.m) and weights times 2A */
+static void tri_points(const ext_in *in, int t, double pts[7][3], double w[7]) {
+    double a[3][3];
+    tri_vertices(in, t, a);
+    double e1[3], e2[3];
+    for (int c = 0; c < 3; c++) { e1[c] = a[1][c] - a[0][c]; e2[c] = a[2][c] - a[0][c]; }
+    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+    double a2 = sqrt(cx * cx + cy * cy + cz * cz);
+    for (int i = 0; i < in->nq; i++) {
+        for (int c = 0; c < 3; c++) pts[i][c] = a[0][c] + in->qu[i] * e1[c] + in->qv[i] * e2[c];
+        w[i] = in->qw[i] * a2;
+    }
+}
+
+static int share_vertex(const ext_in *in, int t1, int t2) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            if (in->F[t1 + (size_t)i * in->Nt] == in->F[t2 + (size_t)j * in->Nt]) return 1;
+    return 0;
+}
+
+/* RWG basis of edge m on triangle t (1-based): f = c (r - v), div = 2c */
+static void basis(const ext_in *in, int m, int t, double *c, double v[3]) {
+    int Ne = in->Ne;
+    if (t == in->plusTri[m]) {
+        *c = in->plusSign[m] * (in->len[m] / (2.0 * in->Ap[m]));
+        for (int k = 0; k < 3; k++) v[k] = in->rp[m + k * Ne];
+    } else {
+        *c = -in->minusSign[m] * (in->len[m] / (2.0 * in->Am[m]));
+        for (int k = 0; k < 3; k++) v[k] = in->rm[m + k * Ne];
+    }
+}
+
+/* Ivec, Isca of edges mo (outer triangle to) and mi (inner triangle ti) */
+static void pair_extract(const ext_in *in, int mo, int to, int mi, int ti, double kr, double ki,
+                         cplx *Iv, cplx *Is) {
+    double po[7][3], wo[7], pi_[7][3], wi[7];
+    tri_points(in, to - 1, po, wo);
+    tri_points(in, ti - 1, pi_, wi);
+    double co, vo[3], ci, vi[3];
+    basis(in, mo, to, &co, vo);
+    basis(in, mi, ti, &ci, vi);
+    int sing = (to == ti) || share_vertex(in, to - 1, ti - 1);
+    double at[3][3];
+    tri_vertices(in, ti - 1, at);
+    for (int p = 0; p < in->nq; p++) {
+        double fo[3] = { co * (po[p][0] - vo[0]), co * (po[p][1] - vo[1]), co * (po[p][2] - vo[2]) };
+        double dvo = 2.0 * co;
+        if (sing) {
+            double I0, J[3];
+            oracle_potential_integrals(at, po[p], &I0, J);
+            /* int f_i / R = c_i (J + (r - v_i) I0), int div_i / R = 2 c_i I0 */
+            double g[3] = { ci * (J[0] + (po[p][0] - vi[0]) * I0), ci * (J[1] + (po[p][1] - vi[1]) * I0),
+                            ci * (J[2] + (po[p][2] - vi[2]) * I0) };
+            Iv->re += wo[p] * (fo[0] * g[0] + fo[1] * g[1] + fo[2] * g[2]) / (4.0 * PI_D);
+            Is->re += wo[p] * dvo * (2.0 * ci * I0) / (4.0 * PI_D);
+        }
+        for (int q = 0; q < in->nq; q++) {
+            double fi[3] = { ci * (pi_[q][0] - vi[0]), ci * (pi_[q][1] - vi[1]), ci * (pi_[q][2] - vi[2]) };
+            double R = dist3(po[p], pi_[q]);
+            cplx G;
+            if (sing) G = smooth_green(kr, ki, R);
+            else G = cexpj_green(kr, ki, R < 1e-15 ? 1e-15 : R);
+            double w = wo[p] * wi[q];
+            double ff = fo[0] * fi[0] + fo[1] * fi[1] + fo[2] * fi[2], dd = dvo * 2.0 * ci;
+            Iv->re += G.re * (w * ff); Iv->im += G.im * (w * ff);
+            Is->re += G.re * (w * dd); Is->im += G.im * (w * dd);
+        }
+    }
+}
+
+int oracle_assemble_z_extract(int Nv, int Nt, int Ne, const double *V, const int32_t *F,
+                              const int32_t *plusTri, const int32_t *minusTri,
+                              const int32_t *plusSign, const int32_t *minusSign,
+                              const double *rp, const double *rm, const double *Ap, const double *Am,
+                              const double *len, int nq, const double *qu, const double *qv, const double *qw,
+                              double k_re, double k_im, double omega, double mu, double eps_re, double eps_im,
+                              int col0, int col1, double *Z, int nthreads) {
+    ext_in in = { Nv, Nt, Ne, V, F, plusTri, minusTri, plusSign, minusSign, rp, rm, Ap, Am, len,
+                  {0}, {0}, {0}, nq };
+    if (nq > 7) return -1;
+    for (int i = 0; i < nq; i++) { in.qu[i] = qu[i]; in.qv[i] = qv[i]; in.qw[i] = qw[i]; }
+    double al_im = omega * mu;
+    double dre = -omega * eps_im, dim = omega * eps_re, d2 = dre * dre + dim * dim;
+    double be_re = dre / d2, be_im = -dim / d2;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int n = col0; n < col1; n++) {
+        int tn[2] = { plusTri[n], minusTri[n] };
+        for (int m = 0; m < Ne; m++) {
+            int tm[2] = { plusTri[m], minusTri[m] };
+            double zr = 0.0, zi = 0.0;
+            for (int a = 0; a < 2; a++) {
+                if (tm[a] == 0) continue;
+                for (int b = 0; b < 2; b++) {
+                    if (tn[b] == 0) continue;
+                    cplx Iv = { 0, 0 }, Is = { 0, 0 };
+                    if (tm[a] == tn[b]) {
+                        /* self pair: the outer-numeric / inner-analytic split is not symmetric in
+                           the two basis functions; the mean of both orders keeps Z symmetric */
+                        cplx Iv2 = { 0, 0 }, Is2 = { 0, 0 };
+                        pair_extract(&in, m, tm[a], n, tn[b], k_re, k_im, &Iv, &Is);
+                        pair_extract(&in, n, tn[b], m, tm[a], k_re, k_im, &Iv2, &Is2);
+                        Iv.re = 0.5 * (Iv.re + Iv2.re); Iv.im = 0.5 * (Iv.im + Iv2.im);
+                        Is.re = 0.5 * (Is.re + Is2.re); Is.im = 0.5 * (Is.im + Is2.im);
+                    } else if (tm[a] < tn[b]) {
+                        pair_extract(&in, m, tm[a], n, tn[b], k_re, k_im, &Iv, &Is);
+                    } else {
+                        pair_extract(&in, n, tn[b], m, tm[a], k_re, k_im, &Iv, &Is);
+                    }
+                    zr += -al_im * Iv.im + be_re * Is.re - be_im * Is.im;
+                    zi += al_im * Iv.re + be_re * Is.im + be_im * Is.re;
+                }
+            }
+            size_t o = 2 * ((size_t)m + (size_t)Ne * n);
+            Z[o] = zr;
+            Z[o + 1] = zi;
+        }
+    }
+    return 0;
+}

@@ -577,3 +577,71 @@ def solve_sweep(prob, freqs=None, assemble=None):
         Ip = port_current(x, prob["wP"], prob["wG"], prob["rwg"]["len"])
         Zin[i], S11[i] = zin_s11(Ip, d.V0, d.Z0)
     return Zin, S11
+
+
+# ---------------------------------------------------------------------------
+# Extraction scheme (no reference counterpart): numerical checks of the
+# analytic potential integrals used by the C oracle and the product.
+# ---------------------------------------------------------------------------
+def _graded_gauss(s0, width, order):
+    """Composite Gauss-Legendre rule on [0, 1] whose panels shrink
+    geometrically towards s0 down to `width`, for integrands with a
+    near-singularity of that width at s0."""
+    edges = {0.0, 1.0}
+    s0 = min(max(s0, 0.0), 1.0)
+    edges.add(s0)
+    h = max(width, 1e-15)
+    while h < 1.0:
+        for e in (s0 - h, s0 + h):
+            if 0.0 < e < 1.0:
+                edges.add(e)
+        h *= 3.0
+    edges = sorted(edges)
+    x, w = np.polynomial.legendre.leggauss(order)
+    xs, ws = [], []
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        if hi - lo <= 0.0:
+            continue
+        xs.append(lo + 0.5 * (x + 1.0) * (hi - lo))
+        ws.append(0.5 * w * (hi - lo))
+    return np.concatenate(xs), np.concatenate(ws)
+
+
+def potential_integrals_numeric(a, r, order=24):
+    """I0 = int_T 1/R dS', J = int_T (r' - r)/R dS' by Duffy-transformed
+    Gauss-Legendre quadrature on the three sub-triangles with apex at the
+    projection rho of r.  After the transform the radial variable U carries a
+    near-singularity of width |d|/|q| at U = 0 (d = height of r over the plane)
+    and the edge variable V one of width dist(rho, edge)/|edge| at the foot of
+    the perpendicular; both are resolved by geometrically graded composite
+    rules, so the reference converges for points near edges and vertices."""
+    a = np.asarray(a, dtype=np.float64)
+    r = np.asarray(r, dtype=np.float64)
+    n = np.cross(a[1] - a[0], a[2] - a[0])
+    n /= np.linalg.norm(n)
+    d = np.dot(r - a[0], n)
+    rho = r - d * n
+    I0 = 0.0
+    J = np.zeros(3)
+    for i in range(3):
+        b, c = a[i], a[(i + 1) % 3]
+        e = c - b
+        cr = np.cross(b - rho, e)
+        area2 = np.dot(cr, n)          # signed: sub-triangles outside the edge subtract
+        if abs(area2) < 1e-300:
+            continue
+        le = np.linalg.norm(e)
+        s0 = np.dot(rho - b, e) / (le * le)
+        hdist = abs(area2) / le
+        v, wv = _graded_gauss(s0, hdist / le, order)
+        qmin = max(hdist, 1e-300)
+        u, wu = _graded_gauss(0.0, max(abs(d) / (qmin + np.linalg.norm(b - rho) + le), 1e-9), order)
+        U, Vv = np.meshgrid(u, v, indexing="ij")
+        W = np.outer(wu, wv)
+        # r' - r = (rho - r) + U q(V), formed without the cancellation of r' - r
+        dv = (rho - r)[None, None, :] + U[..., None] * ((b - rho)[None, None, :] + Vv[..., None] * e[None, None, :])
+        R = np.sqrt((dv ** 2).sum(-1))
+        jac = U * area2
+        I0 += np.sum(W * jac / R)
+        J += np.einsum("ij,ijc->c", W * jac / R, dv)
+    return I0, J

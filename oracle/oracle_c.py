@@ -97,3 +97,44 @@ def assemble_centroid(V, F, rwg, self_alpha, k, omega, mu, eps, nthreads=0):
     if rc != 0:
         raise RuntimeError("oracle_assemble_centroid failed: %d" % rc)
     return Z
+
+
+def potential_integrals(a, r):
+    """Analytic I0, J of the C oracle (oracle_potential_integrals)."""
+    L = lib()
+    aa = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(3, 3))
+    rr = np.ascontiguousarray(np.asarray(r, dtype=np.float64).reshape(3))
+    I0 = C.c_double()
+    J = np.zeros(3)
+    L.oracle_potential_integrals(_p(aa, C.c_double), _p(rr, C.c_double), C.byref(I0), _p(J, C.c_double))
+    return I0.value, J
+
+
+def assemble_z_extract(V, F, rwg, k, omega, mu, eps, rule=-7, col0=0, col1=None, nthreads=0):
+    """Z of the extraction scheme (Dunavant 7-point rule by default)."""
+    import efie_oracle as eo
+    qp, qw = eo.tri_quad_rule(rule)
+    Ne = int(rwg["Ne"])
+    col1 = Ne if col1 is None else col1
+    Vf = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(-1, order="F"))
+    Ff = np.ascontiguousarray(np.asarray(F, dtype=np.int32).reshape(-1, order="F"))
+    i32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(-1, order="F"))
+    f64 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F"))
+    pt, mt, ps, ms = (i32(rwg[x]) for x in ("plusTri", "minusTri", "plusSign", "minusSign"))
+    rp, rm, Ap, Am, ln = (f64(rwg[x]) for x in ("rp", "rm", "Ap", "Am", "len"))
+    qu, qv, qww = (np.ascontiguousarray(x, dtype=np.float64) for x in (qp[:, 0], qp[:, 1], qw))
+    Z = np.zeros((Ne, Ne), dtype=np.complex128, order="F")
+    k = complex(k)
+    eps = complex(eps)
+    L = lib()
+    rc = L.oracle_assemble_z_extract(
+        C.c_int(np.asarray(V).shape[0]), C.c_int(np.asarray(F).shape[0]), C.c_int(Ne), _p(Vf, C.c_double),
+        _p(Ff, C.c_int32), _p(pt, C.c_int32), _p(mt, C.c_int32), _p(ps, C.c_int32), _p(ms, C.c_int32),
+        _p(rp, C.c_double), _p(rm, C.c_double), _p(Ap, C.c_double), _p(Am, C.c_double), _p(ln, C.c_double),
+        C.c_int(len(qw)), _p(qu, C.c_double), _p(qv, C.c_double), _p(qww, C.c_double),
+        C.c_double(k.real), C.c_double(k.imag), C.c_double(omega), C.c_double(mu), C.c_double(eps.real),
+        C.c_double(eps.imag), C.c_int(col0), C.c_int(col1), Z.ctypes.data_as(C.POINTER(C.c_double)),
+        C.c_int(nthreads))
+    if rc != 0:
+        raise RuntimeError("oracle_assemble_z_extract failed: %d" % rc)
+    return Z
