@@ -47,6 +47,9 @@ WORKLOADS = {
     "cfg1": dict(Lp=30e-3, Wp=38e-3, Lg=60e-3, Wg=60e-3, h=1.6e-3, Np=(12, 10), Ng=(16, 16),
                  freqs=(2.0e9, 3.0e9, 11)),
 }
+RULE = {"ref": 0, "extract": -7}
+SCHEME_NAME = {"ref": "reference cached subdivision + softening (GPU option set)",
+               "extract": "Dunavant 7-point rule + analytic 1/R extraction on self/vertex-adjacent pairs"}
 # The reference's GPU option set (main_patch_gpu_mex_sweep_l.m:50-56).
 OPTS_REF_GPU = dict(quad_order=2, near_sing_eps=1.2, self_subdiv=2, self_alpha=0.20, near_subdiv=1,
                     near_alpha=0.15, near_order=2)
@@ -293,8 +296,11 @@ def run_ours(args):
     inp = build_inputs(m, args.workload)
     freqs = inp["freqs"]
     B = args.batch or len(freqs)
-    opts = m.sweep_opts(solver=args.solver, timing=True)
-    plan = m.SweepPlan(*inp["args"], *inp["tail"], opts=opts)
+    opts = m.sweep_opts(solver=args.solver, timing=True, scheme=args.scheme)
+    pargs = list(inp["args"])
+    if args.scheme == "extract":
+        pargs[-1] = None   # no prepack: the rule points come from the mesh
+    plan = m.SweepPlan(*pargs, *inp["tail"], opts=opts, rule_order=RULE[args.scheme])
 
     def batch(step):
         # each rank sweeps its own frequency points (replicas)
@@ -343,7 +349,14 @@ def run_ours(args):
     for s in range(max(1, args.steps)):
         fr = batch(args.warmup + s)
         t0 = time.perf_counter()
-        m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver))
+        if args.scheme == "ref":
+            m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver))
+        else:
+            # plan create (host mesh upload) + run + destroy through the C ABI
+            p2 = m.SweepPlan(*pargs, *inp["tail"], opts=m.sweep_opts(solver=args.solver, scheme="extract"),
+                             rule_order=RULE[args.scheme])
+            p2.run(fr)
+            p2.close()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e = sum(e2e_ms)
     if dist:
@@ -360,7 +373,7 @@ def run_ours(args):
                     else "c128", data="synthetic",
                     config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=B,
                                 solver=args.solver, parallelism="replicas x%d" % world,
-                                scheme="reference cached subdivision + softening (GPU option set)",
+                                scheme=SCHEME_NAME[args.scheme],
                                 l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
                     e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
                              d2h_bytes_per_step=2 * 16 * B),
@@ -389,6 +402,9 @@ def main():
     ap.add_argument("--workload", choices=list(WORKLOADS), default="cfg2")
     ap.add_argument("--batch", type=int, default=0, help="frequency points per step (0 = the whole sweep)")
     ap.add_argument("--solver", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--scheme", choices=["ref", "extract"], default="ref",
+                    help="ref: the reference's cached subdivision + softening; extract: Dunavant 7-point rule "
+                         "+ analytic 1/R extraction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

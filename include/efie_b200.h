@@ -318,6 +318,59 @@ efie_status efie_gassemble_zv_noalloc(int device, void *stream, int32_t Nv, int3
                                       const double *len, efie_c128 k, double omega, double mu, efie_c128 eps,
                                       const double exc[5], efie_c128 *Z, efie_c128 *Vrhs);
 
+/* ---------------------------------------------------------------------- */
+/* Surrogate MLP for adaptive sweeps                                       */
+/* ---------------------------------------------------------------------- */
+/* No counterpart in the reference.  A multilayer perceptron from normalised
+ * (geometry, frequency) features to the normalised Zin, trained and evaluated
+ * by the library's own CUDA kernels: n_layers hidden layers of width n_hidden
+ * with SiLU, a linear output layer; BF16 weight matrices with FP32
+ * accumulation in every layer, FP32 biases, activations and gradients, Adam
+ * on FP32 master weights.  One training step (minibatch gather, forward, MSE
+ * loss, backward, Adam) runs as one captured CUDA graph.
+ *
+ * Parameter vector (get/set_params, loss_grad): for each linear layer
+ * l = 0..n_layers, W_l [out_l x in_l] row-major then b_l [out_l]; in_0 = n_in,
+ * out_{n_layers} = n_out, every other width n_hidden.  X is [n x n_in] and
+ * T, Y are [n x n_out], row-major FP32 host arrays. */
+#define EFIE_MLP_MAX_LAYERS 8
+
+typedef struct efie_mlp efie_mlp;
+
+typedef struct efie_mlp_config {
+    int32_t n_in;       /* default 5: W, L, h, feed offset, frequency */
+    int32_t n_hidden;   /* default 256 */
+    int32_t n_layers;   /* hidden layers, default 4 (<= EFIE_MLP_MAX_LAYERS) */
+    int32_t n_out;      /* default 2: Re, Im */
+    uint64_t seed;      /* initial weights: uniform(-1/sqrt(in), 1/sqrt(in)) */
+} efie_mlp_config;
+
+typedef struct efie_adam_opts {
+    float lr, beta1, beta2, eps, weight_decay;   /* 1e-3, 0.9, 0.999, 1e-8, 0 */
+    int32_t batch;                               /* minibatch rows, default 1024 */
+    int32_t epochs;                              /* default 100 */
+    uint64_t seed;                               /* minibatch shuffling */
+} efie_adam_opts;
+
+void efie_mlp_config_default(efie_mlp_config *cfg);
+void efie_adam_opts_default(efie_adam_opts *opts);
+efie_status efie_mlp_create(efie_ctx *ctx, const efie_mlp_config *cfg, efie_mlp **out);
+void efie_mlp_destroy(efie_mlp *mlp);
+int64_t efie_mlp_num_params(const efie_mlp *mlp);
+efie_status efie_mlp_get_params(efie_mlp *mlp, float *params);
+/* Also resets Adam's moments and step count. */
+efie_status efie_mlp_set_params(efie_mlp *mlp, const float *params);
+efie_status efie_mlp_forward(efie_mlp *mlp, const float *X, int32_t n, float *Y);
+/* loss = mean over the n x n_out entries of (Y - T)^2 and its gradient with
+ * respect to the parameter vector (either output may be NULL). */
+efie_status efie_mlp_loss_grad(efie_mlp *mlp, const float *X, const float *T, int32_t n, double *loss,
+                               float *grad);
+/* opts->epochs passes over the n samples in shuffled minibatches of
+ * opts->batch rows (floor(n / batch) per epoch); loss_history (may be NULL)
+ * receives each epoch's mean minibatch loss. */
+efie_status efie_mlp_train(efie_mlp *mlp, const float *X, const float *T, int32_t n, const efie_adam_opts *opts,
+                           double *loss_history);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,7 +113,27 @@ SIGNATURES = {
     "efie_debug_disable_tensor_cores": (None, [C.c_int]),
     "efie_gassemble_zv_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_int32] + [_P] * 12 +
                                   [c128, C.c_double, C.c_double, c128, c_double_p, _P, _P]),
+    "efie_mlp_config_default": (None, [_P]),
+    "efie_adam_opts_default": (None, [_P]),
+    "efie_mlp_create": (C.c_int, [_P, _P, C.POINTER(_P)]),
+    "efie_mlp_destroy": (None, [_P]),
+    "efie_mlp_num_params": (C.c_int64, [_P]),
+    "efie_mlp_get_params": (C.c_int, [_P, _P]),
+    "efie_mlp_set_params": (C.c_int, [_P, _P]),
+    "efie_mlp_forward": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "efie_mlp_loss_grad": (C.c_int, [_P, _P, _P, C.c_int32, _P, _P]),
+    "efie_mlp_train": (C.c_int, [_P, _P, _P, C.c_int32, _P, _P]),
 }
+
+
+class EfieMlpConfig(C.Structure):
+    _fields_ = [("n_in", C.c_int32), ("n_hidden", C.c_int32), ("n_layers", C.c_int32), ("n_out", C.c_int32),
+                ("seed", C.c_uint64)]
+
+
+class EfieAdamOpts(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float), ("batch", C.c_int32), ("epochs", C.c_int32), ("seed", C.c_uint64)]
 
 NOALLOC_MAX_NE = 16384
 NOALLOC_MAX_NT = 16384

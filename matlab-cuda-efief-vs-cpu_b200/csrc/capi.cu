@@ -221,17 +221,6 @@ efie_status check_eps(double omega, efie_c128 eps) {
     return EFIE_OK;
 }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
-
 }  // namespace
 
 // ---------------------------------------------------------------------------

@@ -30,6 +30,23 @@ int efie_quad_rule(int order, double *u, double *v, double *w);
         if (s_ != EFIE_OK) return s_;          \
     } while (0)
 
+inline efie_status efie_cuda_check(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return EFIE_OK;
+    return efie_fail(EFIE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Makes `dev` current for the lifetime of the guard.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 // A device allocation owned by a context or plan; grows, never shrinks.
 struct DevBuf {
     void *p = nullptr;

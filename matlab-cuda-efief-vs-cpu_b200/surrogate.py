@@ -1,0 +1,324 @@
+"""Surrogate-guided adaptive frequency sweeps for families of patch designs.
+
+No counterpart in the reference (its drivers sweep a fixed frequency list).
+Pieces:
+
+* ``PatchDesign`` / ``sample_designs``: parametric patch-over-ground designs
+  (W, L, h, feed offset) meshed with the library's own producers;
+* ``Surrogate``: the MLP of ``csrc/surrogate.cu`` (CUDA forward, backward and
+  Adam; C ABI ``efie_mlp_*``) from normalised (W, L, h, feed, f) to Zin/Z_SCALE;
+* ``generate_samples``: training data from the EFIE solver itself;
+* ``adaptive_sweep``: the surrogate proposes where the |S11| minimum is, the
+  EFIE solver checks batches of points there, and the surrogate corrected by
+  the solved points interpolates between them.  Solved values always win: the
+  surrogate only places points and fills the gaps, and a sweep whose corrected
+  surrogate still misses the solver by more than ``tol`` after ``max_rounds``
+  falls back to the dense plain sweep.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as nat
+from .api import (SweepPlan, build_rwg_interior, make_patch_with_ground_mesh, pick_port_edge_by_point_and_layer,
+                  sweep_opts)
+
+MU0 = 4.0 * math.pi * 1e-7
+C0 = 299792458.0
+EPS0 = 1.0 / (MU0 * C0 * C0)
+Z_SCALE = 50.0        # Zin / Z_SCALE is the network's target
+BAND = 0.2            # sweeps cover f0 (1 +- BAND), f0 = c / (2 L)
+
+
+# ---------------------------------------------------------------------------
+# Designs
+# ---------------------------------------------------------------------------
+@dataclass
+class PatchDesign:
+    """A patch W x L (x, y) at height h over a square ground plate of side
+    ground_factor * max(W, L), fed at (0, feed) on the patch centreline."""
+    W: float
+    L: float
+    h: float
+    feed: float
+    pitch: float = 2.5e-3          # patch mesh pitch
+    ground_pitch: float = 5e-3     # ground mesh pitch
+    ground_factor: float = 1.6
+
+    @property
+    def f0(self):
+        return C0 / (2.0 * self.L)
+
+    def band(self, n):
+        return np.linspace(self.f0 * (1 - BAND), self.f0 * (1 + BAND), n)
+
+    def cells(self):
+        G = self.ground_factor * max(self.W, self.L)
+        ng = max(2, int(round(G / self.ground_pitch)))
+        return (max(2, int(round(self.W / self.pitch))), max(2, int(round(self.L / self.pitch))), ng, ng)
+
+
+def sample_designs(n, seed=0, W=(25e-3, 45e-3), L=(20e-3, 40e-3), h=(0.8e-3, 3.2e-3), feed_frac=1.0 / 3.0,
+                   pitch=2.5e-3, ground_pitch=5e-3):
+    """n designs with W, L, h uniform in the given ranges and the feed offset
+    uniform within +-feed_frac * L along the centreline."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        w = rng.uniform(*W)
+        l = rng.uniform(*L)
+        hh = rng.uniform(*h)
+        fd = rng.uniform(-feed_frac, feed_frac) * l
+        out.append(PatchDesign(w, l, hh, fd, pitch, ground_pitch))
+    return out
+
+
+def design_inputs(d: PatchDesign):
+    """Mesh, RWG and port edges of a design (library producers, grid vertex order)."""
+    npx, npy, ngx, ngy = d.cells()
+    G = d.ground_factor * max(d.W, d.L)
+    V, F, _, _ = make_patch_with_ground_mesh(d.L, d.W, G, G, d.h, npx, npy, ngx, ngy, vertex_order="grid")
+    rwg = build_rwg_interior({"V": V, "F": F})
+    pe = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, +d.h / 2), +1)
+    ge = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, -d.h / 2), -1)
+    spread = 1.5 * float(np.mean(rwg["len"]))
+    return dict(V=V, F=F, rwg=rwg, pe=pe, ge=ge, spread=spread, Ne=rwg["Ne"])
+
+
+def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None):
+    """A SweepPlan of the design: Dunavant 7-point rule + analytic 1/R extraction."""
+    x = inputs or design_inputs(d)
+    r = x["rwg"]
+    return SweepPlan(x["V"], x["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"],
+                     r["rm"], r["Ap"], r["Am"], r["len"], None, MU0, EPS0, x["pe"], x["ge"], 1.0, x["spread"], 50.0,
+                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch), rule_order=-7)
+
+
+def features(d: PatchDesign, freqs):
+    """Normalised network inputs [n x 5] (float32)."""
+    f = np.asarray(freqs, dtype=np.float64).reshape(-1)
+    X = np.empty((f.size, 5), dtype=np.float32)
+    X[:, 0] = (d.W - 35e-3) / 10e-3
+    X[:, 1] = (d.L - 30e-3) / 10e-3
+    X[:, 2] = (d.h - 2e-3) / 1.2e-3
+    X[:, 3] = d.feed / (d.L / 3.0)
+    X[:, 4] = (f / d.f0 - 1.0) / BAND
+    return X
+
+
+def zin_to_target(Zin):
+    Zin = np.asarray(Zin).reshape(-1)
+    return np.stack([Zin.real, Zin.imag], axis=1).astype(np.float32) / Z_SCALE
+
+
+def target_to_zin(T):
+    T = np.asarray(T, dtype=np.float64)
+    return Z_SCALE * (T[:, 0] + 1j * T[:, 1])
+
+
+def s11(Zin, Z0=50.0):
+    return (Zin - Z0) / (Zin + Z0)
+
+
+# ---------------------------------------------------------------------------
+# The network
+# ---------------------------------------------------------------------------
+class Surrogate:
+    """The MLP of csrc/surrogate.cu (BF16 weights, FP32 accumulate)."""
+
+    def __init__(self, n_in=5, n_hidden=256, n_layers=4, n_out=2, seed=1):
+        cfg = nat.EfieMlpConfig(n_in, n_hidden, n_layers, n_out, seed)
+        h = C.c_void_p()
+        nat.check(nat.lib().efie_mlp_create(nat.context(), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.cfg = dict(n_in=n_in, n_hidden=n_hidden, n_layers=n_layers, n_out=n_out)
+        self.shapes = [(n_in if l == 0 else n_hidden, n_out if l == n_layers else n_hidden)
+                       for l in range(n_layers + 1)]
+        self.n_params = int(nat.lib().efie_mlp_num_params(h))
+        nat.register_plan(self)
+
+    def get_params(self):
+        p = np.zeros(self.n_params, dtype=np.float32)
+        nat.check(nat.lib().efie_mlp_get_params(self._h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        nat.check(nat.lib().efie_mlp_set_params(self._h, p.ctypes.data))
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], self.cfg["n_out"]), dtype=np.float32)
+        nat.check(nat.lib().efie_mlp_forward(self._h, X.ctypes.data, X.shape[0], Y.ctypes.data))
+        return Y
+
+    def loss_grad(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        nat.check(nat.lib().efie_mlp_loss_grad(self._h, X.ctypes.data, T.ctypes.data, X.shape[0], C.byref(loss),
+                                               g.ctypes.data))
+        return loss.value, g
+
+    def train(self, X, T, epochs=100, batch=1024, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0,
+              seed=1):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        o = nat.EfieAdamOpts(lr, beta1, beta2, eps, weight_decay, batch, epochs, seed)
+        hist = np.zeros(max(1, epochs), dtype=np.float64)
+        nat.check(nat.lib().efie_mlp_train(self._h, X.ctypes.data, T.ctypes.data, X.shape[0], C.byref(o),
+                                           hist.ctypes.data))
+        return hist[:epochs]
+
+    def predict_zin(self, d: PatchDesign, freqs):
+        return target_to_zin(self.forward(features(d, freqs)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            nat.lib().efie_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Training data from the solver
+# ---------------------------------------------------------------------------
+def generate_samples(designs, n_freq, seed=0, solver="mixed"):
+    """Zin of every design at n_freq random frequencies of its band: X, T, and
+    the number of solved points."""
+    rng = np.random.default_rng(seed)
+    Xs, Ts = [], []
+    for d in designs:
+        fr = np.sort(d.f0 * (1.0 + BAND * rng.uniform(-1.0, 1.0, n_freq)))
+        plan = design_plan(d, solver=solver)
+        Zin, _ = plan.run(fr)
+        plan.close()
+        Xs.append(features(d, fr))
+        Ts.append(zin_to_target(Zin))
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
+# ---------------------------------------------------------------------------
+# Sweeps
+# ---------------------------------------------------------------------------
+def _refine_min(f, y):
+    """Sub-grid minimum of sampled y(f) by a parabola through the smallest
+    sample and its neighbours."""
+    i = int(np.argmin(y))
+    if 0 < i < len(f) - 1:
+        y0, y1, y2 = y[i - 1], y[i], y[i + 1]
+        den = y0 - 2 * y1 + y2
+        if den > 0:
+            t = 0.5 * (y0 - y2) / den
+            return float(f[i] + t * (f[i + 1] - f[i]))
+    return float(f[i])
+
+
+def dense_sweep(d: PatchDesign, n=201, plan=None):
+    """The plain sweep: n uniformly spaced solves over the design's band."""
+    own = plan is None
+    plan = plan or design_plan(d)
+    fr = d.band(n)
+    Zin, S = plan.run(fr)
+    if own:
+        plan.close()
+    return dict(freqs=fr, Zin=Zin, S11=S, f_min=_refine_min(fr, np.abs(S)), solves=n)
+
+
+def _interp_correction(fs, dz, fq):
+    """Smooth interpolant of complex samples dz at the frequencies fs,
+    evaluated at fq: a not-a-knot cubic spline (a polynomial through the
+    points when there are fewer than four), held constant outside [min fs,
+    max fs]."""
+    from scipy.interpolate import CubicSpline
+
+    o = np.argsort(fs)
+    fs, dz = np.asarray(fs, np.float64)[o], np.asarray(dz, np.complex128)[o]
+    fq = np.clip(np.asarray(fq, np.float64), fs[0], fs[-1])
+    if fs.size == 1:
+        return np.full(fq.shape, dz[0])
+    if fs.size < 4:
+        c = np.polyfit(fs - fs[0], dz, fs.size - 1)
+        return np.polyval(c, fq - fs[0])
+    return CubicSpline(fs, dz.real)(fq) + 1j * CubicSpline(fs, dz.imag)(fq)
+
+
+def adaptive_sweep(d: PatchDesign, net: Surrogate, plan=None, n_points=8, tol=1e-3, max_rounds=3, n_dense=201,
+                   span=0.04):
+    """Locate the |S11| minimum of a design with few EFIE solves.
+
+    Round 1 solves n_points around the surrogate's predicted minimum (spread
+    over +-span * f0); later rounds solve n_points around the current
+    estimate with half the previous spread.  Between solved points the curve
+    is the surrogate plus an interpolant of its error at the solved points.
+    The sweep stops when the corrected surrogate predicted the new round's
+    solved Zin within ``tol`` (relative) and the minimum lies inside the solved
+    window; otherwise, after max_rounds, it falls back to the dense plain
+    sweep of n_dense points.
+    """
+    own = plan is None
+    plan = plan or design_plan(d)
+    fq = d.band(4 * (n_dense - 1) + 1)
+    zs = net.predict_zin(d, fq)
+    f_est = _refine_min(fq, np.abs(s11(zs)))
+    lo, hi = fq[0], fq[-1]
+    fs = np.zeros(0)
+    zsol = np.zeros(0, dtype=complex)
+    sp = span * d.f0
+    rounds = 0
+    converged = False
+    err_pred = np.inf
+    while rounds < max_rounds:
+        rounds += 1
+        new = np.clip(f_est + sp * np.linspace(-1.0, 1.0, n_points), lo, hi)
+        new = np.setdiff1d(np.unique(new), fs)
+        if new.size == 0:
+            break
+        # the corrected surrogate's prediction of the new points, before solving them
+        pred = net.predict_zin(d, new)
+        if fs.size:
+            pred = pred + _interp_correction(fs, zsol - net.predict_zin(d, fs), new)
+        zn, _ = plan.run(new)
+        err_pred = float(np.max(np.abs(pred - zn) / np.abs(zn)))
+        fs = np.concatenate([fs, new])
+        zsol = np.concatenate([zsol, zn])
+        zc = zs + _interp_correction(fs, zsol - net.predict_zin(d, fs), fq)
+        f_est = _refine_min(fq, np.abs(s11(zc)))
+        inside = fs.min() < f_est < fs.max()
+        if err_pred <= tol and inside:
+            converged = True
+            break
+        sp *= 0.5
+    result = dict(f_min=f_est, solves=int(fs.size), rounds=rounds, converged=converged, err_pred=err_pred,
+                  fallback=False, freqs=fs, Zin=zsol)
+    if not converged:
+        dn = dense_sweep(d, n_dense, plan)
+        result.update(f_min=dn["f_min"], solves=int(fs.size) + n_dense, fallback=True)
+    if own:
+        plan.close()
+    return result
+
+
+def uniform_sweep_estimate(d: PatchDesign, n, plan=None, n_fine=801):
+    """The method without the network at the same budget: n uniform solves
+    over the band and a cubic interpolant of Zin between them."""
+    own = plan is None
+    plan = plan or design_plan(d)
+    fr = d.band(n)
+    Zin, _ = plan.run(fr)
+    if own:
+        plan.close()
+    fq = d.band(n_fine)
+    zi = _interp_correction(fr, Zin, fq)
+    return dict(f_min=_refine_min(fq, np.abs(s11(zi))), solves=n)
