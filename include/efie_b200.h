@@ -148,6 +148,14 @@ typedef enum efie_scheme {
                                 self and vertex-adjacent triangle pairs            */
 } efie_scheme;
 
+/* How EFIE_SOLVER_MIXED recovers the complex128 solution from the complex64
+ * LU: flexible GMRES with the LU as right preconditioner (converges also
+ * where u32 * cond(Z) approaches 1), or classical iterative refinement. */
+typedef enum efie_refine_method {
+    EFIE_REFINE_GMRES = 0,
+    EFIE_REFINE_CLASSICAL = 1
+} efie_refine_method;
+
 typedef struct efie_sweep_opts {
     int32_t solver;          /* efie_solver; default EFIE_SOLVER_MIXED          */
     int32_t port_model;      /* efie_port_model; default EFIE_PORT_GAUSS        */
@@ -157,6 +165,7 @@ typedef struct efie_sweep_opts {
     int32_t lu_nb;           /* outer LU panel width 64/128/256 (0 = tuned)     */
     int32_t timing;          /* 1 = record per-phase CUDA-event timings         */
     int32_t batch;           /* frequencies solved together (0 = automatic)     */
+    int32_t refine_method;   /* efie_refine_method; default EFIE_REFINE_GMRES    */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */

@@ -43,7 +43,8 @@ class EfiePrepack(C.Structure):
 class EfieSweepOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("port_model", C.c_int32), ("scheme", C.c_int32),
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
-                ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32)]
+                ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
+                ("refine_method", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
@@ -73,6 +74,7 @@ class EfiePrecomputeOpts(C.Structure):
 SOLVER_FP64, SOLVER_MIXED = 0, 1
 PORT_GAUSS, PORT_EDGE_DIFF = 0, 1
 SCHEME_REF, SCHEME_EXTRACT = 0, 1
+REFINE_GMRES, REFINE_CLASSICAL = 0, 1
 QUAD_DUNAVANT7 = -7
 
 # Every exported symbol of include/efie_b200.h with (restype, argtypes).

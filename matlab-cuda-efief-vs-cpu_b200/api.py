@@ -289,7 +289,9 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # Sweeps
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
-               timing=False, batch=0, lu_nb=0):
+               timing=False, batch=0, lu_nb=0, refine="gmres"):
+    """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
+    scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only)."""
     o = nat.EfieSweepOpts()
     nat.lib().efie_sweep_opts_default(C.byref(o))
     o.solver = {"fp64": nat.SOLVER_FP64, "mixed": nat.SOLVER_MIXED}[solver]
@@ -300,6 +302,7 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.timing = 1 if timing else 0
     o.batch = int(batch)
     o.lu_nb = int(lu_nb)
+    o.refine_method = {"gmres": nat.REFINE_GMRES, "classical": nat.REFINE_CLASSICAL}[refine]
     return o
 
 

@@ -61,6 +61,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->scheme = EFIE_SCHEME_REF;
     o->refine_tol = 1e-10;
     o->refine_max_iter = 30;
+    o->refine_method = EFIE_REFINE_GMRES;
     o->lu_nb = 0;
     o->timing = 0;
     o->batch = 0;
@@ -356,6 +357,8 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         return efie_fail(EFIE_ERR_ARGS, "unknown solver");
     if (!(p->opts.refine_tol > 0)) p->opts.refine_tol = 1e-10;
     if (p->opts.refine_max_iter <= 0) p->opts.refine_max_iter = 30;
+    if (p->opts.refine_method != EFIE_REFINE_GMRES && p->opts.refine_method != EFIE_REFINE_CLASSICAL)
+        return efie_fail(EFIE_ERR_ARGS, "unknown refinement method");
     EFIE_TRY(check_port(mesh, pe, ge));
     const int N = mesh->Ne;
     p->Ne = N;
@@ -460,8 +463,12 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             rc = efie_mixed_factor(ctx, p->sw, p->Z.p, NN, active);
             if (rc != EFIE_OK) break;
             RefineResult rr;
-            rc = efie_mixed_refine(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
-                                   p->opts.refine_max_iter, active, &rr);
+            if (p->opts.refine_method == EFIE_REFINE_CLASSICAL)
+                rc = efie_mixed_refine(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
+                                       p->opts.refine_max_iter, active, &rr);
+            else
+                rc = efie_mixed_gmres(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
+                                      p->opts.refine_max_iter, active, &rr);
             if (rc != EFIE_OK) break;
             S->refine_iters_max = std::max(S->refine_iters_max, rr.iters);
             for (int f = 0; f < nb; f++) {

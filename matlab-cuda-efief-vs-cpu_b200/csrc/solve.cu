@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int r0, int r1, int 
 __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restrict__ Zb, size_t zstride,
                                                   const double2 *__restrict__ xb, const double2 *__restrict__ b,
                                                   float2 *__restrict__ rfb, int vstride, char *__restrict__ ctl,
-                                                  double tol) {
+                                                  double tol, double2 *__restrict__ routb) {
     const int f = blockIdx.y;
     char *c = ctl + 64 * f;
     double *red = reinterpret_cast<double *>(c);
@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restri
             const double2 bb = b[m];
             const double2 r = make_double2(bb.x - t.x, bb.y - t.y);
             rf[m] = make_float2((float)r.x, (float)r.y);
+            if (routb) routb[(size_t)N * f + m] = r;
             q = r.x * r.x + r.y * r.y;
         }
         sq[lane] = q;
@@ -551,7 +552,7 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
     dim3 rg((N + 31) / 32, B);
     tok = log.begin(s);
     k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, static_cast<const double2 *>(x),
-                                  static_cast<const double2 *>(b), rf, w.vstride, ctl, -1.0);
+                                  static_cast<const double2 *>(b), rf, w.vstride, ctl, -1.0, nullptr);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
     int it = 0;
@@ -569,7 +570,7 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
             tok = log.begin(s);
             k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride,
                                           static_cast<const double2 *>(x), static_cast<const double2 *>(b), rf,
-                                          w.vstride, ctl, tol);
+                                          w.vstride, ctl, tol, nullptr);
             EFIE_CUDA(cudaGetLastError());
             log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
         }
@@ -593,6 +594,31 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
         res->converged[f] = *reinterpret_cast<const int *>(c + 28) != 0;
         res->err[f] = *reinterpret_cast<const int *>(c + 36);
     }
+    return EFIE_OK;
+}
+
+efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *x,
+                               const void *b, double tol, void *rout, int nact) {
+    cudaStream_t s = ctx->stream;
+    dim3 rg((w.N + 31) / 32, w.B);
+    size_t tok = ctx->log.begin(s);
+    k_residual<<<rg, 256, 0, s>>>(w.N, static_cast<const double2 *>(Z), zstride, static_cast<const double2 *>(x),
+                                  static_cast<const double2 *>(b), w.vec.as<float2>(), w.vstride, w.ctl.as<char>(),
+                                  tol, static_cast<double2 *>(rout));
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_RESIDUAL, s, tok, 16.0 * (double)w.N * w.N * nact);
+    return EFIE_OK;
+}
+
+efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm) {
+    cudaStream_t s = ctx->stream;
+    const int N = w.N, B = w.B;
+    size_t tok = ctx->log.begin(s);
+    k_fill_c128<<<(unsigned)(((size_t)N * B + 255) / 256), 256, 0, s>>>((size_t)N * B, static_cast<double2 *>(x),
+                                                                        make_double2(0.0, 0.0));
+    k_init_ctl<<<(B + 63) / 64, 64, 0, s>>>(B, w.ctl.as<char>(), bnorm, w.active.as<int>());
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_OTHER, s, tok, 0.0, 2);
     return EFIE_OK;
 }
 

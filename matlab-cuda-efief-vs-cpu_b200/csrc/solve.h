@@ -21,6 +21,11 @@ struct SolveWork {
     DevBuf ctl;      // per f 64 bytes: red[3] @0, counter @24, conv @28, skip @32, err @36
     DevBuf active;   // int[B]: slot holds a frequency of this batch
     DevBuf packA, packB;  // tensor-core operand staging
+    // flexible GMRES (gmres.cu): Krylov basis V [M+1][B][N] and preconditioned
+    // vectors Zm [M][B][N] in complex128, the new vector w [B][N], partial
+    // sums and per-frequency Arnoldi state
+    DevBuf gV, gZ, gw, gpart, gst;
+    int gnch = 0;          // row chunks of the orthogonalisation kernels
 };
 
 struct RefineResult {
@@ -35,6 +40,18 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer);
 efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host);
 efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
                               double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
+// Flexible GMRES on Z x = b with the complex64 LU as right preconditioner;
+// the Arnoldi process and every vector are complex128.  Same contract as
+// efie_mixed_refine (x starts at 0; res->iters counts matrix-vector products).
+efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
+                             double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
+// r = b - Z x for every frequency of the batch (complex128), its complex64
+// copy in w.vec, ||r|| / ||b|| and the convergence flags in w.ctl; r is also
+// stored at rout + N f when rout is not null.
+efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *x,
+                               const void *b, double tol, void *rout, int nact);
+// x = 0 and fresh control blocks (||b|| = bnorm) for every slot.
+efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
                              int ge, double V0, double Z0, void *out);
 
