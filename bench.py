@@ -46,7 +46,16 @@ WORKLOADS = {
     # same plates, patch 12x10 grid, ground 16x16 grid
     "cfg1": dict(Lp=30e-3, Wp=38e-3, Lg=60e-3, Wg=60e-3, h=1.6e-3, Np=(12, 10), Ng=(16, 16),
                  freqs=(2.0e9, 3.0e9, 11)),
+    # large single design: patch 40x32 mm at 0.5 mm (80x64 grid) over a 90x90 mm ground at 2 mm
+    # (45x45 grid), h 1.6 mm: Ne = 21177
+    "cfg5": dict(Lp=32e-3, Wp=40e-3, Lg=90e-3, Wg=90e-3, h=1.6e-3, Np=(80, 64), Ng=(45, 45),
+                 freqs=(2.0e9, 3.0e9, 51)),
 }
+# Design-family workloads (surrogate.sample_designs): cfg3 sweeps 64 designs of
+# uneven size (patch pitch 1.5 mm, ground pitch 3 mm: Ne 1390..3697) at 41
+# points over f0 (1 +- 0.2); cfg4 trains the surrogate on solver samples of
+# that distribution and runs adaptive sweeps against dense 201-point sweeps.
+FAMILY = dict(n=64, seed=3, pitch=1.5e-3, ground_pitch=3e-3, nfreq=41)
 RULE = {"ref": 0, "extract": -7}
 SCHEME_NAME = {"ref": "reference cached subdivision + softening (GPU option set)",
                "extract": "Dunavant 7-point rule + analytic 1/R extraction on self/vertex-adjacent pairs"}
@@ -291,12 +300,14 @@ def run_ours(args):
     m = _pkg()
     nat = importlib.import_module(PKG + "._native")
     nat.context(local)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and it can be graph-captured
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     nat.check(nat.lib().efie_ctx_set_stream(nat.context(local), stream.cuda_stream))
     inp = build_inputs(m, args.workload)
     freqs = inp["freqs"]
     B = args.batch or len(freqs)
-    opts = m.sweep_opts(solver=args.solver, timing=True, scheme=args.scheme)
+    opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -313,7 +324,6 @@ def run_ours(args):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    classes = {k: dict(launches=0, ms=0.0, work=0.0) for k in nat.KERNEL_CLASSES}
     launches = 0
     fallback = 0
     relres = 0.0
@@ -329,9 +339,6 @@ def run_ours(args):
             fallback += st["n_fp64_fallback"]
             relres = max(relres, st["max_relres"])
             iters = max(iters, st["refine_iters_max"])
-            for k, v in st["classes"].items():
-                for f in ("launches", "ms", "work"):
-                    classes[k][f] += v[f]
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
@@ -341,6 +348,11 @@ def run_ours(args):
         ms = float(t.item())
     total_points = args.steps * B * world
     value = total_points / (ms * 1e-3)
+    # per-class breakdown (roofline): one more step with CUDA events around
+    # every launch (eager launches), outside the timed region
+    plan.set_timing(True)
+    plan.run(batch(args.warmup + args.steps))
+    classes = {k: dict(v) for k, v in plan.stats["classes"].items()}
     plan.close()
 
     # e2e: the public API call with host arrays (upload + sweep + results) per step
@@ -380,7 +392,9 @@ def run_ours(args):
                     gpu_launches=launches, clocks=clk.summary(),
                     accuracy=dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback),
                     roofline=roofline(classes),
-                    phases_ms_per_point={k: v["ms"] / (args.steps * B) for k, v in classes.items()})
+                    phases_ms_per_point={k: v["ms"] / B for k, v in classes.items()},
+                    phases_note="one extra step with per-launch CUDA events (eager launches), outside the "
+                                "timed region; the timed steps replay the factorization as a CUDA graph")
         if world == 1 and not args.no_cpu_baseline:
             v, cores, dt = cpu_baseline_sample(inp, 1)
             line["cpu_baseline"] = dict(value=v, unit="freq points/s", cores=cores, kind="port",
@@ -393,13 +407,160 @@ def run_ours(args):
     return 0
 
 
+def _family():
+    sur = importlib.import_module(PKG + ".surrogate")
+    return sur, sur.sample_designs(FAMILY["n"], seed=FAMILY["seed"], pitch=FAMILY["pitch"],
+                                   ground_pitch=FAMILY["ground_pitch"])
+
+
+def run_family(args):
+    """cfg3: one step = one design of the family (host mesh -> plan -> 41-point
+    sweep -> results); designs of uneven Ne, each swept with batched
+    frequencies.  Device time (CUDA events on the library's stream) covers
+    geometry upload, assembly, solve and port reduction; e2e adds the host
+    producers and the result read-back (wall clock)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    nat = importlib.import_module(PKG + "._native")
+    nat.context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    nat.check(nat.lib().efie_ctx_set_stream(nat.context(local), stream.cuda_stream))
+    sur, designs = _family()
+    nf = FAMILY["nfreq"]
+
+    def step(i):
+        d = designs[(i * world + rank) % len(designs)]
+        x = sur.design_inputs(d)
+        plan = sur.design_plan(d, inputs=x)
+        Zin, _ = plan.run(d.band(nf))
+        plan.close()
+        return x["Ne"], Zin
+
+    for i in range(args.warmup):
+        step(i)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    Ns = []
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        for i in range(args.steps):
+            n, _ = step(args.warmup + i)
+            Ns.append(n)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms, wall * 1e3], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, wall = float(t[0].item()), float(t[1].item()) * 1e-3
+    pts = args.steps * nf * world
+    if rank == 0:
+        line = dict(metric=METRIC, value=pts / (ms * 1e-3), unit="freq points/s", n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=ms / args.steps, higher_is_better=True, scaling="weak",
+                    vs_baseline=None, dtype="c128 (assembly, residual) / c64 (LU)", data="synthetic",
+                    config=dict(workload="cfg3", designs=FAMILY["n"], Ne_of_timed_designs=Ns, freqs_per_design=nf,
+                                mesh_pitch_mm=[1e3 * FAMILY["pitch"], 1e3 * FAMILY["ground_pitch"]],
+                                scheme="Dunavant 7-point rule + analytic 1/R extraction", solver="mixed (GMRES)",
+                                parallelism="replicas x%d" % world),
+                    e2e=dict(value=pts / wall, unit="freq points/s", h2d_bytes_per_step=None,
+                             d2h_bytes_per_step=nf * 32),
+                    clocks=clk.summary())
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_surrogate(args):
+    """cfg4: train the surrogate on solver samples of the design family, then
+    locate the |S11| minimum of held-out designs with surrogate-guided
+    adaptive sweeps and with dense 201-point sweeps."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sur, _ = _family()
+    nper = 40
+    ntrain = max(1, args.samples // nper)
+    train = sur.sample_designs(ntrain, seed=11, pitch=FAMILY["pitch"], ground_pitch=FAMILY["ground_pitch"])
+    t0 = time.perf_counter()
+    X, T = sur.generate_samples(train, nper, seed=12)
+    t_data = time.perf_counter() - t0
+    net = sur.Surrogate(seed=13)
+    t0 = time.perf_counter()
+    hist = net.train(X, T, epochs=args.epochs, batch=1024, lr=2e-3)
+    hist2 = net.train(X, T, epochs=max(1, args.epochs // 3), batch=1024, lr=3e-4)
+    t_train = time.perf_counter() - t0
+    test = sur.sample_designs(max(3, args.steps), seed=99, pitch=FAMILY["pitch"], ground_pitch=FAMILY["ground_pitch"])
+    rows = []
+    t_ad = t_dn = t_un = 0.0
+    for d in test:
+        plan = sur.design_plan(d)
+        plan.run(d.band(8))     # warm the plan
+        t0 = time.perf_counter()
+        dn = sur.dense_sweep(d, 201, plan)
+        t_dn += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ad = sur.adaptive_sweep(d, net, plan)
+        t_ad += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        un = sur.uniform_sweep_estimate(d, ad["solves"], plan)
+        t_un += time.perf_counter() - t0
+        step = (d.band(201)[1] - d.band(201)[0])
+        rows.append(dict(Ne=plan.Ne, solves=ad["solves"], rounds=ad["rounds"], fallback=ad["fallback"],
+                         fmin_err_steps=abs(ad["f_min"] - dn["f_min"]) / step,
+                         uniform_err_steps=abs(un["f_min"] - dn["f_min"]) / step))
+        plan.close()
+    nd = len(test)
+    solves = sum(r["solves"] for r in rows)
+    line = dict(metric=METRIC, value=201 * nd / t_ad, unit="dense-equivalent freq points/s", n_gpus=1,
+                steps=nd, warmup=1, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="c128/c64 solver; MLP bf16 weights, fp32 accumulate", data="synthetic",
+                config=dict(workload="cfg4", train_samples=int(len(X)), train_designs=ntrain, epochs=args.epochs,
+                            mlp="5 -> 4 x 256 SiLU -> 3 (log|Zin|, cos, sin arg Zin)", test_designs=nd),
+                surrogate=dict(data_s=t_data, solver_samples_per_s=len(X) / t_data, train_s=t_train,
+                               loss_first=float(hist[0]), loss_last=float(hist2[-1]),
+                               adaptive_solves_per_design=solves / nd,
+                               adaptive_solved_points_per_s=solves / t_ad,
+                               dense_points_per_s=201 * nd / t_dn,
+                               fmin_err_steps_max=max(r["fmin_err_steps"] for r in rows),
+                               fmin_err_steps_mean=statistics.mean(r["fmin_err_steps"] for r in rows),
+                               uniform_same_budget_err_steps_mean=statistics.mean(r["uniform_err_steps"]
+                                                                                  for r in rows),
+                               fallbacks=sum(1 for r in rows if r["fallback"]), designs=rows),
+                e2e=dict(value=201 * nd / t_ad, unit="dense-equivalent freq points/s", h2d_bytes_per_step=None,
+                         d2h_bytes_per_step=None))
+    print(json.dumps(line), flush=True)
+    net.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS), default="cfg2")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["cfg3", "cfg4"], default="cfg2")
+    ap.add_argument("--samples", type=int, default=20000, help="cfg4: solver samples for training")
+    ap.add_argument("--epochs", type=int, default=300, help="cfg4: training epochs")
     ap.add_argument("--batch", type=int, default=0, help="frequency points per step (0 = the whole sweep)")
     ap.add_argument("--solver", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--scheme", choices=["ref", "extract"], default="ref",
@@ -410,7 +571,15 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
+        if args.workload in ("cfg3", "cfg4"):
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no design-family or "
+                              "surrogate sweep; its CPU path is timed on the single-design workloads"}))
+            return 0
         return run_reference(args)
+    if args.workload == "cfg3":
+        return run_family(args)
+    if args.workload == "cfg4":
+        return run_surrogate(args)
     return run_ours(args)
 
 

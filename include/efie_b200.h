@@ -166,6 +166,9 @@ typedef struct efie_sweep_opts {
     int32_t timing;          /* 1 = record per-phase CUDA-event timings         */
     int32_t batch;           /* frequencies solved together (0 = automatic)     */
     int32_t refine_method;   /* efie_refine_method; default EFIE_REFINE_GMRES    */
+    int32_t graphs;          /* 1 (default): with timing off, the mixed LU of a
+                                batch replays a CUDA graph captured on the
+                                plan's first batch; 0: eager launches        */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */
@@ -236,6 +239,10 @@ efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
 efie_status efie_plan_run(efie_plan *plan, const double *freqs, int32_t Nf,
                           efie_c128 *Zin, efie_c128 *S11, efie_c128 *I, efie_sweep_stats *stats);
 void efie_plan_destroy(efie_plan *plan);
+/* Switch the per-kernel-class CUDA-event timing of later runs on (1) or off
+ * (0).  Timed runs launch the factorization eagerly; untimed runs replay it
+ * as a CUDA graph (opts->graphs). */
+efie_status efie_plan_set_timing(efie_plan *plan, int32_t timing);
 
 /* ---------------------------------------------------------------------- */
 /* Boundary-data producers (MATLAB-side in the reference)                  */

@@ -44,7 +44,7 @@ class EfieSweepOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("port_model", C.c_int32), ("scheme", C.c_int32),
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
                 ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
-                ("refine_method", C.c_int32)]
+                ("refine_method", C.c_int32), ("graphs", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
@@ -102,6 +102,7 @@ SIGNATURES = {
                                    C.POINTER(EfieSweepOpts), C.c_int32, C.POINTER(_P)]),
     "efie_plan_run": (C.c_int, [_P, c_double_p, C.c_int32, _P, _P, _P, C.POINTER(EfieSweepStats)]),
     "efie_plan_destroy": (None, [_P]),
+    "efie_plan_set_timing": (C.c_int, [_P, C.c_int32]),
     "efie_make_patch_with_ground_mesh": (C.c_int, [C.c_double] * 5 + [C.c_int32] * 5 + [c_double_p, c_int32_p]),
     "efie_build_rwg_interior": (C.c_int, [C.c_int32, c_double_p, C.c_int32, c_int32_p, C.c_int32, c_int32_p,
                                           c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p,

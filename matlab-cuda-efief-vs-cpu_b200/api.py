@@ -289,7 +289,7 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # Sweeps
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
-               timing=False, batch=0, lu_nb=0, refine="gmres"):
+               timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True):
     """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
     scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only)."""
     o = nat.EfieSweepOpts()
@@ -303,6 +303,7 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.batch = int(batch)
     o.lu_nb = int(lu_nb)
     o.refine_method = {"gmres": nat.REFINE_GMRES, "classical": nat.REFINE_CLASSICAL}[refine]
+    o.graphs = 1 if graphs else 0
     return o
 
 
@@ -416,6 +417,11 @@ class SweepPlan:
                                           I.ctypes.data if I is not None else None, C.byref(st)))
         self.stats = st.as_dict()
         return (Zin, S11, I) if return_currents else (Zin, S11)
+
+    def set_timing(self, on):
+        """Per-kernel-class event timing of later runs (eager launches) or not
+        (the factorization replays a CUDA graph)."""
+        nat.check(nat.lib().efie_plan_set_timing(self._h, 1 if on else 0))
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

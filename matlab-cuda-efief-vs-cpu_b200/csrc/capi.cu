@@ -62,6 +62,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->refine_tol = 1e-10;
     o->refine_max_iter = 30;
     o->refine_method = EFIE_REFINE_GMRES;
+    o->graphs = 1;
     o->lu_nb = 0;
     o->timing = 0;
     o->batch = 0;
@@ -300,9 +301,63 @@ struct efie_plan {
     DevBuf Z, b, x, wport, out, scratch, ipiv, info, lwork;
     int lwork_elems = -1;
     SolveWork sw;
+    // the mixed factorization as a CUDA graph (captured on the first untimed
+    // batch, replayed for every later one) and its per-class launch counts
+    cudaGraphExec_t factor_graph = nullptr;
+    int graph_launches[EFIE_NUM_KERNEL_CLASSES] = {0};
+    double graph_work[EFIE_NUM_KERNEL_CLASSES] = {0};
+    ~efie_plan() {
+        if (factor_graph) cudaGraphExecDestroy(factor_graph);
+    }
 };
 
 namespace {
+
+// The mixed factorization of one batch.  With timing off (and graphs not
+// disabled) the kernel sequence -- about 4 launches per 64-column block, all
+// with fixed arguments for a given plan -- is captured once and replayed as a
+// CUDA graph; with timing on it runs eagerly so each launch keeps its events.
+efie_status plan_factor(efie_plan *p, const int *active, int nact) {
+    efie_ctx *ctx = p->ctx;
+    const size_t NN = (size_t)p->Ne * p->Ne;
+    EFIE_TRY(efie_mixed_factor_prepare(ctx, p->sw, active));
+    // the legacy default stream cannot be captured: launch eagerly there
+    const bool graph = !ctx->log.timing && p->opts.graphs && ctx->stream != nullptr;
+    if (!graph) return efie_mixed_factor_launch(ctx, p->sw, p->Z.p, NN, nact);
+    KernelLog &log = ctx->log;
+    if (!p->factor_graph) {
+        int l0[EFIE_NUM_KERNEL_CLASSES];
+        double w0[EFIE_NUM_KERNEL_CLASSES];
+        for (int c = 0; c < EFIE_NUM_KERNEL_CLASSES; c++) l0[c] = log.launches[c], w0[c] = log.work[c];
+        cudaGraph_t g = nullptr;
+        EFIE_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        // the captured sequence works on every slot; `active` (device) gates them
+        efie_status st = efie_mixed_factor_launch(ctx, p->sw, p->Z.p, NN, p->B);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (st != EFIE_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&p->factor_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            p->factor_graph = nullptr;
+            return efie_fail(EFIE_ERR_CUDA, std::string("factor graph: ") + cudaGetErrorString(e));
+        }
+        for (int c = 0; c < EFIE_NUM_KERNEL_CLASSES; c++) {
+            p->graph_launches[c] = log.launches[c] - l0[c];
+            p->graph_work[c] = (log.work[c] - w0[c]) * nact / std::max(1, p->B);
+            log.launches[c] = l0[c];
+            log.work[c] = w0[c];
+        }
+    }
+    EFIE_CUDA(cudaGraphLaunch(p->factor_graph, ctx->stream));
+    for (int c = 0; c < EFIE_NUM_KERNEL_CLASSES; c++) {
+        log.launches[c] += p->graph_launches[c];
+        log.work[c] += p->graph_work[c];
+    }
+    return EFIE_OK;
+}
 
 // complex128 LU (cuSOLVER) of Z_f in place and x_f = Z_f^-1 V
 efie_status plan_solve_fp64(efie_plan *p, int slot, int fi) {
@@ -417,6 +472,12 @@ extern "C" efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, co
     return EFIE_OK;
 }
 
+extern "C" efie_status efie_plan_set_timing(efie_plan *p, int32_t timing) {
+    if (!p) return efie_fail(EFIE_ERR_ARGS, "null plan");
+    p->opts.timing = timing ? 1 : 0;
+    return EFIE_OK;
+}
+
 extern "C" void efie_plan_destroy(efie_plan *p) {
     if (!p) return;
     DeviceGuard dg(p->ctx->device);
@@ -460,7 +521,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         if (rc != EFIE_OK) break;
         bool fallback[EFIE_MAX_BATCH] = {false};
         if (mixed) {
-            rc = efie_mixed_factor(ctx, p->sw, p->Z.p, NN, active);
+            rc = plan_factor(p, active, nb);
             if (rc != EFIE_OK) break;
             RefineResult rr;
             if (p->opts.refine_method == EFIE_REFINE_CLASSICAL)

@@ -9,13 +9,16 @@
 // accumulate in FP32 in tensor memory (TMEM), which keeps the update close to
 // FP32 accuracy (the LU is then refined in FP64).
 //
-// Operands are packed per LU step into 128B-swizzled K-major tiles that sit
-// contiguously in global memory, so each CTA fetches them with plain bulk
-// copies (cp.async.bulk, the TMA engine; no multicast, local memory only).
-// One CTA computes a 128 x 256 accumulator tile (64 complex rows x 256
-// complex columns): one elected thread issues tcgen05.mma, two shared-memory
-// stages double-buffer the K' chunks, and all four warps drain TMEM with
-// tcgen05.ld for the read-modify-write epilogue on the row-major planes.
+// Operands are packed per LU step into 64B-swizzled K-major tiles (16 TF32
+// per row) that sit contiguously in global memory, so each CTA fetches them
+// with plain bulk copies (cp.async.bulk, the TMA engine; no multicast, local
+// memory only).  One CTA computes a 128 x 256 accumulator tile (64 complex
+// rows x 256 complex columns): one elected thread issues tcgen05.mma over a
+// 4-stage shared-memory ring of K' chunks -- it issues chunk c's MMAs before
+// waiting for chunk c-1's to retire, so the tensor pipe always holds queued
+// work while the bulk loads run three chunks ahead -- and all four warps drain
+// TMEM with tcgen05.ld for the read-modify-write epilogue on the row-major
+// planes.
 // Every mbarrier wait is bounded; a timeout sets the device error flag.
 #include <cstdint>
 
@@ -26,17 +29,19 @@ namespace {
 constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
 constexpr int TM = 128;          // accumulator rows (64 complex rows)
 constexpr int TN = 256;          // accumulator columns (complex columns)
-constexpr int KC = 32;           // fp32 elements per 128-byte swizzle row (one K' chunk)
-constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 16 chunks
-constexpr int A_TILE = TM * KC;       // floats per A tile (16 KB)
-constexpr int B_TILE = TN * KC;       // floats per B tile (32 KB)
-constexpr int STAGE_FLOATS = 2 * A_TILE + 2 * B_TILE;   // hi/lo of A and B: 96 KB
-constexpr int NSTAGE = 2;
-constexpr size_t GEMM_SMEM = sizeof(float) * NSTAGE * STAGE_FLOATS + 1024 + 64;
+constexpr int KC = 16;           // fp32 elements per 64-byte swizzle row (one K' chunk)
+constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 32 chunks
+constexpr int A_TILE = TM * KC;       // floats per A tile (8 KB)
+constexpr int B_TILE = TN * KC;       // floats per B tile (16 KB)
+constexpr int STAGE_FLOATS = 2 * A_TILE + 2 * B_TILE;   // hi/lo of A and B: 48 KB
+constexpr int NSTAGE = 4;
+constexpr int NBAR = 2 * NSTAGE + 1;  // full[NSTAGE], empty[NSTAGE], done
+constexpr size_t GEMM_SMEM = sizeof(float) * NSTAGE * STAGE_FLOATS + 1024 + 8 * NBAR + 16;
 
-// byte offset of element (row r, k) inside a K-major 128B-swizzled tile
+// byte offset of element (row r, k) inside a K-major 64B-swizzled tile: the
+// 16-byte chunk index (k / 4) XOR (r / 2) mod 4, 8-row atoms of 512 bytes
 __host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) {
-    return r * 128u + ((((k >> 2) ^ (r & 7u)) & 7u) << 4) + ((k & 3u) << 2);
+    return r * 64u + ((((k >> 2) ^ (r >> 1)) & 3u) << 4) + ((k & 3u) << 2);
 }
 
 __device__ __forceinline__ float tf32_rna(float x) {
@@ -67,7 +72,7 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol,
     float *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
     for (int e = threadIdx.x; e < A_TILE; e += 256) {
-        const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
+        const int r = e >> 4, kq = e & 15;           // consecutive threads: consecutive k
         const int kp = chunk * KC + kq;              // K' index
         const bool second = kp >= K;
         const int kk = second ? kp - K : kp;         // column within the L block
@@ -169,14 +174,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ uint64_t desc_sw128(const void *smem_tile) {
+__device__ __forceinline__ uint64_t desc_sw64(const void *smem_tile) {
     const uint32_t a = smem_u32(smem_tile);
     uint64_t d = 0;
     d |= (uint64_t)((a & 0x3FFFFu) >> 4);      // start address
     d |= (uint64_t)1 << 16;                    // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)(512 >> 4) << 32;           // stride byte offset: 8 rows x 64 B
     d |= (uint64_t)1 << 46;                    // descriptor version (sm_100)
-    d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+    d |= (uint64_t)4 << 61;                    // SWIZZLE_64B
     return d;
 }
 
@@ -226,14 +231,15 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
     extern __shared__ uint8_t dyn_raw[];
     // 1024-byte alignment for the swizzled tiles
     float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_FLOATS);  // full[2], empty[2], done
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 5);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_FLOATS);  // full[], empty[], done
+    uint64_t *full = bars, *empty = bars + NSTAGE, *done = bars + 2 * NSTAGE;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + NBAR);
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile_n = blockIdx.x, tile_m = blockIdx.y;
 
     if (tid == 0) {
-        for (int i = 0; i < 5; i++) mbar_init(&bars[i], 1);
+        for (int i = 0; i < NBAR; i++) mbar_init(&bars[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -254,20 +260,18 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
         const uint32_t bytes = sizeof(float) * (2 * A_TILE + 2 * B_TILE);
         auto load = [&](int c) {
             float *st = stage + (c % NSTAGE) * STAGE_FLOATS;
-            mbar_expect_tx(&bars[c % NSTAGE], bytes);
-            bulk_g2s(st, ga + (size_t)c * 2 * A_TILE, sizeof(float) * 2 * A_TILE, &bars[c % NSTAGE]);
-            bulk_g2s(st + 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, sizeof(float) * 2 * B_TILE, &bars[c % NSTAGE]);
+            mbar_expect_tx(&full[c % NSTAGE], bytes);
+            bulk_g2s(st, ga + (size_t)c * 2 * A_TILE, sizeof(float) * 2 * A_TILE, &full[c % NSTAGE]);
+            bulk_g2s(st + 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, sizeof(float) * 2 * B_TILE, &full[c % NSTAGE]);
         };
-        load(0);
-        if (nchunk > 1) load(1);
+        for (int c = 0; c < NSTAGE && c < nchunk; c++) load(c);
         for (int c = 0; c < nchunk && ok; c++) {
             const int sidx = c % NSTAGE;
-            const uint32_t phase = (c / NSTAGE) & 1;
-            if (!mbar_wait(&bars[sidx], phase, err)) { ok = false; break; }
+            if (!mbar_wait(&full[sidx], (c / NSTAGE) & 1, err)) { ok = false; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const float *st = stage + sidx * STAGE_FLOATS;
-            const uint64_t ahi = desc_sw128(st), alo = desc_sw128(st + A_TILE);
-            const uint64_t bhi = desc_sw128(st + 2 * A_TILE), blo = desc_sw128(st + 2 * A_TILE + B_TILE);
+            const uint64_t ahi = desc_sw64(st), alo = desc_sw64(st + A_TILE);
+            const uint64_t bhi = desc_sw64(st + 2 * A_TILE), blo = desc_sw64(st + 2 * A_TILE + B_TILE);
 #pragma unroll
             for (int kk = 0; kk < KC / 8; kk++) {
                 const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
@@ -276,19 +280,22 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
                 mma_tf32(tmem, ahi + adv, blo + adv, 1u);
                 mma_tf32(tmem, ahi + adv, bhi + adv, 1u);
             }
-            mma_commit(&bars[2 + sidx]);   // stage sidx free once these MMAs have read it
-            if (c + NSTAGE < nchunk) {
-                if (!mbar_wait(&bars[2 + sidx], phase, err)) { ok = false; break; }
-                load(c + NSTAGE);
+            mma_commit(&empty[sidx]);   // stage sidx free once these MMAs have read it
+            // refill the stage of chunk c - 1: its MMAs were queued ahead of chunk
+            // c's, so waiting for them leaves chunk c's MMAs on the tensor pipe
+            const int cp = c - 1;
+            if (cp >= 0 && cp + NSTAGE < nchunk) {
+                if (!mbar_wait(&empty[cp % NSTAGE], (cp / NSTAGE) & 1, err)) { ok = false; break; }
+                load(cp + NSTAGE);
             }
         }
-        mma_commit(&bars[4]);              // all MMAs of this tile done
+        mma_commit(done);                  // all MMAs of this tile done
         if (!ok) *ok_sh = 0;
     }
     __syncthreads();
     // every thread waits for the accumulator (bounded); the decision is made
     // uniform per warp because tcgen05.ld is a warp-collective instruction
-    bool have = mbar_wait(&bars[4], 0, err);
+    bool have = mbar_wait(done, 0, err);
     have = __all_sync(0xffffffffu, have) && (*ok_sh != 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
@@ -344,6 +351,18 @@ efie_status efie_tc_attrs() {
 }
 
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
+
+// Staging for the largest update of an N x N LU (per frequency slot), and the
+// kernel attributes: done when the workspace is created, so that the factor
+// sequence allocates nothing and can be captured into a CUDA graph.
+efie_status efie_gemm_workspace(SolveWork &w) {
+    EFIE_TRY(efie_tc_attrs());
+    const int mt0 = (w.N + 63) / 64, nt0 = (w.N + TN - 1) / TN;
+    const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
+    EFIE_TRY(w.packA.reserve(sizeof(float) * astride * w.B));
+    EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * w.B));
+    return EFIE_OK;
+}
 
 // C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] for every
 // active frequency: tensor cores when the block spans enough work, CUDA cores

@@ -64,107 +64,200 @@ __global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__res
 // Diagonal block bi of every frequency (blockIdx.x = f): unblocked LU without
 // pivoting of A[k:k+kb, k:k+kb] and the inverses of its unit-lower L and upper
 // U factors (kept for the panel products and the triangular solves).
+//
+// 512 threads; thread t owns row r = t / 8 and columns 8 (t mod 8) ... + 7 of
+// the block in registers (the 8 threads of a row share a warp).  Step j
+// reads the pivot row and the pivot column from shared memory; while
+// updating, the threads that hold row j + 1 and column j + 1 store them
+// (double-buffered), so a step is one barrier and one reciprocal.  Only the
+// column group that contains the pivot column needs per-column predicates.
+// The inverses follow in one 64-step sweep with the factors staged in shared
+// memory: forward substitution for L^-1 (X = I; X[r] -= l_rj X[j], r > j)
+// and backward substitution for U^-1 (Y = I; Y[j] *= 1/u_jj, then
+// Y[r] -= u_rj Y[j], r < j).  Row buffers carry one pad entry per 8 columns
+// so that the 8 column groups of a warp hit distinct banks.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
-                                                      size_t pstride, int ld, float2 *__restrict__ dinv,
-                                                      size_t dstride, char *__restrict__ ctl,
-                                                      const int *__restrict__ active) {
+constexpr int DG = 8;                                        // columns per thread
+__device__ __forceinline__ int padc(int c) { return c + (c >> 3); }
+
+__device__ __forceinline__ void cfms(float2 &acc, float2 l, float2 u) {   // acc -= l * u
+    acc.x -= l.x * u.x - l.y * u.y;
+    acc.y -= l.x * u.y + l.y * u.x;
+}
+
+__global__ void __launch_bounds__(512) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
+                                                     size_t pstride, int ld, float2 *__restrict__ dinv,
+                                                     size_t dstride, char *__restrict__ ctl,
+                                                     const int *__restrict__ active) {
     const int f = blockIdx.x;
     if (!active[f]) return;
-    extern __shared__ float2 dyn[];
-    float2(*a)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);
-    float2(*w)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));
+    __shared__ float2 prow[2][72];
+    __shared__ float2 colb[2][NB];
+    __shared__ float2 LU[NB][NB + 1];
+    __shared__ float2 rdiag[NB];
+    __shared__ float2 xrow[2][72];
+    __shared__ float2 yrow[2][72];
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
     int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
-    const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += 1024) {
-        const int i = e / NB, j = e % NB;
-        float2 v = make_float2(0.f, 0.f);
-        if (i < kb && j < kb) v = make_float2(Ar[(size_t)(k + i) * ld + k + j], Ai[(size_t)(k + i) * ld + k + j]);
-        else if (i == j) v = make_float2(1.f, 0.f);  // pad to identity
-        a[i][j] = v;
+    const int t = threadIdx.x, r = t >> 3, c0 = (t & 7) * DG;
+    float2 a[DG];
+    if (r < kb) {
+        // 8 consecutive floats of each plane: 32-byte aligned (ld, k, c0 are multiples of 8)
+        const float4 *pr = reinterpret_cast<const float4 *>(Ar + (size_t)(k + r) * ld + k + c0);
+        const float4 *pi = reinterpret_cast<const float4 *>(Ai + (size_t)(k + r) * ld + k + c0);
+#pragma unroll
+        for (int v = 0; v < 2; v++) {
+            const float4 re = pr[v], im = pi[v];
+            a[4 * v + 0] = make_float2(re.x, im.x);
+            a[4 * v + 1] = make_float2(re.y, im.y);
+            a[4 * v + 2] = make_float2(re.z, im.z);
+            a[4 * v + 3] = make_float2(re.w, im.w);
+        }
+#pragma unroll
+        for (int c = 0; c < DG; c++)
+            if (c0 + c >= kb) a[c] = make_float2(0.f, 0.f);   // columns past the block: zero
+    } else {
+#pragma unroll
+        for (int c = 0; c < DG; c++) a[c] = make_float2(c0 + c == r ? 1.f : 0.f, 0.f);  // identity padding
     }
+    // ---- LU without pivoting ----
+    // a column group's 8 entries are contiguous in the padded row buffers
+    const int gofs = c0 + (c0 >> 3);
+    if (r == 0) {
+#pragma unroll
+        for (int c = 0; c < DG; c++) prow[0][gofs + c] = a[c];
+    }
+    if (c0 == 0) colb[0][r] = a[0];
     __syncthreads();
-    for (int j = 0; j < NB - 1; j++) {
-        const float2 p = a[j][j];
+    for (int j = 0; j < NB; j++) {
+        const int buf = j & 1;
+        const float2 *pb = prow[buf] + gofs;
+        float2 *pn = prow[buf ^ 1] + gofs;
+        const float2 p = prow[buf][padc(j)];
         const float den = p.x * p.x + p.y * p.y;
-        if (tid == 0 && !(den > 0.f)) atomicExch(err, 1);
-        const float2 pinv = make_float2(p.x / den, -p.y / den);
-        if (tid > j && tid < NB) a[tid][j] = cmulf(a[tid][j], pinv);
-        __syncthreads();
-        for (int e = tid; e < NB * NB; e += 1024) {
-            const int i = e / NB, c = e % NB;
-            if (i > j && c > j) {
-                const float2 l = a[i][j], u = a[j][c];
-                a[i][c].x -= l.x * u.x - l.y * u.y;
-                a[i][c].y -= l.x * u.y + l.y * u.x;
+        if (t == 0 && !(den > 0.f)) atomicExch(err, 1);
+        if (r > j && c0 + DG > j) {
+            const float rd = 1.0f / den;
+            const float2 l = cmulf(colb[buf][r], make_float2(p.x * rd, -p.y * rd));
+            if (c0 > j) {
+#pragma unroll
+                for (int c = 0; c < DG; c++) cfms(a[c], l, pb[c]);
+            } else {
+                const int jc = j - c0;   // 0..7: the pivot column inside this group
+#pragma unroll
+                for (int c = 0; c < DG; c++) {
+                    if (c == jc) a[c] = l;   // L entry
+                    else if (c > jc) cfms(a[c], l, pb[c]);
+                }
+            }
+            if (r == j + 1) {
+#pragma unroll
+                for (int c = 0; c < DG; c++) pn[c] = a[c];
+            }
+            const int nc = j + 1 - c0;   // next pivot column inside this group, if 0..7
+            if (nc >= 0 && nc < DG) {
+#pragma unroll
+                for (int c = 0; c < DG; c++)
+                    if (c == nc) colb[buf ^ 1][r] = a[c];
             }
         }
         __syncthreads();
     }
-    if (tid == 0) {
-        const float2 p = a[NB - 1][NB - 1];
-        if (!(p.x * p.x + p.y * p.y > 0.f)) atomicExch(err, 1);
-    }
-    for (int e = tid; e < NB * NB; e += 1024) {
-        const int i = e / NB, j = e % NB;
-        if (i < kb && j < kb) {
-            Ar[(size_t)(k + i) * ld + k + j] = a[i][j].x;
-            Ai[(size_t)(k + i) * ld + k + j] = a[i][j].y;
-        }
-    }
-    // Linv: unit lower; column c by forward substitution, 16 threads per column
-    const int c = tid >> 4, sub = tid & 15;
-    for (int i = 0; i < NB; i++) {
-        float2 s = make_float2(0.f, 0.f);
-        for (int j = c + sub; j < i; j += 16) {
-            const float2 l = a[i][j], x = w[j][c];
-            s.x += l.x * x.x - l.y * x.y;
-            s.y += l.x * x.y + l.y * x.x;
-        }
+    // factors: back to the planes and into shared memory
 #pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-            s.x += __shfl_xor_sync(0xffffffffu, s.x, o, 16);
-            s.y += __shfl_xor_sync(0xffffffffu, s.y, o, 16);
+    for (int c = 0; c < DG; c++) LU[r][c0 + c] = a[c];
+    if (r < kb) {
+        float4 *pr = reinterpret_cast<float4 *>(Ar + (size_t)(k + r) * ld + k + c0);
+        float4 *pi = reinterpret_cast<float4 *>(Ai + (size_t)(k + r) * ld + k + c0);
+        if (c0 + DG <= kb) {
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+                pr[v] = make_float4(a[4 * v].x, a[4 * v + 1].x, a[4 * v + 2].x, a[4 * v + 3].x);
+                pi[v] = make_float4(a[4 * v].y, a[4 * v + 1].y, a[4 * v + 2].y, a[4 * v + 3].y);
+            }
+        } else {
+            float *sr = Ar + (size_t)(k + r) * ld + k + c0, *si = Ai + (size_t)(k + r) * ld + k + c0;
+#pragma unroll
+            for (int c = 0; c < DG; c++)
+                if (c0 + c < kb) {
+                    sr[c] = a[c].x;
+                    si[c] = a[c].y;
+                }
         }
-        if (sub == 0) w[i][c] = (i < c) ? make_float2(0.f, 0.f) : (i == c ? make_float2(1.f, 0.f) : make_float2(-s.x, -s.y));
-        __syncthreads();
     }
-    for (int e = tid; e < NB * NB; e += 1024) Linv[e] = w[e / NB][e % NB];
     __syncthreads();
-    // Uinv: upper; column c by backward substitution
-    for (int i = NB - 1; i >= 0; i--) {
-        float2 s = make_float2(0.f, 0.f);
-        for (int j = i + 1 + sub; j <= c; j += 16) {
-            const float2 u = a[i][j], x = w[j][c];
-            s.x += u.x * x.x - u.y * x.y;
-            s.y += u.x * x.y + u.y * x.x;
-        }
+    if (t < NB) {
+        const float2 u = LU[t][t];
+        const float rd = 1.0f / (u.x * u.x + u.y * u.y);
+        rdiag[t] = make_float2(u.x * rd, -u.y * rd);
+    }
+    // ---- L^-1 (forward) and U^-1 (backward) in one sweep ----
+    float2 x[DG], y[DG];
 #pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-            s.x += __shfl_xor_sync(0xffffffffu, s.x, o, 16);
-            s.y += __shfl_xor_sync(0xffffffffu, s.y, o, 16);
-        }
-        if (sub == 0) {
-            float2 r = make_float2(0.f, 0.f);
-            if (i <= c) {
-                const float2 d = a[i][i];
-                const float den = d.x * d.x + d.y * d.y;
-                const float2 rhs = (i == c) ? make_float2(1.f - s.x, -s.y) : make_float2(-s.x, -s.y);
-                r = make_float2((rhs.x * d.x + rhs.y * d.y) / den, (rhs.y * d.x - rhs.x * d.y) / den);
+    for (int c = 0; c < DG; c++) {
+        x[c] = make_float2(c0 + c == r ? 1.f : 0.f, 0.f);
+        y[c] = x[c];
+    }
+    __syncthreads();
+    for (int s = 0; s < NB; s++) {
+        const int jl = s, ju = NB - 1 - s, buf = s & 1;
+        float2 *xb = xrow[buf] + gofs, *yb = yrow[buf] + gofs;
+        if (r == ju) {
+            const float2 dv = rdiag[ju];
+#pragma unroll
+            for (int c = 0; c < DG; c++) {
+                y[c] = cmulf(y[c], dv);
+                yb[c] = y[c];
             }
-            w[i][c] = r;
+        }
+        if (r == jl) {
+#pragma unroll
+            for (int c = 0; c < DG; c++) xb[c] = x[c];
         }
         __syncthreads();
+        // row jl of L^-1 is zero right of the diagonal, row ju of U^-1 left of it
+        if (r > jl && c0 <= jl) {
+            const float2 lr = LU[r][jl];
+            const int lim = jl - c0;   // columns c <= lim of this group
+            if (lim >= DG - 1) {
+#pragma unroll
+                for (int c = 0; c < DG; c++) cfms(x[c], lr, xb[c]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < DG; c++)
+                    if (c <= lim) cfms(x[c], lr, xb[c]);
+            }
+        }
+        if (r < ju && c0 + DG - 1 >= ju) {
+            const float2 ur = LU[r][ju];
+            const int lim = ju - c0;   // columns c >= lim of this group
+            if (lim <= 0) {
+#pragma unroll
+                for (int c = 0; c < DG; c++) cfms(y[c], ur, yb[c]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < DG; c++)
+                    if (c >= lim) cfms(y[c], ur, yb[c]);
+            }
+        }
     }
-    for (int e = tid; e < NB * NB; e += 1024) Uinv[e] = w[e / NB][e % NB];
+#pragma unroll
+    for (int c = 0; c < DG; c++) {
+        Linv[r * NB + c0 + c] = x[c];
+        Uinv[r * NB + c0 + c] = y[c];
+    }
 }
 
 // ---------------------------------------------------------------------------
 // Panels: U12 = Linv * A12 (row panel) and L21 = A21 * Uinv (column panel).
 // One 64x64 tile per CTA, in place.  blockIdx.y: 0 row panel, 1 column panel;
-// blockIdx.z: frequency.
+// blockIdx.z: frequency.  Thread (ty, tx) = (t / 16, t mod 16) computes rows
+// ty + 16a and columns tx + 16b (a, b < 4): the 16 threads of a half-warp
+// read 16 consecutive complex entries of a shared-memory row, which is
+// conflict-free for 64-bit loads.  Tiles are loaded with float4 reads of
+// the re/im planes (rows are 16-byte aligned: ld and the offsets are
+// multiples of 64).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, float *__restrict__ planes,
                                                 size_t pstride, int ld, const float2 *__restrict__ dinv,
@@ -181,31 +274,45 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     const int off = k + kb + blockIdx.x * NB;
     if (off >= N) return;
     const int ext = min(NB, N - off);
-    const float2 *inv = rowp ? Linv : Uinv;
-    for (int e = tid; e < NB * NB; e += 256) M[e / NB][e % NB] = inv[e];
-    for (int e = tid; e < NB * NB; e += 256) {
-        const int i = e / NB, j = e % NB;
-        float2 v = make_float2(0.f, 0.f);
-        if (rowp) {
-            if (i < kb && j < ext) v = make_float2(Ar[(size_t)(k + i) * ld + off + j], Ai[(size_t)(k + i) * ld + off + j]);
-        } else {
-            if (i < ext && j < kb) v = make_float2(Ar[(size_t)(off + i) * ld + k + j], Ai[(size_t)(off + i) * ld + k + j]);
+    const float4 *inv4 = reinterpret_cast<const float4 *>(rowp ? Linv : Uinv);   // 2 complex per float4
+    for (int e = tid; e < NB * NB / 2; e += 256) {
+        const float4 v = inv4[e];
+        const int i = (2 * e) / NB, j = (2 * e) % NB;
+        M[i][j] = make_float2(v.x, v.y);
+        M[i][j + 1] = make_float2(v.z, v.w);
+    }
+    // tile rows: row panel rows k..k+kb (columns off..off+ext); column panel rows off..off+ext (columns k..k+kb)
+    const int nrow = rowp ? kb : ext, ncol = rowp ? ext : kb;
+    const size_t base = rowp ? (size_t)k * ld + off : (size_t)off * ld + k;
+    for (int e = tid; e < NB * NB / 4; e += 256) {
+        const int i = e >> 4, j = (e & 15) * 4;
+        float4 re = make_float4(0.f, 0.f, 0.f, 0.f), im = re;
+        if (i < nrow && j < ncol) {
+            re = *reinterpret_cast<const float4 *>(Ar + base + (size_t)i * ld + j);
+            im = *reinterpret_cast<const float4 *>(Ai + base + (size_t)i * ld + j);
         }
-        T[i][j] = v;
+        T[i][j] = make_float2(re.x, im.x);
+        T[i][j + 1] = make_float2(re.y, im.y);
+        T[i][j + 2] = make_float2(re.z, im.z);
+        T[i][j + 3] = make_float2(re.w, im.w);
     }
     __syncthreads();
-    const int r0 = (tid >> 4) * 4, c0 = (tid & 15) * 4;
+    const int ty = tid >> 4, tx = tid & 15;
     float2 acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
+    // row panel: out = M * T; column panel: out = T * M
+    const float2(*X)[NB + 1] = rowp ? M : T;
+    const float2(*Y)[NB + 1] = rowp ? T : M;
+#pragma unroll 4
     for (int q = 0; q < NB; q++) {
         float2 x[4], y[4];
 #pragma unroll
         for (int a = 0; a < 4; a++) {
-            x[a] = rowp ? M[r0 + a][q] : T[r0 + a][q];
-            y[a] = rowp ? T[q][c0 + a] : M[q][c0 + a];
+            x[a] = X[ty + 16 * a][q];
+            y[a] = Y[q][tx + 16 * a];
         }
 #pragma unroll
         for (int a = 0; a < 4; a++)
@@ -219,17 +326,10 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) {
-            const int i = r0 + a, j = c0 + b;
-            if (rowp) {
-                if (i < kb && j < ext) {
-                    Ar[(size_t)(k + i) * ld + off + j] = acc[a][b].x;
-                    Ai[(size_t)(k + i) * ld + off + j] = acc[a][b].y;
-                }
-            } else {
-                if (i < ext && j < kb) {
-                    Ar[(size_t)(off + i) * ld + k + j] = acc[a][b].x;
-                    Ai[(size_t)(off + i) * ld + k + j] = acc[a][b].y;
-                }
+            const int i = ty + 16 * a, j = tx + 16 * b;
+            if (i < nrow && j < ncol) {
+                Ar[base + (size_t)i * ld + j] = acc[a][b].x;
+                Ai[base + (size_t)i * ld + j] = acc[a][b].y;
             }
         }
 }
@@ -434,7 +534,6 @@ __global__ void k_init_ctl(int B, char *__restrict__ ctl, double bnorm, const in
 efie_status set_smem_attrs() {
     static bool done = false;
     if (done) return EFIE_OK;
-    EFIE_CUDA(cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
     EFIE_CUDA(cudaFuncSetAttribute(k_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
     done = true;
@@ -467,19 +566,30 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(w.ctl.reserve(64 * (size_t)B + 64));
     EFIE_TRY(w.active.reserve(sizeof(int) * B));
     EFIE_TRY(efie_trsv_workspace(w));
+    EFIE_TRY(efie_gemm_workspace(w));
+    return EFIE_OK;
+}
+
+efie_status efie_mixed_factor_prepare(efie_ctx *ctx, SolveWork &w, const int *active_host) {
+    cudaStream_t s = ctx->stream;
+    EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 64 * (size_t)w.B, s));
+    EFIE_CUDA(cudaMemcpyAsync(w.active.p, active_host, sizeof(int) * w.B, cudaMemcpyHostToDevice, s));
     return EFIE_OK;
 }
 
 efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host) {
+    int nact = 0;
+    for (int f = 0; f < w.B; f++) nact += active_host[f] ? 1 : 0;
+    EFIE_TRY(efie_mixed_factor_prepare(ctx, w, active_host));
+    return efie_mixed_factor_launch(ctx, w, Z, zstride, nact);
+}
+
+efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, int nact) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int N = w.N, ld = w.ld, B = w.B;
     float *planes = w.planes.as<float>();
     char *ctl = w.ctl.as<char>();
-    int nact = 0;
-    for (int f = 0; f < B; f++) nact += active_host[f] ? 1 : 0;
-    EFIE_CUDA(cudaMemsetAsync(w.ctl.p, 0, 64 * (size_t)B, s));
-    EFIE_CUDA(cudaMemcpyAsync(w.active.p, active_host, sizeof(int) * B, cudaMemcpyHostToDevice, s));
     const int *active = w.active.as<int>();
     dim3 tg((N + 31) / 32, (N + 31) / 32, B);
     size_t tok = log.begin(s);
@@ -497,8 +607,7 @@ efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
             const int bi = k / NB, kb = std::min(NB, N - k);
             const int s1 = k + kb, rest = N - s1;
             tok = log.begin(s);
-            k_diag_factor<<<B, 1024, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl,
-                                                     active);
+            k_diag_factor<<<B, 512, 0, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
             if (rest > 0) {
                 dim3 pg((rest + NB - 1) / NB, 2, B);
                 k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, active);

@@ -38,6 +38,13 @@ struct RefineResult {
 int efie_solve_nb();
 efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer);
 efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const int *active_host);
+// The two halves of efie_mixed_factor: host-side set-up of a batch (control
+// blocks, active mask), then the kernel sequence alone -- no allocation, no
+// host copy, no synchronisation -- which plan_run captures once into a CUDA
+// graph and replays for every batch.
+efie_status efie_mixed_factor_prepare(efie_ctx *ctx, SolveWork &w, const int *active_host);
+efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, int nact);
+efie_status efie_gemm_workspace(SolveWork &w);
 efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
                               double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
 // Flexible GMRES on Z x = b with the complex64 LU as right preconditioner;

@@ -6,7 +6,9 @@ Pieces:
 * ``PatchDesign`` / ``sample_designs``: parametric patch-over-ground designs
   (W, L, h, feed offset) meshed with the library's own producers;
 * ``Surrogate``: the MLP of ``csrc/surrogate.cu`` (CUDA forward, backward and
-  Adam; C ABI ``efie_mlp_*``) from normalised (W, L, h, feed, f) to Zin/Z_SCALE;
+  Adam; C ABI ``efie_mlp_*``) from normalised (W, L, h, feed, f) to
+  (log|Zin/Z_SCALE|, cos arg Zin, sin arg Zin), a target whose error is a
+  relative error of Zin at every magnitude;
 * ``generate_samples``: training data from the EFIE solver itself;
 * ``adaptive_sweep``: the surrogate proposes where the |S11| minimum is, the
   EFIE solver checks batches of points there, and the surrogate corrected by
@@ -30,7 +32,8 @@ from .api import (SweepPlan, build_rwg_interior, make_patch_with_ground_mesh, pi
 MU0 = 4.0 * math.pi * 1e-7
 C0 = 299792458.0
 EPS0 = 1.0 / (MU0 * C0 * C0)
-Z_SCALE = 50.0        # Zin / Z_SCALE is the network's target
+Z_SCALE = 50.0        # |Zin| is learned as log(|Zin| / Z_SCALE)
+N_OUT = 3             # log|Zin|, cos(arg Zin), sin(arg Zin)
 BAND = 0.2            # sweeps cover f0 (1 +- BAND), f0 = c / (2 L)
 
 
@@ -111,13 +114,17 @@ def features(d: PatchDesign, freqs):
 
 
 def zin_to_target(Zin):
-    Zin = np.asarray(Zin).reshape(-1)
-    return np.stack([Zin.real, Zin.imag], axis=1).astype(np.float32) / Z_SCALE
+    Zin = np.asarray(Zin, dtype=np.complex128).reshape(-1)
+    a = np.abs(Zin)
+    ph = Zin / np.where(a > 0, a, 1.0)
+    return np.stack([np.log(np.maximum(a, 1e-300) / Z_SCALE), ph.real, ph.imag], axis=1).astype(np.float32)
 
 
 def target_to_zin(T):
     T = np.asarray(T, dtype=np.float64)
-    return Z_SCALE * (T[:, 0] + 1j * T[:, 1])
+    u = T[:, 1] + 1j * T[:, 2]
+    n = np.abs(u)
+    return Z_SCALE * np.exp(T[:, 0]) * u / np.where(n > 0, n, 1.0)
 
 
 def s11(Zin, Z0=50.0):
@@ -130,7 +137,7 @@ def s11(Zin, Z0=50.0):
 class Surrogate:
     """The MLP of csrc/surrogate.cu (BF16 weights, FP32 accumulate)."""
 
-    def __init__(self, n_in=5, n_hidden=256, n_layers=4, n_out=2, seed=1):
+    def __init__(self, n_in=5, n_hidden=256, n_layers=4, n_out=N_OUT, seed=1):
         cfg = nat.EfieMlpConfig(n_in, n_hidden, n_layers, n_out, seed)
         h = C.c_void_p()
         nat.check(nat.lib().efie_mlp_create(nat.context(), C.byref(cfg), C.byref(h)))
@@ -254,22 +261,28 @@ def _interp_correction(fs, dz, fq):
     return CubicSpline(fs, dz.real)(fq) + 1j * CubicSpline(fs, dz.imag)(fq)
 
 
-def adaptive_sweep(d: PatchDesign, net: Surrogate, plan=None, n_points=8, tol=1e-3, max_rounds=3, n_dense=201,
+def adaptive_sweep(d: PatchDesign, net: Surrogate, plan=None, n_points=8, tol=1e-3, max_rounds=4, n_dense=201,
                    span=0.04):
     """Locate the |S11| minimum of a design with few EFIE solves.
 
     Round 1 solves n_points around the surrogate's predicted minimum (spread
-    over +-span * f0); later rounds solve n_points around the current
+    over +-span * f0); each later round solves n_points around the current
     estimate with half the previous spread.  Between solved points the curve
     is the surrogate plus an interpolant of its error at the solved points.
-    The sweep stops when the corrected surrogate predicted the new round's
-    solved Zin within ``tol`` (relative) and the minimum lies inside the solved
-    window; otherwise, after max_rounds, it falls back to the dense plain
-    sweep of n_dense points.
+    A round converges when the minimum is bracketed by solved points (or sits
+    at a band edge a solved point reaches) and either the corrected surrogate
+    predicted the round's new solves within ``tol`` (relative |dZin|) or the
+    minimum moved by less than 0.1 dense-grid step since the previous round.
+    Other dips of the raw surrogate that come within its observed |S11| error
+    of the found minimum are then solved too (n_points / 2 each), so that a
+    secondary minimum is not taken for the global one.  Without convergence
+    after max_rounds the sweep falls back to the dense plain sweep of n_dense
+    points (the full solve).
     """
     own = plan is None
     plan = plan or design_plan(d)
     fq = d.band(4 * (n_dense - 1) + 1)
+    step = (fq[-1] - fq[0]) / (n_dense - 1)
     zs = net.predict_zin(d, fq)
     f_est = _refine_min(fq, np.abs(s11(zs)))
     lo, hi = fq[0], fq[-1]
@@ -279,27 +292,52 @@ def adaptive_sweep(d: PatchDesign, net: Surrogate, plan=None, n_points=8, tol=1e
     rounds = 0
     converged = False
     err_pred = np.inf
+
+    def corrected(fs, zsol):
+        return zs + _interp_correction(fs, zsol - net.predict_zin(d, fs), fq)
+
+    def solve(new):
+        nonlocal fs, zsol
+        new = np.setdiff1d(np.unique(np.clip(new, lo, hi)), fs)
+        if new.size == 0:
+            return new, np.zeros(0, complex)
+        zn, _ = plan.run(new)
+        fs = np.concatenate([fs, new])
+        zsol = np.concatenate([zsol, zn])
+        return new, zn
+
     while rounds < max_rounds:
         rounds += 1
-        new = np.clip(f_est + sp * np.linspace(-1.0, 1.0, n_points), lo, hi)
-        new = np.setdiff1d(np.unique(new), fs)
+        cand = f_est + sp * np.linspace(-1.0, 1.0, n_points)
+        pred_all = corrected(fs, zsol) if fs.size else zs
+        new, zn = solve(cand)
         if new.size == 0:
             break
         # the corrected surrogate's prediction of the new points, before solving them
-        pred = net.predict_zin(d, new)
-        if fs.size:
-            pred = pred + _interp_correction(fs, zsol - net.predict_zin(d, fs), new)
-        zn, _ = plan.run(new)
+        pred = np.interp(new, fq, pred_all.real) + 1j * np.interp(new, fq, pred_all.imag)
         err_pred = float(np.max(np.abs(pred - zn) / np.abs(zn)))
-        fs = np.concatenate([fs, new])
-        zsol = np.concatenate([zsol, zn])
-        zc = zs + _interp_correction(fs, zsol - net.predict_zin(d, fs), fq)
-        f_est = _refine_min(fq, np.abs(s11(zc)))
-        inside = fs.min() < f_est < fs.max()
-        if err_pred <= tol and inside:
+        f_prev = f_est
+        f_est = _refine_min(fq, np.abs(s11(corrected(fs, zsol))))
+        tol_f = 1e-9 * d.f0
+        inside = (fs.min() < f_est < fs.max()) or (f_est <= lo + tol_f and fs.min() <= lo + tol_f) or \
+                 (f_est >= hi - tol_f and fs.max() >= hi - tol_f)
+        stable = rounds > 1 and abs(f_est - f_prev) <= 0.1 * step
+        if inside and (err_pred <= tol or stable):
             converged = True
             break
         sp *= 0.5
+    if converged:
+        # other dips of the surrogate within its observed error of the found minimum
+        s_raw = np.abs(s11(zs))
+        s_at = np.abs(s11(net.predict_zin(d, fs)))
+        delta = 3.0 * float(np.max(np.abs(s_at - np.abs(s11(zsol)))))
+        best = float(np.min(np.abs(s11(corrected(fs, zsol)))))
+        i = np.arange(1, fq.size - 1)
+        dips = i[(s_raw[i] <= s_raw[i - 1]) & (s_raw[i] <= s_raw[i + 1])]
+        dips = [fq[k] for k in dips if s_raw[k] <= best + delta and not (fs.min() <= fq[k] <= fs.max())]
+        for c in sorted(dips, key=lambda f: np.interp(f, fq, s_raw))[:3]:
+            solve(c + 0.5 * span * d.f0 * np.linspace(-1.0, 1.0, max(2, n_points // 2)))
+        f_est = _refine_min(fq, np.abs(s11(corrected(fs, zsol))))
     result = dict(f_min=f_est, solves=int(fs.size), rounds=rounds, converged=converged, err_pred=err_pred,
                   fallback=False, freqs=fs, Zin=zsol)
     if not converged:
