@@ -402,7 +402,8 @@ __global__ void __launch_bounds__(256) k_update_simt(int N, int r0, int r1, int 
 __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restrict__ Zb, size_t zstride,
                                                   const double2 *__restrict__ xb, const double2 *__restrict__ b,
                                                   float2 *__restrict__ rfb, int vstride, char *__restrict__ ctl,
-                                                  double tol, double2 *__restrict__ routb) {
+                                                  double tol, double2 *__restrict__ routb,
+                                                  double *__restrict__ partb) {
     const int f = blockIdx.y;
     char *c = ctl + 64 * f;
     double *red = reinterpret_cast<double *>(c);
@@ -446,10 +447,13 @@ __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restri
         sq[lane] = q;
     }
     __syncthreads();
+    // per-CTA partial sums, added in CTA order by the last CTA: the norm (and
+    // with it every later rounding) does not depend on the CTA schedule
+    double *part_f = partb + (size_t)gridDim.x * f;
     if (threadIdx.x == 0) {
         double q = 0.0;
         for (int i = 0; i < 32; i++) q += sq[i];
-        atomicAdd(red, q);
+        part_f[blockIdx.x] = q;
         __threadfence();
         const unsigned int done = atomicAdd(counter, 1u);
         last = (done == gridDim.x - 1);
@@ -457,7 +461,9 @@ __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restri
     __syncthreads();
     if (last && threadIdx.x == 0) {
         __threadfence();
-        const double rr = sqrt(*((volatile double *)red));
+        double acc = 0.0;
+        for (unsigned int i = 0; i < gridDim.x; i++) acc += ((volatile double *)part_f)[i];
+        const double rr = sqrt(acc);
         const double rel = rr / red[1];
         red[2] = rel;
         red[0] = 0.0;
@@ -564,6 +570,7 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(w.dinv.reserve(sizeof(float2) * w.dstride * B));
     EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.vstride * B));
     EFIE_TRY(w.ctl.reserve(64 * (size_t)B + 64));
+    EFIE_TRY(w.rpart.reserve(sizeof(double) * (size_t)B * ((N + 31) / 32)));
     EFIE_TRY(w.active.reserve(sizeof(int) * B));
     EFIE_TRY(efie_trsv_workspace(w));
     EFIE_TRY(efie_gemm_workspace(w));
@@ -661,7 +668,8 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
     dim3 rg((N + 31) / 32, B);
     tok = log.begin(s);
     k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, static_cast<const double2 *>(x),
-                                  static_cast<const double2 *>(b), rf, w.vstride, ctl, -1.0, nullptr);
+                                  static_cast<const double2 *>(b), rf, w.vstride, ctl, -1.0, nullptr,
+                                  w.rpart.as<double>());
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
     int it = 0;
@@ -679,7 +687,7 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
             tok = log.begin(s);
             k_residual<<<rg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride,
                                           static_cast<const double2 *>(x), static_cast<const double2 *>(b), rf,
-                                          w.vstride, ctl, tol, nullptr);
+                                          w.vstride, ctl, tol, nullptr, w.rpart.as<double>());
             EFIE_CUDA(cudaGetLastError());
             log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
         }
@@ -713,7 +721,7 @@ efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_
     size_t tok = ctx->log.begin(s);
     k_residual<<<rg, 256, 0, s>>>(w.N, static_cast<const double2 *>(Z), zstride, static_cast<const double2 *>(x),
                                   static_cast<const double2 *>(b), w.vec.as<float2>(), w.vstride, w.ctl.as<char>(),
-                                  tol, static_cast<double2 *>(rout));
+                                  tol, static_cast<double2 *>(rout), w.rpart.as<double>());
     EFIE_CUDA(cudaGetLastError());
     ctx->log.end(EFIE_K_RESIDUAL, s, tok, 16.0 * (double)w.N * w.N * nact);
     return EFIE_OK;

@@ -19,6 +19,7 @@ struct SolveWork {
     DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]
     DevBuf prog;     // triangular-solve progress counters: u64 [2][B][grid] on 64-byte lines
     DevBuf ctl;      // per f 64 bytes: red[3] @0, counter @24, conv @28, skip @32, err @36
+    DevBuf rpart;    // residual-norm partial sums: double [B][ceil(N/32)]
     DevBuf active;   // int[B]: slot holds a frequency of this batch
     DevBuf packA, packB;  // tensor-core operand staging
     // flexible GMRES (gmres.cu): Krylov basis V [M+1][B][N] and preconditioned
