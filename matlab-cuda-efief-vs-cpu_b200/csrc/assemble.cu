@@ -42,10 +42,18 @@ __device__ __forceinline__ size_t pair_slot(int t1, int t2, int Nt, bool sym) {
     return (size_t)hi * (size_t)(hi + 1) / 2 + (size_t)lo;
 }
 
-__device__ __forceinline__ void store_mom(double *dst, const double *a) {
-    double2 *d2 = reinterpret_cast<double2 *>(dst);
+// Triangle-pair moments, component-major: component c (S0, S1x, S1y, S1z, S2x,
+// S2y, S2z, S3; complex) of pair slot q at p[c * stride + q].  Consecutive
+// threads handle consecutive slots, so every store and every gather load is
+// a coalesced run of 16-byte values.
+struct MomStore {
+    double2 *p;
+    size_t stride;
+};
+
+__device__ __forceinline__ void store_mom(MomStore M, size_t slot, const double *a) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) d2[i] = make_double2(a[2 * i], a[2 * i + 1]);
+    for (int i = 0; i < 8; i++) M.p[(size_t)i * M.stride + slot] = make_double2(a[2 * i], a[2 * i + 1]);
 }
 
 // ---------------------------------------------------------------------------
@@ -56,7 +64,7 @@ __device__ __forceinline__ void store_mom(double *dst, const double *a) {
 template <int NQ>
 __global__ void __launch_bounds__(256) k_regular_moments(
     int Nt, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
-    const uint8_t *__restrict__ skip, double kr, double ki, double *__restrict__ mom) {
+    const uint8_t *__restrict__ skip, double kr, double ki, MomStore mom) {
     __shared__ double4 sp[8][NQ];
     __shared__ double4 so[8];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -115,13 +123,13 @@ __global__ void __launch_bounds__(256) k_regular_moments(
         m[14] += w * (pq.x * t1r[0] + pq.y * t1r[1] + pq.z * t1r[2]);
         m[15] += w * (pq.x * t1i[0] + pq.y * t1i[1] + pq.z * t1i[2]);
     }
-    store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+    store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
 }
 
 // Generic point count (any Nq a prepack may carry).
 __global__ void __launch_bounds__(256) k_regular_moments_any(
     int Nt, int Nq, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
-    const uint8_t *__restrict__ skip, double kr, double ki, double *__restrict__ mom) {
+    const uint8_t *__restrict__ skip, double kr, double ki, MomStore mom) {
     const int t1 = blockIdx.x * 32 + (threadIdx.x & 31);
     const int t2 = blockIdx.y * 8 + (threadIdx.x >> 5);
     if (t1 >= Nt || t2 >= Nt) return;
@@ -151,7 +159,7 @@ __global__ void __launch_bounds__(256) k_regular_moments_any(
             m[14] += gr * dd; m[15] += gi * dd;
         }
     }
-    store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+    store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -182,7 +190,7 @@ __device__ __forceinline__ void acc_qpe(double *m, const double4 &pp, const doub
 __global__ void __launch_bounds__(256) k_near_moments(
     int Nt, bool sym, int n_pairs, const int2 *__restrict__ list, int P,
     const double4 *__restrict__ origin, const double4 *__restrict__ pts, const double *__restrict__ aeq,
-    double near_alpha, double kr, double ki, double *__restrict__ mom) {
+    double near_alpha, double kr, double ki, MomStore mom) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n_pairs) return;
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(256) k_near_moments(
     }
 #pragma unroll
     for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
-    if (lane == 0) store_mom(mom + 16 * pair_slot(t1, t2, Nt, sym), m);
+    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
 }
 
 // ---------------------------------------------------------------------------
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(256) k_near_moments(
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_self_moments(
     int Nt, bool sym, int P, int Nq2, const double4 *__restrict__ pts, const double *__restrict__ self_a,
-    int NsS, double kr, double ki, double *__restrict__ mom) {
+    int NsS, double kr, double ki, MomStore mom) {
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (t >= Nt) return;
@@ -247,7 +255,7 @@ __global__ void __launch_bounds__(256) k_self_moments(
     }
 #pragma unroll
     for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
-    if (lane == 0) store_mom(mom + 16 * pair_slot(t, t, Nt, sym), m);
+    if (lane == 0) store_mom(mom, pair_slot(t, t, Nt, sym), m);
 }
 
 // ---------------------------------------------------------------------------
@@ -320,7 +328,7 @@ __device__ __forceinline__ void smooth_green(double kr, double ki, double R, dou
 __global__ void __launch_bounds__(256) k_singular_moments(
     int Nt, int n_pairs, const int2 *__restrict__ list, int NQ, const double4 *__restrict__ origin,
     const double4 *__restrict__ pts, const double4 *__restrict__ vtx, double kr, double ki,
-    double *__restrict__ mom) {
+    MomStore mom) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n_pairs) return;
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(256) k_singular_moments(
             m[i + 6] = s;
         }
     }
-    if (lane == 0) store_mom(mom + 16 * pair_slot(t1, t2, Nt, true), m);
+    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, true), m);
 }
 
 // ---------------------------------------------------------------------------
@@ -379,7 +387,7 @@ __global__ void __launch_bounds__(256) k_singular_moments(
 // in the reference's (im, in) order (kernel_Z_fastquad, fastquad.cu:373-409).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double2 z_entry(int m, int n, int Ne, int Nt, bool sym, const int *__restrict__ etri,
-                                           const double4 *__restrict__ ecd, const double *__restrict__ mom,
+                                           const double4 *__restrict__ ecd, const MomStore mom,
                                            double alr, double ali, double ber, double bei) {
     double zr = 0.0, zi = 0.0;
 #pragma unroll
@@ -392,9 +400,11 @@ __device__ __forceinline__ double2 z_entry(int m, int n, int Ne, int Nt, bool sy
             const int t2 = etri[b * Ne + n];
             if (t2 < 0) continue;
             const double4 dn = ecd[b * Ne + n];
-            const double2 *s = reinterpret_cast<const double2 *>(mom + 16 * pair_slot(t1, t2, Nt, sym));
-            const double2 S0 = s[0], S3 = s[7];
-            double2 S1x = s[1], S1y = s[2], S1z = s[3], S2x = s[4], S2y = s[5], S2z = s[6];
+            const double2 *s = mom.p + pair_slot(t1, t2, Nt, sym);
+            const size_t q = mom.stride;
+            const double2 S0 = __ldg(s), S3 = __ldg(s + 7 * q);
+            double2 S1x = __ldg(s + q), S1y = __ldg(s + 2 * q), S1z = __ldg(s + 3 * q), S2x = __ldg(s + 4 * q),
+                    S2y = __ldg(s + 5 * q), S2z = __ldg(s + 6 * q);
             if (sym && t1 > t2) {  // stored for (t2, t1): swap the one-sided moments
                 double2 tx = S1x, ty = S1y, tz = S1z;
                 S1x = S2x; S1y = S2y; S1z = S2z;
@@ -418,7 +428,7 @@ __device__ __forceinline__ double2 z_entry(int m, int n, int Ne, int Nt, bool sy
 // Thread per entry, m fastest (column-major Z, coalesced stores).
 __global__ void __launch_bounds__(256) k_gather_z(
     int Ne, int Nt, bool sym, const int *__restrict__ etri, const double4 *__restrict__ ecd,
-    const double *__restrict__ mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+    const MomStore mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
     const int m = blockIdx.x * 64 + (threadIdx.x & 63);
     const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
     if (m >= Ne || n >= Ne) return;
@@ -429,7 +439,7 @@ __global__ void __launch_bounds__(256) k_gather_z(
 // evaluated; an off-diagonal tile is also stored transposed through shared
 // memory, so Z(n,m) is a bit-exact copy of Z(m,n).
 __global__ void __launch_bounds__(256) k_gather_z_sym(
-    int Ne, int Nt, const int *__restrict__ etri, const double4 *__restrict__ ecd, const double *__restrict__ mom,
+    int Ne, int Nt, const int *__restrict__ etri, const double4 *__restrict__ ecd, const MomStore mom,
     double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
     const int bm = blockIdx.x, bn = blockIdx.y;
     if (bm > bn) return;
@@ -680,7 +690,7 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     }
     EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
-    EFIE_TRY(g.moments.reserve(sizeof(double) * 16 * g.npairs));
+    EFIE_TRY(g.moments.reserve(sizeof(double2) * 8 * g.npairs));   // 8 component planes of npairs
     return EFIE_OK;
 }
 
@@ -688,7 +698,7 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int Nt = g.Nt, Ne = g.Ne;
-    double *mom = g.moments.as<double>();
+    const MomStore mom{g.moments.as<double2>(), g.npairs};
     dim3 grid((Nt + 31) / 32, (Nt + 7) / 8);
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();

@@ -161,7 +161,7 @@ struct GeomDev {
     DevBuf tri_vtx;           // double4[3*Nt] vertices relative to origin (extraction scheme)
     DevBuf adj_list;          // int2[] vertex-adjacent pairs t1 < t2 (extraction scheme)
     int n_adj = 0;
-    DevBuf moments;           // double[16 * npairs]
+    DevBuf moments;           // double2[8][npairs]: component-major triangle-pair moments
     size_t npairs = 0;
 };
 

@@ -12,13 +12,15 @@
 // Operands are packed per LU step into 64B-swizzled K-major tiles (16 TF32
 // per row) that sit contiguously in global memory, so each CTA fetches them
 // with plain bulk copies (cp.async.bulk, the TMA engine; no multicast, local
-// memory only).  One CTA computes a 128 x 256 accumulator tile (64 complex
-// rows x 256 complex columns): one elected thread issues tcgen05.mma over a
-// 4-stage shared-memory ring of K' chunks -- it issues chunk c's MMAs before
-// waiting for chunk c-1's to retire, so the tensor pipe always holds queued
-// work while the bulk loads run three chunks ahead -- and all four warps drain
-// TMEM with tcgen05.ld for the read-modify-write epilogue on the row-major
-// planes.
+// memory only).  One CTA computes two 128 x 256 accumulator tiles (2 x 64
+// complex rows x 256 complex columns) in the 512 TMEM columns of its SM, both
+// fed by the same B chunk, which halves the B bytes per MMA.  One elected
+// thread issues tcgen05.mma over a 3-stage shared-memory ring of K' chunks --
+// it issues chunk c's MMAs before waiting for chunk c-1's to retire, so the
+// tensor pipe always holds queued work while the bulk loads run ahead -- and
+// all four warps drain TMEM with tcgen05.ld for the read-modify-write
+// epilogue on the row-major planes, reading the next 32 columns of C while
+// they update the current ones.
 // Every mbarrier wait is bounded; a timeout sets the device error flag.
 #include <cstdint>
 
@@ -33,8 +35,9 @@ constexpr int KC = 16;           // fp32 elements per 64-byte swizzle row (one K
 constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 32 chunks
 constexpr int A_TILE = TM * KC;       // floats per A tile (8 KB)
 constexpr int B_TILE = TN * KC;       // floats per B tile (16 KB)
-constexpr int STAGE_FLOATS = 2 * A_TILE + 2 * B_TILE;   // hi/lo of A and B: 48 KB
-constexpr int NSTAGE = 4;
+constexpr int MT = 2;            // 128-row accumulator tiles per CTA (TMEM columns: MT x 256)
+constexpr int STAGE_FLOATS = MT * 2 * A_TILE + 2 * B_TILE;   // hi/lo of MT A tiles and of B: 64 KB
+constexpr int NSTAGE = 3;
 constexpr int NBAR = 2 * NSTAGE + 1;  // full[NSTAGE], empty[NSTAGE], done
 constexpr size_t GEMM_SMEM = sizeof(float) * NSTAGE * STAGE_FLOATS + 1024 + 8 * NBAR + 16;
 
@@ -218,7 +221,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // ---------------------------------------------------------------------------
 // The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk,
+// C[r0:r1, c0:c1] -= (packed A) * (packed B) for the CTA's tiles; grid
+// (column tiles, pairs of 64-row tiles, frequency), 128 threads.
+__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
                                                       const float *__restrict__ Apackb, size_t astride,
                                                       const float *__restrict__ Bpackb, size_t bstride,
                                                       float *__restrict__ planes, size_t pstride, int ld,
@@ -236,7 +241,8 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + NBAR);
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile_n = blockIdx.x, tile_m = blockIdx.y;
+    const int tile_n = blockIdx.x, tile_m0 = blockIdx.y * MT;
+    const int nm = min(MT, mt - tile_m0);            // accumulator tiles of this CTA (1 or 2)
 
     if (tid == 0) {
         for (int i = 0; i < NBAR; i++) mbar_init(&bars[i], 1);
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TN));
+                     "r"(MT * TN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -255,14 +261,15 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
     bool ok = true;
     if (tid == 0) *ok_sh = 1;
     if (tid == 0) {
-        const float *ga = Apack + (size_t)tile_m * nchunk * 2 * A_TILE;
         const float *gb = Bpack + (size_t)tile_n * nchunk * 2 * B_TILE;
-        const uint32_t bytes = sizeof(float) * (2 * A_TILE + 2 * B_TILE);
+        const uint32_t abytes = sizeof(float) * 2 * A_TILE, bbytes = sizeof(float) * 2 * B_TILE;
         auto load = [&](int c) {
             float *st = stage + (c % NSTAGE) * STAGE_FLOATS;
-            mbar_expect_tx(&full[c % NSTAGE], bytes);
-            bulk_g2s(st, ga + (size_t)c * 2 * A_TILE, sizeof(float) * 2 * A_TILE, &full[c % NSTAGE]);
-            bulk_g2s(st + 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, sizeof(float) * 2 * B_TILE, &full[c % NSTAGE]);
+            mbar_expect_tx(&full[c % NSTAGE], nm * abytes + bbytes);
+            for (int mi = 0; mi < nm; mi++)
+                bulk_g2s(st + mi * 2 * A_TILE, Apack + ((size_t)(tile_m0 + mi) * nchunk + c) * 2 * A_TILE, abytes,
+                         &full[c % NSTAGE]);
+            bulk_g2s(st + MT * 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, bbytes, &full[c % NSTAGE]);
         };
         for (int c = 0; c < NSTAGE && c < nchunk; c++) load(c);
         for (int c = 0; c < nchunk && ok; c++) {
@@ -270,15 +277,18 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
             if (!mbar_wait(&full[sidx], (c / NSTAGE) & 1, err)) { ok = false; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const float *st = stage + sidx * STAGE_FLOATS;
-            const uint64_t ahi = desc_sw64(st), alo = desc_sw64(st + A_TILE);
-            const uint64_t bhi = desc_sw64(st + 2 * A_TILE), blo = desc_sw64(st + 2 * A_TILE + B_TILE);
+            const uint64_t bhi = desc_sw64(st + MT * 2 * A_TILE), blo = desc_sw64(st + MT * 2 * A_TILE + B_TILE);
+            for (int mi = 0; mi < nm; mi++) {
+                const uint64_t ahi = desc_sw64(st + mi * 2 * A_TILE), alo = desc_sw64(st + mi * 2 * A_TILE + A_TILE);
+                const uint32_t acc = tmem + (uint32_t)(mi * TN);
 #pragma unroll
-            for (int kk = 0; kk < KC / 8; kk++) {
-                const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
-                // small terms first, then the leading product
-                mma_tf32(tmem, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
-                mma_tf32(tmem, ahi + adv, blo + adv, 1u);
-                mma_tf32(tmem, ahi + adv, bhi + adv, 1u);
+                for (int kk = 0; kk < KC / 8; kk++) {
+                    const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+                    // small terms first, then the leading product
+                    mma_tf32(acc, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
+                    mma_tf32(acc, ahi + adv, blo + adv, 1u);
+                    mma_tf32(acc, ahi + adv, bhi + adv, 1u);
+                }
             }
             mma_commit(&empty[sidx]);   // stage sidx free once these MMAs have read it
             // refill the stage of chunk c - 1: its MMAs were queued ahead of chunk
@@ -289,50 +299,69 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
                 load(cp + NSTAGE);
             }
         }
-        mma_commit(done);                  // all MMAs of this tile done
+        mma_commit(done);                  // all MMAs of this CTA done
         if (!ok) *ok_sh = 0;
     }
     __syncthreads();
-    // every thread waits for the accumulator (bounded); the decision is made
+    // every thread waits for the accumulators (bounded); the decision is made
     // uniform per warp because tcgen05.ld is a warp-collective instruction
     bool have = mbar_wait(done, 0, err);
     have = __all_sync(0xffffffffu, have) && (*ok_sh != 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-        const int half = warp & 1;                  // rows 0-31 or 32-63 of the complex block
+        const int half = warp & 1;                  // rows 0-31 or 32-63 of a complex block
         float *plane = (warp < 2) ? Ar : Ai;        // warps 0,1: real part; 2,3: imaginary part
-        const int row = r0 + tile_m * 64 + half * 32 + lane;
-        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int j = 0; j < TN / 32; j++) {
-            uint32_t v[32];
-            tmem_ld32(tbase + j * 32, v);
-            const int col0 = c0 + tile_n * TN + j * 32;
-            if (row < r1 && col0 < c1) {
-                float *p = plane + (size_t)row * ld + col0;
-                if (col0 + 32 <= c1) {
-                    float4 *p4 = reinterpret_cast<float4 *>(p);
+        constexpr int NJ = TN / 32;
+        for (int mi = 0; mi < nm; mi++) {
+            const int row = r0 + (tile_m0 + mi) * 64 + half * 32 + lane;
+            const bool rok = row < r1;
+            const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mi * TN);
+            float *prow = plane + (size_t)(rok ? row : r0) * ld + c0 + tile_n * TN;
+            const int ncol = c1 - (c0 + tile_n * TN);   // valid columns of this tile (may exceed TN)
+            // C of chunk j + 1 is read while chunk j is updated
+            float4 cur[8], nxt[8];
+            auto fetch = [&](int j, float4 (&d)[8]) {
+                if (rok && (j + 1) * 32 <= ncol) {
+                    const float4 *p4 = reinterpret_cast<const float4 *>(prow + j * 32);
 #pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        float4 a = p4[q];
-                        a.x -= __uint_as_float(v[4 * q]);
-                        a.y -= __uint_as_float(v[4 * q + 1]);
-                        a.z -= __uint_as_float(v[4 * q + 2]);
-                        a.w -= __uint_as_float(v[4 * q + 3]);
-                        p4[q] = a;
-                    }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 32; q++)
-                        if (col0 + q < c1) p[q] -= __uint_as_float(v[q]);
+                    for (int q = 0; q < 8; q++) d[q] = p4[q];
                 }
+            };
+            fetch(0, cur);
+#pragma unroll 1
+            for (int j = 0; j < NJ; j++) {
+                if (j + 1 < NJ) fetch(j + 1, nxt);
+                uint32_t v[32];
+                tmem_ld32(tbase + j * 32, v);
+                const int col0 = j * 32;
+                if (rok && col0 < ncol) {
+                    float *p = prow + col0;
+                    if (col0 + 32 <= ncol) {
+                        float4 *p4 = reinterpret_cast<float4 *>(p);
+#pragma unroll
+                        for (int q = 0; q < 8; q++) {
+                            float4 a = cur[q];
+                            a.x -= __uint_as_float(v[4 * q]);
+                            a.y -= __uint_as_float(v[4 * q + 1]);
+                            a.z -= __uint_as_float(v[4 * q + 2]);
+                            a.w -= __uint_as_float(v[4 * q + 3]);
+                            p4[q] = a;
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 32; q++)
+                            if (col0 + q < ncol) p[q] -= __uint_as_float(v[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) cur[q] = nxt[q];
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MT * TN));
     }
 }
 
@@ -399,9 +428,9 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
-    k_update_tc<<<dim3(nt, mt, B), 128, GEMM_SMEM, st>>>(N, r0, r1, c0, c1, nchunk, w.packA.as<float>(), astride,
-                                                         w.packB.as<float>(), bstride, planes, w.pstride, w.ld,
-                                                         w.ctl.as<char>(), active);
+    k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 128, GEMM_SMEM, st>>>(
+        N, r0, r1, c0, c1, nchunk, mt, w.packA.as<float>(), astride, w.packB.as<float>(), bstride, planes, w.pstride,
+        w.ld, w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;
