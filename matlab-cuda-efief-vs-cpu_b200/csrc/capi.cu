@@ -338,7 +338,10 @@ efie_status plan_factor(efie_plan *p, const int *active, int nact) {
             if (g) cudaGraphDestroy(g);
             return st;
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&p->factor_graph, g, 0);
+        // keep the priorities of the capturing streams (the panel chain ahead of
+        // the bulk trailing updates) in the replayed graph
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiateWithFlags(&p->factor_graph, g, cudaGraphInstantiateFlagUseNodePriority);
         if (g) cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             p->factor_graph = nullptr;
@@ -462,6 +465,9 @@ extern "C" efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, co
     p->ctx = ctx;
     efie_status s = plan_common(p, mesh, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, opts);
     if (s == EFIE_OK) s = efie_geom_upload(ctx, mesh, pre, scheme, rule_order, p->g);
+    // a symmetric gather writes Z(n,m) as a copy of Z(m,n): the refinement's
+    // products then read only the upper triangle
+    if (s == EFIE_OK) p->sw.zsym = p->g.symmetric;
     if (s == EFIE_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         s = efie_fail(EFIE_ERR_CUDA, "geometry upload failed");
     if (s != EFIE_OK) {

@@ -17,10 +17,12 @@
 // fed by the same B chunk, which halves the B bytes per MMA.  One elected
 // thread issues tcgen05.mma over a 3-stage shared-memory ring of K' chunks --
 // it issues chunk c's MMAs before waiting for chunk c-1's to retire, so the
-// tensor pipe always holds queued work while the bulk loads run ahead -- and
-// all four warps drain TMEM with tcgen05.ld for the read-modify-write
-// epilogue on the row-major planes, reading the next 32 columns of C while
-// they update the current ones.
+// tensor pipe always holds queued work while the bulk loads run ahead.
+// Meanwhile the other warps prefetch the CTA's rows of C into L2 (bulk
+// prefetch), and at the end all eight warps drain TMEM with tcgen05.ld -- two
+// warps per TMEM lane quarter, each taking half of the columns -- for the
+// read-modify-write epilogue on the row-major planes, reading the next 32
+// columns of C while they update the current ones.
 // Every mbarrier wait is bounded; a timeout sets the device error flag.
 #include <cstdint>
 
@@ -222,8 +224,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
 // ---------------------------------------------------------------------------
 // C[r0:r1, c0:c1] -= (packed A) * (packed B) for the CTA's tiles; grid
-// (column tiles, pairs of 64-row tiles, frequency), 128 threads.
-__global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
+// (column tiles, pairs of 64-row tiles, frequency), 256 threads.
+__global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
                                                       const float *__restrict__ Apackb, size_t astride,
                                                       const float *__restrict__ Bpackb, size_t bstride,
                                                       float *__restrict__ planes, size_t pstride, int ld,
@@ -301,6 +303,18 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
         }
         mma_commit(done);                  // all MMAs of this CTA done
         if (!ok) *ok_sh = 0;
+    } else if (warp > 0) {
+        // C rows of this CTA into L2 while the MMAs run: (accumulator, plane, row) segments
+        const int ncol = min(TN, c1 - (c0 + tile_n * TN));
+        const uint32_t bytes = (uint32_t)((ncol * 4 + 15) & ~15);
+        for (int e = tid - 32; e < nm * 2 * 64; e += 224) {
+            const int mi = e >> 7, pl = (e >> 6) & 1, rr = e & 63;
+            const int row = r0 + (tile_m0 + mi) * 64 + rr;
+            if (row < r1 && ncol > 0) {
+                const float *src = (pl ? Ai : Ar) + (size_t)row * ld + c0 + tile_n * TN;
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+            }
+        }
     }
     __syncthreads();
     // every thread waits for the accumulators (bounded); the decision is made
@@ -309,13 +323,16 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
     have = __all_sync(0xffffffffu, have) && (*ok_sh != 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-        const int half = warp & 1;                  // rows 0-31 or 32-63 of a complex block
-        float *plane = (warp < 2) ? Ar : Ai;        // warps 0,1: real part; 2,3: imaginary part
+        // TMEM lane quarter of this warp (tcgen05.ld reaches lanes 32 (warp mod 4) ...)
+        const int quarter = warp & 3;
+        const int half = quarter & 1;               // rows 0-31 or 32-63 of a complex block
+        float *plane = (quarter < 2) ? Ar : Ai;     // quarters 0,1: real part; 2,3: imaginary part
         constexpr int NJ = TN / 32;
+        const int j0 = (warp >> 2) * (NJ / 2), j1 = j0 + NJ / 2;   // this warp's half of the columns
         for (int mi = 0; mi < nm; mi++) {
             const int row = r0 + (tile_m0 + mi) * 64 + half * 32 + lane;
             const bool rok = row < r1;
-            const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mi * TN);
+            const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mi * TN);
             float *prow = plane + (size_t)(rok ? row : r0) * ld + c0 + tile_n * TN;
             const int ncol = c1 - (c0 + tile_n * TN);   // valid columns of this tile (may exceed TN)
             // C of chunk j + 1 is read while chunk j is updated
@@ -327,10 +344,10 @@ __global__ void __launch_bounds__(128, 1) k_update_tc(int N, int r0, int r1, int
                     for (int q = 0; q < 8; q++) d[q] = p4[q];
                 }
             };
-            fetch(0, cur);
+            fetch(j0, cur);
 #pragma unroll 1
-            for (int j = 0; j < NJ; j++) {
-                if (j + 1 < NJ) fetch(j + 1, nxt);
+            for (int j = j0; j < j1; j++) {
+                if (j + 1 < j1) fetch(j + 1, nxt);
                 uint32_t v[32];
                 tmem_ld32(tbase + j * 32, v);
                 const int col0 = j * 32;
@@ -390,6 +407,8 @@ efie_status efie_gemm_workspace(SolveWork &w) {
     const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
     EFIE_TRY(w.packA.reserve(sizeof(float) * astride * w.B));
     EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * w.B));
+    EFIE_TRY(w.packA2.reserve(sizeof(float) * astride * w.B));
+    EFIE_TRY(w.packB2.reserve(sizeof(float) * bstride * w.B));
     return EFIE_OK;
 }
 
@@ -397,7 +416,7 @@ efie_status efie_gemm_workspace(SolveWork &w) {
 // active frequency: tensor cores when the block spans enough work, CUDA cores
 // otherwise.
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact) {
+                             int nact, int slot) {
     const int rows = r1 - r0, cols = c1 - c0;
     if (rows <= 0 || cols <= 0 || K <= 0) return EFIE_OK;
     const bool tc = !g_tc_disabled && K <= KMAX && (double)rows * cols >= 64.0 * 256.0 && cols >= 96;
@@ -414,23 +433,24 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     // per-frequency staging sized for the largest update of an N x N LU
     const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
     const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
-    EFIE_TRY(w.packA.reserve(sizeof(float) * astride * B));
-    EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * B));
+    DevBuf &pA = slot ? w.packA2 : w.packA, &pB = slot ? w.packB2 : w.packB;
+    EFIE_TRY(pA.reserve(sizeof(float) * astride * B));
+    EFIE_TRY(pB.reserve(sizeof(float) * bstride * B));
     float *planes = w.planes.as<float>();
     const int *active = w.active.as<int>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
     k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld,
-                                                  w.packA.as<float>(), astride, active);
+                                                  pA.as<float>(), astride, active);
     k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(float) * 2 * B_TILE, st>>>(N, c0, c1, krow, K, nchunk, planes,
-                                                                          w.pstride, w.ld, w.packB.as<float>(),
-                                                                          bstride, active);
+                                                                          w.pstride, w.ld, pB.as<float>(), bstride,
+                                                                          active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
-    k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 128, GEMM_SMEM, st>>>(
-        N, r0, r1, c0, c1, nchunk, mt, w.packA.as<float>(), astride, w.packB.as<float>(), bstride, planes, w.pstride,
-        w.ld, w.ctl.as<char>(), active);
+    k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 256, GEMM_SMEM, st>>>(
+        N, r0, r1, c0, c1, nchunk, mt, pA.as<float>(), astride, pB.as<float>(), bstride, planes, w.pstride, w.ld,
+        w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;

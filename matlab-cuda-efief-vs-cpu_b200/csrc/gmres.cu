@@ -339,7 +339,123 @@ __global__ void k_gm_reset_skip(int B, char *__restrict__ ctl, const int *__rest
     *ctl_skip(ctl, f) = *ctl_conv(ctl, f) || !active[f];
 }
 
+// ---------------------------------------------------------------------------
+// y_f = Z_f x_f for a symmetric Z_f (full column-major storage, upper
+// triangle read once).  Tile t = (I, J), I <= J, of ST x ST entries
+// (t = J (J + 1) / 2 + I): rows I, columns J.  It contributes Z_IJ x_J to y_I
+// and, off the diagonal, Z_IJ^T x_I to y_J; both partial vectors go to
+// P[f][t][2][ST] and k_symv_reduce adds them in a fixed order, so the
+// product is bit-reproducible.  Warp w takes the tile's columns w, w + 8, ...;
+// lane l its rows l + 32 q.  A frequency whose flag (flags[f * fstride]) is
+// set is skipped.
+// ---------------------------------------------------------------------------
+constexpr int ST = 128;
+
+__device__ __forceinline__ void tile_of(int t, int &I, int &J) {
+    int j = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((j + 1) * (j + 2) / 2 <= t) j++;
+    while (j * (j + 1) / 2 > t) j--;
+    J = j;
+    I = t - j * (j + 1) / 2;
+}
+
+__global__ void __launch_bounds__(256) k_symv_tiles(int N, const double2 *__restrict__ Zb, size_t zstride,
+                                                    const double2 *__restrict__ xb, double2 *__restrict__ P,
+                                                    const int *__restrict__ flags, int fstride) {
+    const int f = blockIdx.y;
+    if (flags[(size_t)f * fstride]) return;
+    int I, J;
+    tile_of(blockIdx.x, I, J);
+    const double2 *Z = Zb + zstride * f;
+    const double2 *x = xb + (size_t)N * f;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r0 = I * ST, c0 = J * ST;
+    __shared__ double2 rsum[8][ST];
+    __shared__ double2 csum[ST];
+    double2 xr[4], rs[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int m = r0 + lane + 32 * q;
+        xr[q] = m < N ? x[m] : make_double2(0.0, 0.0);
+        rs[q] = make_double2(0.0, 0.0);
+    }
+    for (int cc = warp; cc < ST; cc += 8) {
+        const int n = c0 + cc;
+        double2 cs = make_double2(0.0, 0.0);
+        if (n < N) {
+            const double2 xn = x[n];
+            const double2 *col = Z + (size_t)N * n;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int m = r0 + lane + 32 * q;
+                if (m < N) {
+                    const double2 a = col[m];
+                    rs[q].x += a.x * xn.x - a.y * xn.y;
+                    rs[q].y += a.x * xn.y + a.y * xn.x;
+                    cs.x += a.x * xr[q].x - a.y * xr[q].y;
+                    cs.y += a.x * xr[q].y + a.y * xr[q].x;
+                }
+            }
+        }
+        if (I != J) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cs.x += __shfl_xor_sync(0xffffffffu, cs.x, o);
+                cs.y += __shfl_xor_sync(0xffffffffu, cs.y, o);
+            }
+            if (lane == 0) csum[cc] = cs;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) rsum[warp][lane + 32 * q] = rs[q];
+    __syncthreads();
+    double2 *out = P + ((size_t)f * gridDim.x + blockIdx.x) * 2 * ST;
+    if (threadIdx.x < ST) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < 8; w++) {
+            t.x += rsum[w][threadIdx.x].x;
+            t.y += rsum[w][threadIdx.x].y;
+        }
+        out[threadIdx.x] = t;
+    } else if (I != J) {
+        out[threadIdx.x] = csum[threadIdx.x - ST];
+    }
+}
+
+// y_I = sum_{J >= I} (row part of tile (I, J)) + sum_{J < I} (column part of tile (J, I))
+__global__ void __launch_bounds__(ST) k_symv_reduce(int N, int nb, const double2 *__restrict__ P,
+                                                    double2 *__restrict__ yb, const int *__restrict__ flags,
+                                                    int fstride) {
+    const int f = blockIdx.y;
+    if (flags[(size_t)f * fstride]) return;
+    const int I = blockIdx.x, r = threadIdx.x, m = I * ST + r;
+    const size_t ntiles = (size_t)nb * (nb + 1) / 2;
+    const double2 *Pf = P + (size_t)f * ntiles * 2 * ST;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int J = 0; J < nb; J++) {
+        double2 v;
+        if (J < I) v = Pf[((size_t)I * (I + 1) / 2 + J) * 2 * ST + ST + r];   // tile (J, I), column part
+        else v = Pf[((size_t)J * (J + 1) / 2 + I) * 2 * ST + r];             // tile (I, J), row part
+        acc.x += v.x;
+        acc.y += v.y;
+    }
+    if (m < N) yb[(size_t)N * f + m] = acc;
+}
+
 inline unsigned cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+efie_status symv(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const double2 *x, double2 *y,
+                 const int *flags, int fstride) {
+    const int nb = (w.N + ST - 1) / ST;
+    const size_t ntiles = (size_t)nb * (nb + 1) / 2;
+    EFIE_TRY(w.spart.reserve(sizeof(double2) * ntiles * 2 * ST * w.B));
+    cudaStream_t s = ctx->stream;
+    k_symv_tiles<<<dim3((unsigned)ntiles, w.B), 256, 0, s>>>(w.N, static_cast<const double2 *>(Z), zstride, x,
+                                                              w.spart.as<double2>(), flags, fstride);
+    k_symv_reduce<<<dim3(nb, w.B), ST, 0, s>>>(w.N, nb, w.spart.as<double2>(), y, flags, fstride);
+    EFIE_CUDA(cudaGetLastError());
+    return EFIE_OK;
+}
 
 efie_status gm_workspace(SolveWork &w) {
     const size_t NB = (size_t)w.N * w.B;
@@ -349,6 +465,10 @@ efie_status gm_workspace(SolveWork &w) {
     EFIE_TRY(w.gw.reserve(sizeof(double2) * NB));
     EFIE_TRY(w.gpart.reserve(sizeof(double2) * (size_t)w.B * w.gnch * (GM_M + 1) + sizeof(double) * w.B * w.gnch));
     EFIE_TRY(w.gst.reserve(sizeof(GmState) * w.B));
+    if (w.zsym) {
+        const int nb = (w.N + ST - 1) / ST;
+        EFIE_TRY(w.spart.reserve(sizeof(double2) * ((size_t)nb * (nb + 1) / 2) * 2 * ST * w.B));
+    }
     return EFIE_OK;
 }
 
@@ -372,9 +492,17 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
     for (int f = 0; f < B; f++) nact += active_host[f] ? 1 : 0;
     const double zbytes = 16.0 * (double)N * N, lubytes = 8.0 * (double)N * N;
     const double tol_inner = 0.5 * tol;
+    const int *ctl_skip0 = reinterpret_cast<const int *>(ctl + 32);   // ctl skip flag of slot f: [16 f]
+    auto residual = [&]() -> efie_status {
+        if (!w.zsym) return efie_true_residual(ctx, w, Z, zstride, x, b, tol, V, nact);
+        size_t tk = log.begin(s);
+        EFIE_TRY(symv(ctx, w, Z, zstride, static_cast<const double2 *>(x), wv, ctl_skip0, 16));
+        log.end(EFIE_K_RESIDUAL, s, tk, 8.0 * (double)N * N * nact, 2);
+        return efie_residual_finish(ctx, w, wv, b, tol, V, nact);
+    };
     EFIE_TRY(efie_refine_init(ctx, w, x, bnorm));
-    // r0 = b (x = 0): the residual kernel also stores it at V slot 0
-    EFIE_TRY(efie_true_residual(ctx, w, Z, zstride, x, b, tol, V, nact));
+    // r0 = b (x = 0): the residual also stores it at V slot 0
+    EFIE_TRY(residual());
     std::vector<char> hctl(64 * (size_t)B);
     std::vector<int> hstop(B);
     int matvecs = 0;
@@ -395,9 +523,14 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
             EFIE_TRY(efie_trsv(ctx, w, false, yv, dv, zj, epoch));
             log.end(EFIE_K_TRSV, s, tok, lubytes * nact, 2);
             tok = log.begin(s);
-            k_gm_matvec<<<mg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, zj, wv, st);
-            EFIE_CUDA(cudaGetLastError());
-            log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
+            if (w.zsym) {
+                EFIE_TRY(symv(ctx, w, Z, zstride, zj, wv, &st[0].stop, (int)(sizeof(GmState) / sizeof(int))));
+                log.end(EFIE_K_RESIDUAL, s, tok, 0.5 * zbytes * nact, 2);
+            } else {
+                k_gm_matvec<<<mg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, zj, wv, st);
+                EFIE_CUDA(cudaGetLastError());
+                log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
+            }
             tok = log.begin(s);
             k_gm_zero_col<<<B, GM_M + 1, 0, s>>>(B, j, st);
             for (int pass = 0; pass < 2; pass++) {
@@ -432,7 +565,7 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
         EFIE_CUDA(cudaGetLastError());
         log.end(EFIE_K_OTHER, s, tok, 0.0, 3);
         // true residual; a restart begins from it
-        EFIE_TRY(efie_true_residual(ctx, w, Z, zstride, x, b, tol, V, nact));
+        EFIE_TRY(residual());
         EFIE_CUDA(cudaMemcpyAsync(hctl.data(), ctl, 64 * (size_t)B, cudaMemcpyDeviceToHost, s));
         EFIE_CUDA(cudaStreamSynchronize(s));
         all_conv = true;

@@ -475,6 +475,60 @@ __global__ void __launch_bounds__(256) k_residual(int N, const double2 *__restri
     }
 }
 
+// r_f = b - y_f for a precomputed y_f = Z_f x_f; the rest as k_residual
+// (complex64 copy, optional complex128 copy, ||r_f|| summed in CTA order by
+// the last CTA, convergence flags).  Block = 256 rows, grid (rows / 256, B).
+__global__ void __launch_bounds__(256) k_resid_finish(int N, const double2 *__restrict__ yb,
+                                                      const double2 *__restrict__ b, float2 *__restrict__ rfb,
+                                                      int vstride, char *__restrict__ ctl, double tol,
+                                                      double2 *__restrict__ routb, double *__restrict__ partb) {
+    const int f = blockIdx.y;
+    char *c = ctl + 64 * f;
+    double *red = reinterpret_cast<double *>(c);
+    unsigned int *counter = reinterpret_cast<unsigned int *>(c + 24);
+    int *conv = reinterpret_cast<int *>(c + 28);
+    int *skip = reinterpret_cast<int *>(c + 32);
+    if (*skip) return;
+    __shared__ double sq[8];
+    __shared__ bool last;
+    const int m = blockIdx.x * 256 + threadIdx.x;
+    double q = 0.0;
+    if (m < N) {
+        const double2 y = yb[(size_t)N * f + m], bb = b[m];
+        const double2 r = make_double2(bb.x - y.x, bb.y - y.y);
+        rfb[(size_t)vstride * f + m] = make_float2((float)r.x, (float)r.y);
+        if (routb) routb[(size_t)N * f + m] = r;
+        q = r.x * r.x + r.y * r.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0) sq[threadIdx.x >> 5] = q;
+    __syncthreads();
+    double *part_f = partb + (size_t)gridDim.x * f;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < 8; i++) t += sq[i];
+        part_f[blockIdx.x] = t;
+        __threadfence();
+        const unsigned int done = atomicAdd(counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double acc = 0.0;
+        for (unsigned int i = 0; i < gridDim.x; i++) acc += ((volatile double *)part_f)[i];
+        const double rel = sqrt(acc) / red[1];
+        red[2] = rel;
+        red[0] = 0.0;
+        *counter = 0u;
+        if (rel <= tol) {
+            *conv = 1;
+            *skip = 1;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Port reduction + Zin/S11 (patch_sweep_fastquad_cuda.cu:777-799 for the
 // Gaussian model; patch_sweep_cuda.cu:484-494 for the edge difference).
@@ -574,6 +628,14 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(w.active.reserve(sizeof(int) * B));
     EFIE_TRY(efie_trsv_workspace(w));
     EFIE_TRY(efie_gemm_workspace(w));
+    if (!w.hi) {
+        int least = 0, greatest = 0;
+        EFIE_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        EFIE_CUDA(cudaStreamCreateWithPriority(&w.hi, cudaStreamNonBlocking, greatest));
+        EFIE_CUDA(cudaStreamCreateWithPriority(&w.lo, cudaStreamNonBlocking, least));
+        for (cudaEvent_t *e : {&w.ev_start, &w.ev_panel, &w.ev_rest, &w.ev_hi})
+            EFIE_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     return EFIE_OK;
 }
 
@@ -591,46 +653,91 @@ efie_status efie_mixed_factor(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
     return efie_mixed_factor_launch(ctx, w, Z, zstride, nact);
 }
 
+namespace {
+
+// Launches of a scope go to `s` (ctx->stream is the launch stream of every helper).
+struct OnStream {
+    efie_ctx *c;
+    cudaStream_t old;
+    OnStream(efie_ctx *ctx, cudaStream_t s) : c(ctx), old(ctx->stream) { c->stream = s; }
+    ~OnStream() { c->stream = old; }
+};
+
+}  // namespace
+
+// Two-level blocked LU with look-ahead.  Outer panel P = columns [K0, Kend)
+// is factored by 64-wide diagonal blocks whose panel products and updates
+// stay inside its L-shaped region (the panel chain F_P, latency bound).  Its
+// deferred trailing update D_P (rows and columns >= Kend, K = Kend - K0) is
+// split into the L-shaped strip of the next panel, D_P^next = rows
+// [Kend, K1) x columns >= Kend and rows >= K1 x columns [Kend, K1)
+// (K1 = Kend + KB), and the rest, D_P^rest = rows and columns >= K1.  The
+// panel chain and D^next run on the high-priority stream; D^rest runs on the
+// low-priority stream after F_P, so F_{P+1} overlaps D_P^rest (they touch
+// disjoint parts of the matrix; D_P^next waits for D_{P-1}^rest, whose
+// region contains it).
 efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, int nact) {
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s0 = ctx->stream;
     KernelLog &log = ctx->log;
     const int N = w.N, ld = w.ld, B = w.B;
     float *planes = w.planes.as<float>();
     char *ctl = w.ctl.as<char>();
     const int *active = w.active.as<int>();
     dim3 tg((N + 31) / 32, (N + 31) / 32, B);
-    size_t tok = log.begin(s);
-    k_z_to_planes<<<tg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
+    size_t tok = log.begin(s0);
+    k_z_to_planes<<<tg, 256, 0, s0>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, s, tok, 24.0 * (double)N * N * nact);
+    log.end(EFIE_K_PANEL, s0, tok, 24.0 * (double)N * N * nact);
     float2 *dinv = w.dinv.as<float2>();
-    // Two-level blocking: outer panels of KB columns are factored with 64-wide
-    // diagonal blocks whose updates stay inside the panel's L-shaped region;
-    // the rest of the trailing matrix gets one update with K = KB.
+    EFIE_CUDA(cudaEventRecord(w.ev_start, s0));
+    EFIE_CUDA(cudaStreamWaitEvent(w.hi, w.ev_start, 0));
     const int KB = w.kb_outer;
-    for (int K0 = 0; K0 < N; K0 += KB) {
-        const int Kend = std::min(N, K0 + KB);
-        for (int k = K0; k < Kend; k += NB) {
-            const int bi = k / NB, kb = std::min(NB, N - k);
-            const int s1 = k + kb, rest = N - s1;
-            tok = log.begin(s);
-            k_diag_factor<<<B, 512, 0, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
-            if (rest > 0) {
-                dim3 pg((rest + NB - 1) / NB, 2, B);
-                k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, active);
+    bool rest_pending = false;   // ev_rest holds the record of the previous D^rest
+    {
+        OnStream on(ctx, w.hi);
+        cudaStream_t s = w.hi;
+        for (int K0 = 0; K0 < N; K0 += KB) {
+            const int Kend = std::min(N, K0 + KB), K1 = std::min(N, Kend + KB);
+            // F_P: the panel chain
+            for (int k = K0; k < Kend; k += NB) {
+                const int bi = k / NB, kb = std::min(NB, N - k);
+                const int s1 = k + kb, rest = N - s1;
+                tok = log.begin(s);
+                k_diag_factor<<<B, 512, 0, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
+                if (rest > 0) {
+                    dim3 pg((rest + NB - 1) / NB, 2, B);
+                    k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
+                                                        active);
+                }
+                EFIE_CUDA(cudaGetLastError());
+                log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
+                if (s1 < Kend) {
+                    // rows of this panel below the block, every column to the right
+                    EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact));
+                    // rows below the panel, the panel's remaining columns
+                    EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, s1, Kend, k, k, kb, nact));
+                }
             }
-            EFIE_CUDA(cudaGetLastError());
-            log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
-            if (s1 < Kend) {
-                // rows of this panel below the block, every column to the right
-                EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact));
-                // rows below the panel, the panel's remaining columns
-                EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, s1, Kend, k, k, kb, nact));
+            if (Kend >= N) break;
+            EFIE_CUDA(cudaEventRecord(w.ev_panel, s));
+            // D_P^next on the critical stream, after D_{P-1}^rest
+            if (rest_pending) EFIE_CUDA(cudaStreamWaitEvent(s, w.ev_rest, 0));
+            EFIE_TRY(efie_gemm_update(ctx, w, Kend, K1, Kend, N, K0, K0, Kend - K0, nact));
+            EFIE_TRY(efie_gemm_update(ctx, w, K1, N, Kend, K1, K0, K0, Kend - K0, nact));
+            // D_P^rest on the low-priority stream, after F_P
+            if (K1 < N) {
+                OnStream on_lo(ctx, w.lo);
+                EFIE_CUDA(cudaStreamWaitEvent(w.lo, w.ev_panel, 0));
+                EFIE_TRY(efie_gemm_update(ctx, w, K1, N, K1, N, K0, K0, Kend - K0, nact, 1));
+                EFIE_CUDA(cudaEventRecord(w.ev_rest, w.lo));
+                rest_pending = true;
             }
         }
-        // the deferred trailing update with the whole panel
-        EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, Kend, N, K0, K0, Kend - K0, nact));
     }
+    // join both streams back into the caller's stream
+    EFIE_CUDA(cudaEventRecord(w.ev_hi, w.hi));
+    EFIE_CUDA(cudaStreamWaitEvent(s0, w.ev_hi, 0));
+    if (rest_pending) EFIE_CUDA(cudaStreamWaitEvent(s0, w.ev_rest, 0));
     return EFIE_OK;
 }
 
@@ -724,6 +831,18 @@ efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_
                                   tol, static_cast<double2 *>(rout), w.rpart.as<double>());
     EFIE_CUDA(cudaGetLastError());
     ctx->log.end(EFIE_K_RESIDUAL, s, tok, 16.0 * (double)w.N * w.N * nact);
+    return EFIE_OK;
+}
+
+efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, const void *b, double tol, void *rout,
+                                 int nact) {
+    cudaStream_t s = ctx->stream;
+    size_t tok = ctx->log.begin(s);
+    k_resid_finish<<<dim3((w.N + 255) / 256, w.B), 256, 0, s>>>(
+        w.N, static_cast<const double2 *>(y), static_cast<const double2 *>(b), w.vec.as<float2>(), w.vstride,
+        w.ctl.as<char>(), tol, static_cast<double2 *>(rout), w.rpart.as<double>());
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_RESIDUAL, s, tok, 0.0);
     return EFIE_OK;
 }
 

@@ -27,6 +27,25 @@ struct SolveWork {
     // sums and per-frequency Arnoldi state
     DevBuf gV, gZ, gw, gpart, gst;
     int gnch = 0;          // row chunks of the orthogonalisation kernels
+    // Z is bit-exactly symmetric (symmetric gather): matrix-vector products read
+    // only its upper triangle (128 x 128 tiles, partial vectors in spart)
+    bool zsym = false;
+    DevBuf spart;
+    // look-ahead LU: the panel chain runs on `hi` (highest priority) while the
+    // bulk of each deferred trailing update runs on `lo`, with its own operand
+    // staging (packA2/packB2)
+    cudaStream_t hi = nullptr, lo = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_panel = nullptr, ev_rest = nullptr, ev_hi = nullptr;
+    DevBuf packA2, packB2;
+    SolveWork() = default;
+    SolveWork(const SolveWork &) = delete;
+    SolveWork &operator=(const SolveWork &) = delete;
+    ~SolveWork() {
+        if (hi) cudaStreamDestroy(hi);
+        if (lo) cudaStreamDestroy(lo);
+        for (cudaEvent_t e : {ev_start, ev_panel, ev_rest, ev_hi})
+            if (e) cudaEventDestroy(e);
+    }
 };
 
 struct RefineResult {
@@ -58,6 +77,10 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
 // stored at rout + N f when rout is not null.
 efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *x,
                                const void *b, double tol, void *rout, int nact);
+// r = b - y for a precomputed y = Z x (complex128, [B][N]); otherwise as
+// efie_true_residual.
+efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, const void *b, double tol, void *rout,
+                                 int nact);
 // x = 0 and fresh control blocks (||b|| = bnorm) for every slot.
 efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
@@ -71,7 +94,7 @@ efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs
 // active frequency: tensor cores when the block is large enough (K <= 256),
 // CUDA cores otherwise (efie_update_simt, K <= 64 per call).
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact);
+                             int nact, int slot = 0);
 efie_status efie_update_simt(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
                              int nact);
 extern "C" void efie_debug_disable_tensor_cores(int disable);
