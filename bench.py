@@ -307,7 +307,9 @@ def run_ours(args):
     inp = build_inputs(m, args.workload)
     freqs = inp["freqs"]
     B = args.batch or len(freqs)
-    opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme)
+    # frequency slots of the plan: automatic, but no more than the points of a step
+    opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
+                        batch=B if B < 8 else 0)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh

@@ -4,12 +4,17 @@
 // The complex product is realified into one real GEMM per 64-row block:
 //     [ Re ]   [ Lr  -Li ]   [ Ur ]
 //     [ Im ] = [ Li   Lr ] * [ Ui ]        (M' = 128 rows, K' = 2 kb)
-// and every operand is split into two TF32 terms, x = hi + lo with
-// hi = tf32(x), lo = tf32(x - hi); the three products hi*hi + hi*lo + lo*hi
-// accumulate in FP32 in tensor memory (TMEM), which keeps the update close to
-// FP32 accuracy (the LU is then refined in FP64).
+// and every operand is split into two FP16 terms after an exact power-of-two
+// scaling: each complex row of L21 by s_i and each column of U12 by t_j so
+// that the largest magnitude of the row (column) over the update's K range
+// lies in [1/2, 1); then x = hi + lo with hi = fp16(x), lo = fp16(x - hi)
+// (22 significant bits, the precision of a TF32 pair at half the bytes).  The
+// three products hi*hi + hi*lo + lo*hi accumulate in FP32 in tensor memory
+// (TMEM, kind::f16, K = 16 per instruction) and the epilogue multiplies by
+// 1/(s_i t_j), which is exact.  The update stays close to FP32 accuracy
+// normwise (the LU is then refined in FP64).
 //
-// Operands are packed per LU step into 64B-swizzled K-major tiles (16 TF32
+// Operands are packed per LU step into 64B-swizzled K-major tiles (32 FP16
 // per row) that sit contiguously in global memory, so each CTA fetches them
 // with plain bulk copies (cp.async.bulk, the TMA engine; no multicast, local
 // memory only).  One CTA computes two 128 x 256 accumulator tiles (2 x 64
@@ -26,6 +31,8 @@
 // Every mbarrier wait is bounded; a timeout sets the device error flag.
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "solve.h"
 
 namespace {
@@ -33,30 +40,68 @@ namespace {
 constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
 constexpr int TM = 128;          // accumulator rows (64 complex rows)
 constexpr int TN = 256;          // accumulator columns (complex columns)
-constexpr int KC = 16;           // fp32 elements per 64-byte swizzle row (one K' chunk)
-constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 32 chunks
-constexpr int A_TILE = TM * KC;       // floats per A tile (8 KB)
-constexpr int B_TILE = TN * KC;       // floats per B tile (16 KB)
+constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K' chunk)
+constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 16 chunks
+constexpr int A_TILE = TM * KC;       // halves per A tile (8 KB)
+constexpr int B_TILE = TN * KC;       // halves per B tile (16 KB)
 constexpr int MT = 2;            // 128-row accumulator tiles per CTA (TMEM columns: MT x 256)
-constexpr int STAGE_FLOATS = MT * 2 * A_TILE + 2 * B_TILE;   // hi/lo of MT A tiles and of B: 64 KB
+constexpr int STAGE_HALVES = MT * 2 * A_TILE + 2 * B_TILE;   // hi/lo of MT A tiles and of B: 64 KB
 constexpr int NSTAGE = 3;
 constexpr int NBAR = 2 * NSTAGE + 1;  // full[NSTAGE], empty[NSTAGE], done
-constexpr size_t GEMM_SMEM = sizeof(float) * NSTAGE * STAGE_FLOATS + 1024 + 8 * NBAR + 16;
+constexpr size_t GEMM_SMEM = sizeof(__half) * NSTAGE * STAGE_HALVES + 1024 + 8 * NBAR + 16 + sizeof(float) * TN;
 
-// byte offset of element (row r, k) inside a K-major 64B-swizzled tile: the
-// 16-byte chunk index (k / 4) XOR (r / 2) mod 4, 8-row atoms of 512 bytes
+// byte offset of element (row r, k) inside a K-major 64B-swizzled tile of
+// fp16: the 16-byte chunk index (k / 8) XOR (r / 2) mod 4, 8-row atoms of 512 bytes
 __host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) {
-    return r * 64u + ((((k >> 2) ^ (r >> 1)) & 3u) << 4) + ((k & 3u) << 2);
+    return r * 64u + ((((k >> 3) ^ (r >> 1)) & 3u) << 4) + ((k & 7u) << 1);
 }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+// 2^-e with max * 2^-e in [1/2, 1) (1 for a zero maximum)
+__device__ __forceinline__ float pow2_scale(float mx) {
+    if (!(mx > 0.f)) return 1.f;
+    int e;
+    frexpf(mx, &e);
+    return ldexpf(1.f, -e);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ---------------------------------------------------------------------------
+// Scales of one update: 1/s_i per complex row of L[r0:r1, kcol:kcol+K] and
+// 1/t_j per column of U[krow:krow+K, c0:c1] are stored (inverse scales, used
+// by the epilogue; the packers use their reciprocals, also exact).  Grid x:
+// row blocks of 8 rows (a warp per row) then column blocks of 256 columns.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_scales(int N, int r0, int r1, int kcol, int c0, int c1, int krow, int K,
+                                                int nrb, const float *__restrict__ planes, size_t pstride, int ld,
+                                                float *__restrict__ isa, size_t sastride, float *__restrict__ isb,
+                                                size_t sbstride, const int *__restrict__ active) {
+    const int f = blockIdx.y;
+    if (!active[f]) return;
+    const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
+    if ((int)blockIdx.x < nrb) {
+        const int i = r0 + blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+        if (i >= r1) return;
+        float mx = 0.f;
+        for (int k = lane; k < K; k += 32) {
+            const size_t o = (size_t)i * ld + kcol + k;
+            mx = fmaxf(mx, fmaxf(fabsf(Ar[o]), fabsf(Ai[o])));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) isa[sastride * f + (i - r0)] = 1.f / pow2_scale(mx);
+    } else {
+        const int j = c0 + ((int)blockIdx.x - nrb) * 256 + threadIdx.x;
+        if (j >= c1) return;
+        float mx = 0.f;
+        for (int k = 0; k < K; k++) {
+            const size_t o = (size_t)(krow + k) * ld + j;
+            mx = fmaxf(mx, fmaxf(fabsf(Ar[o]), fabsf(Ai[o])));
+        }
+        isb[sbstride * f + (j - c0)] = 1.f / pow2_scale(mx);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -65,76 +110,82 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 // Tiles are built in shared memory in their final swizzled byte layout and
 // written out with coalesced 16-byte stores.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
+    h = __float2half_rn(v);
+    l = __float2half_rn(v - __half2float(h));
+}
+
 __global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
-                                                float *__restrict__ outb, size_t ostride,
+                                                const float *__restrict__ isa, size_t sastride,
+                                                __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
-    __shared__ __align__(1024) float hi[A_TILE];
-    __shared__ __align__(1024) float lo[A_TILE];
+    __shared__ __align__(1024) __half hi[A_TILE];
+    __shared__ __align__(1024) __half lo[A_TILE];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
-    float *out = outb + ostride * f;
+    __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
     for (int e = threadIdx.x; e < A_TILE; e += 256) {
-        const int r = e >> 4, kq = e & 15;           // consecutive threads: consecutive k
+        const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
         const int kp = chunk * KC + kq;              // K' index
         const bool second = kp >= K;
         const int kk = second ? kp - K : kp;         // column within the L block
-        const int row = r0 + tile * 64 + (r & 63);
+        const int rl = tile * 64 + (r & 63);         // complex row within the update
+        const int row = r0 + rl;
         float v = 0.f;
         if (row < r1 && kk < K) {
             const size_t o = (size_t)row * ld + kcol + kk;
             if (r < 64) v = second ? -Ai[o] : Ar[o];     // [ Lr  -Li ]
             else v = second ? Ar[o] : Ai[o];            // [ Li   Lr ]
+            v *= 1.f / isa[sastride * f + rl];          // exact: a power of two
         }
-        const float h = tf32_rna(v);
-        const uint32_t off = swz(r, kq) >> 2;
-        hi[off] = h;
-        lo[off] = tf32_rna(v - h);
+        const uint32_t off = swz(r, kq) >> 1;
+        split_half(v, hi[off], lo[off]);
     }
     __syncthreads();
     float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * A_TILE);
     const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
-    for (int e = threadIdx.x; e < A_TILE / 4; e += 256) {
+    for (int e = threadIdx.x; e < A_TILE / 8; e += 256) {
         dst[e] = h4[e];
-        dst[A_TILE / 4 + e] = l4[e];
+        dst[A_TILE / 8 + e] = l4[e];
     }
 }
 
 __global__ void __launch_bounds__(256) k_pack_b(int N, int c0, int c1, int krow, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
-                                                float *__restrict__ outb, size_t ostride,
+                                                const float *__restrict__ isb, size_t sbstride,
+                                                __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
-    extern __shared__ __align__(1024) float dynb[];
-    float *hi = dynb, *lo = dynb + B_TILE;
+    extern __shared__ __align__(1024) __half dynb[];
+    __half *hi = dynb, *lo = dynb + B_TILE;
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
-    float *out = outb + ostride * f;
+    __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
     for (int e = threadIdx.x; e < B_TILE; e += 256) {
         const int kq = e >> 8, n = e & 255;          // consecutive threads: consecutive columns
         const int kp = chunk * KC + kq;
         const bool second = kp >= K;
         const int kk = second ? kp - K : kp;
-        const int col = c0 + tile * TN + n;
+        const int cl = tile * TN + n;
+        const int col = c0 + cl;
         float v = 0.f;
         if (col < c1 && kk < K) {
             const size_t o = (size_t)(krow + kk) * ld + col;
-            v = second ? Ai[o] : Ar[o];                  // [ Ur ; Ui ]
+            v = (second ? Ai[o] : Ar[o]) * (1.f / isb[sbstride * f + cl]);   // [ Ur ; Ui ], exact scaling
         }
-        const float h = tf32_rna(v);
-        const uint32_t off = swz(n, kq) >> 2;
-        hi[off] = h;
-        lo[off] = tf32_rna(v - h);
+        const uint32_t off = swz(n, kq) >> 1;
+        split_half(v, hi[off], lo[off]);
     }
     __syncthreads();
     float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * B_TILE);
     const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
-    for (int e = threadIdx.x; e < B_TILE / 4; e += 256) {
+    for (int e = threadIdx.x; e < B_TILE / 8; e += 256) {
         dst[e] = h4[e];
-        dst[B_TILE / 4 + e] = l4[e];
+        dst[B_TILE / 8 + e] = l4[e];
     }
 }
 
@@ -190,15 +241,15 @@ __device__ __forceinline__ uint64_t desc_sw64(const void *smem_tile) {
     return d;
 }
 
-// kind::tf32, D = F32, A = B = TF32, both K-major, N = 256, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
+// kind::f16, D = F32, A = B = F16, both K-major, N = 256, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TN >> 3) << 17) |
                            ((uint32_t)(TM >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
         "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
@@ -226,22 +277,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // C[r0:r1, c0:c1] -= (packed A) * (packed B) for the CTA's tiles; grid
 // (column tiles, pairs of 64-row tiles, frequency), 256 threads.
 __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
-                                                      const float *__restrict__ Apackb, size_t astride,
-                                                      const float *__restrict__ Bpackb, size_t bstride,
+                                                      const __half *__restrict__ Apackb, size_t astride,
+                                                      const __half *__restrict__ Bpackb, size_t bstride,
+                                                      const float *__restrict__ isab, size_t sastride,
+                                                      const float *__restrict__ isbb, size_t sbstride,
                                                       float *__restrict__ planes, size_t pstride, int ld,
                                                       char *__restrict__ ctl, const int *__restrict__ active) {
     const int f = blockIdx.z;
     if (!active[f]) return;
-    const float *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
+    const __half *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
+    const float *isa = isab + sastride * f, *isb = isbb + sbstride * f;
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
     extern __shared__ uint8_t dyn_raw[];
     // 1024-byte alignment for the swizzled tiles
-    float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_FLOATS);  // full[], empty[], done
+    __half *stage = reinterpret_cast<__half *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_HALVES);  // full[], empty[], done
     uint64_t *full = bars, *empty = bars + NSTAGE, *done = bars + 2 * NSTAGE;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + NBAR);
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
+    float *col_is = reinterpret_cast<float *>(bars + 8);   // 16-byte aligned: inverse column scales of the tile
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile_n = blockIdx.x, tile_m0 = blockIdx.y * MT;
     const int nm = min(MT, mt - tile_m0);            // accumulator tiles of this CTA (1 or 2)
@@ -263,10 +318,10 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
     bool ok = true;
     if (tid == 0) *ok_sh = 1;
     if (tid == 0) {
-        const float *gb = Bpack + (size_t)tile_n * nchunk * 2 * B_TILE;
-        const uint32_t abytes = sizeof(float) * 2 * A_TILE, bbytes = sizeof(float) * 2 * B_TILE;
+        const __half *gb = Bpack + (size_t)tile_n * nchunk * 2 * B_TILE;
+        const uint32_t abytes = sizeof(__half) * 2 * A_TILE, bbytes = sizeof(__half) * 2 * B_TILE;
         auto load = [&](int c) {
-            float *st = stage + (c % NSTAGE) * STAGE_FLOATS;
+            __half *st = stage + (c % NSTAGE) * STAGE_HALVES;
             mbar_expect_tx(&full[c % NSTAGE], nm * abytes + bbytes);
             for (int mi = 0; mi < nm; mi++)
                 bulk_g2s(st + mi * 2 * A_TILE, Apack + ((size_t)(tile_m0 + mi) * nchunk + c) * 2 * A_TILE, abytes,
@@ -278,18 +333,18 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
             const int sidx = c % NSTAGE;
             if (!mbar_wait(&full[sidx], (c / NSTAGE) & 1, err)) { ok = false; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const float *st = stage + sidx * STAGE_FLOATS;
+            const __half *st = stage + sidx * STAGE_HALVES;
             const uint64_t bhi = desc_sw64(st + MT * 2 * A_TILE), blo = desc_sw64(st + MT * 2 * A_TILE + B_TILE);
             for (int mi = 0; mi < nm; mi++) {
                 const uint64_t ahi = desc_sw64(st + mi * 2 * A_TILE), alo = desc_sw64(st + mi * 2 * A_TILE + A_TILE);
                 const uint32_t acc = tmem + (uint32_t)(mi * TN);
 #pragma unroll
-                for (int kk = 0; kk < KC / 8; kk++) {
-                    const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+                for (int kk = 0; kk < KC / 16; kk++) {
+                    const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 16 fp16 = 32 bytes along K
                     // small terms first, then the leading product
-                    mma_tf32(acc, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
-                    mma_tf32(acc, ahi + adv, blo + adv, 1u);
-                    mma_tf32(acc, ahi + adv, bhi + adv, 1u);
+                    mma_f16(acc, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
+                    mma_f16(acc, ahi + adv, blo + adv, 1u);
+                    mma_f16(acc, ahi + adv, bhi + adv, 1u);
                 }
             }
             mma_commit(&empty[sidx]);   // stage sidx free once these MMAs have read it
@@ -304,6 +359,11 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
         mma_commit(done);                  // all MMAs of this CTA done
         if (!ok) *ok_sh = 0;
     } else if (warp > 0) {
+        // inverse column scales of the tile into shared memory
+        for (int j = tid - 32; j < TN; j += 224) {
+            const int cl = tile_n * TN + j;
+            col_is[j] = (c0 + cl < c1) ? isb[cl] : 0.f;
+        }
         // C rows of this CTA into L2 while the MMAs run: (accumulator, plane, row) segments
         const int ncol = min(TN, c1 - (c0 + tile_n * TN));
         const uint32_t bytes = (uint32_t)((ncol * 4 + 15) & ~15);
@@ -330,8 +390,10 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
         constexpr int NJ = TN / 32;
         const int j0 = (warp >> 2) * (NJ / 2), j1 = j0 + NJ / 2;   // this warp's half of the columns
         for (int mi = 0; mi < nm; mi++) {
-            const int row = r0 + (tile_m0 + mi) * 64 + half * 32 + lane;
+            const int rl = (tile_m0 + mi) * 64 + half * 32 + lane;   // complex row within the update
+            const int row = r0 + rl;
             const bool rok = row < r1;
+            const float rs = rok ? isa[rl] : 0.f;
             const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mi * TN);
             float *prow = plane + (size_t)(rok ? row : r0) * ld + c0 + tile_n * TN;
             const int ncol = c1 - (c0 + tile_n * TN);   // valid columns of this tile (may exceed TN)
@@ -357,17 +419,18 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
                         float4 *p4 = reinterpret_cast<float4 *>(p);
 #pragma unroll
                         for (int q = 0; q < 8; q++) {
+                            const float4 cs = *reinterpret_cast<const float4 *>(col_is + col0 + 4 * q);
                             float4 a = cur[q];
-                            a.x -= __uint_as_float(v[4 * q]);
-                            a.y -= __uint_as_float(v[4 * q + 1]);
-                            a.z -= __uint_as_float(v[4 * q + 2]);
-                            a.w -= __uint_as_float(v[4 * q + 3]);
+                            a.x -= __uint_as_float(v[4 * q]) * (rs * cs.x);
+                            a.y -= __uint_as_float(v[4 * q + 1]) * (rs * cs.y);
+                            a.z -= __uint_as_float(v[4 * q + 2]) * (rs * cs.z);
+                            a.w -= __uint_as_float(v[4 * q + 3]) * (rs * cs.w);
                             p4[q] = a;
                         }
                     } else {
 #pragma unroll
                         for (int q = 0; q < 32; q++)
-                            if (col0 + q < ncol) p[q] -= __uint_as_float(v[q]);
+                            if (col0 + q < ncol) p[q] -= __uint_as_float(v[q]) * (rs * col_is[col0 + q]);
                     }
                 }
 #pragma unroll
@@ -391,7 +454,7 @@ efie_status efie_tc_attrs() {
     if (done) return EFIE_OK;
     EFIE_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
     EFIE_CUDA(cudaFuncSetAttribute(k_pack_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(float) * 2 * B_TILE)));
+                                   (int)(sizeof(__half) * 2 * B_TILE)));
     done = true;
     return EFIE_OK;
 }
@@ -405,10 +468,13 @@ efie_status efie_gemm_workspace(SolveWork &w) {
     EFIE_TRY(efie_tc_attrs());
     const int mt0 = (w.N + 63) / 64, nt0 = (w.N + TN - 1) / TN;
     const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
-    EFIE_TRY(w.packA.reserve(sizeof(float) * astride * w.B));
-    EFIE_TRY(w.packB.reserve(sizeof(float) * bstride * w.B));
-    EFIE_TRY(w.packA2.reserve(sizeof(float) * astride * w.B));
-    EFIE_TRY(w.packB2.reserve(sizeof(float) * bstride * w.B));
+    EFIE_TRY(w.packA.reserve(sizeof(__half) * astride * w.B));
+    EFIE_TRY(w.packB.reserve(sizeof(__half) * bstride * w.B));
+    EFIE_TRY(w.packA2.reserve(sizeof(__half) * astride * w.B));
+    EFIE_TRY(w.packB2.reserve(sizeof(__half) * bstride * w.B));
+    const size_t sa = (size_t)mt0 * 64, sb = (size_t)nt0 * TN;
+    for (DevBuf *d : {&w.sclA, &w.sclA2}) EFIE_TRY(d->reserve(sizeof(float) * sa * w.B));
+    for (DevBuf *d : {&w.sclB, &w.sclB2}) EFIE_TRY(d->reserve(sizeof(float) * sb * w.B));
     return EFIE_OK;
 }
 
@@ -434,23 +500,30 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
     const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
     DevBuf &pA = slot ? w.packA2 : w.packA, &pB = slot ? w.packB2 : w.packB;
-    EFIE_TRY(pA.reserve(sizeof(float) * astride * B));
-    EFIE_TRY(pB.reserve(sizeof(float) * bstride * B));
+    DevBuf &sA = slot ? w.sclA2 : w.sclA, &sB = slot ? w.sclB2 : w.sclB;
+    const size_t sastride = (size_t)mt0 * 64, sbstride = (size_t)nt0 * TN;
+    EFIE_TRY(pA.reserve(sizeof(__half) * astride * B));
+    EFIE_TRY(pB.reserve(sizeof(__half) * bstride * B));
+    EFIE_TRY(sA.reserve(sizeof(float) * sastride * B));
+    EFIE_TRY(sB.reserve(sizeof(float) * sbstride * B));
     float *planes = w.planes.as<float>();
     const int *active = w.active.as<int>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
+    const int nrb = (rows + 7) / 8, ncb = (cols + 255) / 256;
+    k_scales<<<dim3(nrb + ncb, B), 256, 0, st>>>(N, r0, r1, kcol, c0, c1, krow, K, nrb, planes, w.pstride, w.ld,
+                                                  sA.as<float>(), sastride, sB.as<float>(), sbstride, active);
     k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld,
-                                                  pA.as<float>(), astride, active);
-    k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(float) * 2 * B_TILE, st>>>(N, c0, c1, krow, K, nchunk, planes,
-                                                                          w.pstride, w.ld, pB.as<float>(), bstride,
-                                                                          active);
+                                                  sA.as<float>(), sastride, pA.as<__half>(), astride, active);
+    k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(__half) * 2 * B_TILE, st>>>(
+        N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, sB.as<float>(), sbstride, pB.as<__half>(), bstride,
+        active);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
+    log.end(EFIE_K_PANEL, st, tok, 0.0, 3);
     tok = log.begin(st);
     k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 256, GEMM_SMEM, st>>>(
-        N, r0, r1, c0, c1, nchunk, mt, pA.as<float>(), astride, pB.as<float>(), bstride, planes, w.pstride, w.ld,
-        w.ctl.as<char>(), active);
+        N, r0, r1, c0, c1, nchunk, mt, pA.as<__half>(), astride, pB.as<__half>(), bstride, sA.as<float>(), sastride,
+        sB.as<float>(), sbstride, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;

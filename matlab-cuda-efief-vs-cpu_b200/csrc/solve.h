@@ -21,7 +21,7 @@ struct SolveWork {
     DevBuf ctl;      // per f 64 bytes: red[3] @0, counter @24, conv @28, skip @32, err @36
     DevBuf rpart;    // residual-norm partial sums: double [B][ceil(N/32)]
     DevBuf active;   // int[B]: slot holds a frequency of this batch
-    DevBuf packA, packB;  // tensor-core operand staging
+    DevBuf packA, packB;  // tensor-core operand staging (FP16 hi/lo tiles)
     // flexible GMRES (gmres.cu): Krylov basis V [M+1][B][N] and preconditioned
     // vectors Zm [M][B][N] in complex128, the new vector w [B][N], partial
     // sums and per-frequency Arnoldi state
@@ -37,6 +37,7 @@ struct SolveWork {
     cudaStream_t hi = nullptr, lo = nullptr;
     cudaEvent_t ev_start = nullptr, ev_panel = nullptr, ev_rest = nullptr, ev_hi = nullptr;
     DevBuf packA2, packB2;
+    DevBuf sclA, sclB, sclA2, sclB2;   // power-of-two inverse scales of the FP16 operands (per row / column)
     SolveWork() = default;
     SolveWork(const SolveWork &) = delete;
     SolveWork &operator=(const SolveWork &) = delete;
