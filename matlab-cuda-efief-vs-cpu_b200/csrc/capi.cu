@@ -5,6 +5,8 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "efie_internal.h"
@@ -112,7 +114,110 @@ extern "C" void efie_ctx_destroy(efie_ctx *ctx) {
     if (ctx->solver) cusolverDnDestroy(ctx->solver);
     ctx->status.release();
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    efie_pool_trim(ctx->device);
     delete ctx;
+}
+
+namespace {
+
+struct DevicePool {
+    std::multimap<size_t, void *> free;   // size -> block
+    size_t cached = 0;
+    size_t cap = 0;
+};
+
+std::mutex g_pool_mu;
+// never destroyed: cached blocks are left to the driver at process exit
+std::map<int, DevicePool> *g_pools = new std::map<int, DevicePool>();
+
+DevicePool &pool_of(int dev) {
+    DevicePool &P = (*g_pools)[dev];
+    if (!P.cap) {
+        size_t fr = 0, total = 0;
+        if (cudaMemGetInfo(&fr, &total) == cudaSuccess) P.cap = total / 10 * 4;
+        else P.cap = 1;
+    }
+    return P;
+}
+
+void trim_locked(DevicePool &P) {
+    for (auto &kv : P.free) cudaFree(kv.second);
+    P.free.clear();
+    P.cached = 0;
+}
+
+}  // namespace
+
+void *efie_pool_get(size_t n, size_t *got, cudaError_t *err) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        DevicePool &P = pool_of(dev);
+        auto it = P.free.lower_bound(n);
+        if (it != P.free.end() && it->first <= 2 * n) {
+            void *p = it->second;
+            *got = it->first;
+            P.cached -= it->first;
+            P.free.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // clear the sticky-free allocation error
+        {
+            std::lock_guard<std::mutex> lk(g_pool_mu);
+            trim_locked(pool_of(dev));
+        }
+        e = cudaMalloc(&p, n);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (err) *err = e;
+        return nullptr;
+    }
+    *got = n;
+    return p;
+}
+
+void efie_pool_put(void *p, size_t bytes) {
+    // the block's last users may still run: finish them as cudaFree would
+    cudaDeviceSynchronize();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    DevicePool &P = pool_of(dev);
+    if (bytes > P.cap) {
+        cudaFree(p);
+        return;
+    }
+    P.free.emplace(bytes, p);
+    P.cached += bytes;
+    while (P.cached > P.cap && !P.free.empty()) {   // drop the largest blocks first
+        auto it = std::prev(P.free.end());
+        cudaFree(it->second);
+        P.cached -= it->first;
+        P.free.erase(it);
+    }
+}
+
+void efie_pool_trim(int device) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        trim_locked(pool_of(device));
+    }
+    cudaSetDevice(prev);
+}
+
+size_t efie_pool_cached(int device) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools->find(device);
+    return it == g_pools->end() ? 0 : it->second.cached;
 }
 
 extern "C" efie_status efie_ctx_set_stream(efie_ctx *ctx, void *stream) {
@@ -393,6 +498,9 @@ int choose_batch(int N, int requested, int solver) {
     if (requested > 0) return std::min(requested, EFIE_MAX_BATCH);
     size_t freeb = 0, total = 0;
     if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    freeb += efie_pool_cached(dev);   // cached blocks are available to this plan
     const double per = 26.0 * (double)N * N + 1e6;
     int B = (int)std::floor(0.35 * (double)freeb / per);
     return std::max(1, std::min(B, 8));

@@ -47,25 +47,33 @@ struct DeviceGuard {
     }
 };
 
+// Device memory of the current device through a per-device cache: a freed
+// block is kept (after the device has finished with it, like cudaFree) and
+// handed to a later request of at most twice its size, so a caller that
+// creates and destroys plans of the same problem repeatedly stops paying for
+// cudaMalloc/cudaFree of gigabytes.  The cache is capped (40 % of the device)
+// and emptied by efie_pool_trim (context destruction) or when cudaMalloc fails.
+void *efie_pool_get(size_t n, size_t *got, cudaError_t *err);
+void efie_pool_put(void *p, size_t bytes);
+void efie_pool_trim(int device);
+size_t efie_pool_cached(int device);
+
 // A device allocation owned by a context or plan; grows, never shrinks.
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
     efie_status reserve(size_t n) {
         if (n <= bytes) return EFIE_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, n ? n : 1);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return efie_fail(EFIE_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-        }
-        bytes = n;
+        release();
+        cudaError_t e = cudaSuccess;
+        size_t got = 0;
+        p = efie_pool_get(n ? n : 1, &got, &e);
+        if (!p) return efie_fail(EFIE_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        bytes = got;
         return EFIE_OK;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) efie_pool_put(p, bytes);
         p = nullptr;
         bytes = 0;
     }

@@ -68,40 +68,18 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// ---------------------------------------------------------------------------
-// Scales of one update: 1/s_i per complex row of L[r0:r1, kcol:kcol+K] and
-// 1/t_j per column of U[krow:krow+K, c0:c1] are stored (inverse scales, used
-// by the epilogue; the packers use their reciprocals, also exact).  Grid x:
-// row blocks of 8 rows (a warp per row) then column blocks of 256 columns.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_scales(int N, int r0, int r1, int kcol, int c0, int c1, int krow, int K,
-                                                int nrb, const float *__restrict__ planes, size_t pstride, int ld,
-                                                float *__restrict__ isa, size_t sastride, float *__restrict__ isb,
-                                                size_t sbstride, const int *__restrict__ active) {
-    const int f = blockIdx.y;
-    if (!active[f]) return;
-    const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
-    if ((int)blockIdx.x < nrb) {
-        const int i = r0 + blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-        if (i >= r1) return;
-        float mx = 0.f;
-        for (int k = lane; k < K; k += 32) {
-            const size_t o = (size_t)i * ld + kcol + k;
-            mx = fmaxf(mx, fmaxf(fabsf(Ar[o]), fabsf(Ai[o])));
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) isa[sastride * f + (i - r0)] = 1.f / pow2_scale(mx);
-    } else {
-        const int j = c0 + ((int)blockIdx.x - nrb) * 256 + threadIdx.x;
-        if (j >= c1) return;
-        float mx = 0.f;
-        for (int k = 0; k < K; k++) {
-            const size_t o = (size_t)(krow + k) * ld + j;
-            mx = fmaxf(mx, fmaxf(fabsf(Ar[o]), fabsf(Ai[o])));
-        }
-        isb[sbstride * f + (j - c0)] = 1.f / pow2_scale(mx);
-    }
+// Largest magnitude of a row of L over the 64-column blocks [b0, b1), and of a
+// column of U over the 64-row blocks [b0, b1): the maxima are written with
+// the factors (k_panels), so a scale costs at most four loads.
+__device__ __forceinline__ float row_max(const float *lm, int row, int nblk, int b0, int b1) {
+    float m = 0.f;
+    for (int b = b0; b < b1; b++) m = fmaxf(m, lm[(size_t)row * nblk + b]);
+    return m;
+}
+__device__ __forceinline__ float col_max(const float *um, int ld, int col, int b0, int b1) {
+    float m = 0.f;
+    for (int b = b0; b < b1; b++) m = fmaxf(m, um[(size_t)b * ld + col]);
+    return m;
 }
 
 // ---------------------------------------------------------------------------
@@ -117,16 +95,23 @@ __device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
 
 __global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
-                                                const float *__restrict__ isa, size_t sastride,
+                                                const float *__restrict__ lmaxb, size_t mstride, int nblk,
                                                 __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
     __shared__ __align__(1024) __half hi[A_TILE];
     __shared__ __align__(1024) __half lo[A_TILE];
+    __shared__ float rscale[64];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
+    if (threadIdx.x < 64) {
+        const int row = r0 + tile * 64 + threadIdx.x;
+        rscale[threadIdx.x] =
+            row < r1 ? pow2_scale(row_max(lmaxb + mstride * f, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
+    }
+    __syncthreads();
     for (int e = threadIdx.x; e < A_TILE; e += 256) {
         const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
         const int kp = chunk * KC + kq;              // K' index
@@ -139,7 +124,7 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol,
             const size_t o = (size_t)row * ld + kcol + kk;
             if (r < 64) v = second ? -Ai[o] : Ar[o];     // [ Lr  -Li ]
             else v = second ? Ar[o] : Ai[o];            // [ Li   Lr ]
-            v *= 1.f / isa[sastride * f + rl];          // exact: a power of two
+            v *= rscale[r & 63];                        // exact: a power of two
         }
         const uint32_t off = swz(r, kq) >> 1;
         split_half(v, hi[off], lo[off]);
@@ -155,16 +140,23 @@ __global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol,
 
 __global__ void __launch_bounds__(256) k_pack_b(int N, int c0, int c1, int krow, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
-                                                const float *__restrict__ isb, size_t sbstride,
+                                                const float *__restrict__ umaxb, size_t mstride,
                                                 __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
     extern __shared__ __align__(1024) __half dynb[];
     __half *hi = dynb, *lo = dynb + B_TILE;
+    __shared__ float cscale[TN];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
+    {
+        const int col = c0 + tile * TN + threadIdx.x;   // 256 threads: one column each
+        cscale[threadIdx.x] =
+            col < c1 ? pow2_scale(col_max(umaxb + mstride * f, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
+    }
+    __syncthreads();
     for (int e = threadIdx.x; e < B_TILE; e += 256) {
         const int kq = e >> 8, n = e & 255;          // consecutive threads: consecutive columns
         const int kp = chunk * KC + kq;
@@ -175,7 +167,7 @@ __global__ void __launch_bounds__(256) k_pack_b(int N, int c0, int c1, int krow,
         float v = 0.f;
         if (col < c1 && kk < K) {
             const size_t o = (size_t)(krow + kk) * ld + col;
-            v = (second ? Ai[o] : Ar[o]) * (1.f / isb[sbstride * f + cl]);   // [ Ur ; Ui ], exact scaling
+            v = (second ? Ai[o] : Ar[o]) * cscale[n];   // [ Ur ; Ui ], exact scaling
         }
         const uint32_t off = swz(n, kq) >> 1;
         split_half(v, hi[off], lo[off]);
@@ -279,14 +271,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
                                                       const __half *__restrict__ Apackb, size_t astride,
                                                       const __half *__restrict__ Bpackb, size_t bstride,
-                                                      const float *__restrict__ isab, size_t sastride,
-                                                      const float *__restrict__ isbb, size_t sbstride,
+                                                      const float *__restrict__ lmaxb, const float *__restrict__ umaxb,
+                                                      size_t mstride, int nblk, int kcol, int krow, int K,
                                                       float *__restrict__ planes, size_t pstride, int ld,
                                                       char *__restrict__ ctl, const int *__restrict__ active) {
     const int f = blockIdx.z;
     if (!active[f]) return;
     const __half *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
-    const float *isa = isab + sastride * f, *isb = isbb + sbstride * f;
+    const float *lm = lmaxb + mstride * f, *um = umaxb + mstride * f;
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
     extern __shared__ uint8_t dyn_raw[];
@@ -361,8 +353,8 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
     } else if (warp > 0) {
         // inverse column scales of the tile into shared memory
         for (int j = tid - 32; j < TN; j += 224) {
-            const int cl = tile_n * TN + j;
-            col_is[j] = (c0 + cl < c1) ? isb[cl] : 0.f;
+            const int col = c0 + tile_n * TN + j;
+            col_is[j] = (col < c1) ? 1.f / pow2_scale(col_max(um, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
         }
         // C rows of this CTA into L2 while the MMAs run: (accumulator, plane, row) segments
         const int ncol = min(TN, c1 - (c0 + tile_n * TN));
@@ -393,7 +385,7 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
             const int rl = (tile_m0 + mi) * 64 + half * 32 + lane;   // complex row within the update
             const int row = r0 + rl;
             const bool rok = row < r1;
-            const float rs = rok ? isa[rl] : 0.f;
+            const float rs = rok ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
             const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mi * TN);
             float *prow = plane + (size_t)(rok ? row : r0) * ld + c0 + tile_n * TN;
             const int ncol = c1 - (c0 + tile_n * TN);   // valid columns of this tile (may exceed TN)
@@ -472,9 +464,6 @@ efie_status efie_gemm_workspace(SolveWork &w) {
     EFIE_TRY(w.packB.reserve(sizeof(__half) * bstride * w.B));
     EFIE_TRY(w.packA2.reserve(sizeof(__half) * astride * w.B));
     EFIE_TRY(w.packB2.reserve(sizeof(__half) * bstride * w.B));
-    const size_t sa = (size_t)mt0 * 64, sb = (size_t)nt0 * TN;
-    for (DevBuf *d : {&w.sclA, &w.sclA2}) EFIE_TRY(d->reserve(sizeof(float) * sa * w.B));
-    for (DevBuf *d : {&w.sclB, &w.sclB2}) EFIE_TRY(d->reserve(sizeof(float) * sb * w.B));
     return EFIE_OK;
 }
 
@@ -500,30 +489,23 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
     const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
     DevBuf &pA = slot ? w.packA2 : w.packA, &pB = slot ? w.packB2 : w.packB;
-    DevBuf &sA = slot ? w.sclA2 : w.sclA, &sB = slot ? w.sclB2 : w.sclB;
-    const size_t sastride = (size_t)mt0 * 64, sbstride = (size_t)nt0 * TN;
     EFIE_TRY(pA.reserve(sizeof(__half) * astride * B));
     EFIE_TRY(pB.reserve(sizeof(__half) * bstride * B));
-    EFIE_TRY(sA.reserve(sizeof(float) * sastride * B));
-    EFIE_TRY(sB.reserve(sizeof(float) * sbstride * B));
     float *planes = w.planes.as<float>();
     const int *active = w.active.as<int>();
+    const float *lmax = w.lmax.as<float>(), *umax = w.umax.as<float>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
-    const int nrb = (rows + 7) / 8, ncb = (cols + 255) / 256;
-    k_scales<<<dim3(nrb + ncb, B), 256, 0, st>>>(N, r0, r1, kcol, c0, c1, krow, K, nrb, planes, w.pstride, w.ld,
-                                                  sA.as<float>(), sastride, sB.as<float>(), sbstride, active);
-    k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld,
-                                                  sA.as<float>(), sastride, pA.as<__half>(), astride, active);
+    k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld, lmax,
+                                                  w.mstride, w.nblk, pA.as<__half>(), astride, active);
     k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(__half) * 2 * B_TILE, st>>>(
-        N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, sB.as<float>(), sbstride, pB.as<__half>(), bstride,
-        active);
+        N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, umax, w.mstride, pB.as<__half>(), bstride, active);
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, st, tok, 0.0, 3);
+    log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
     k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 256, GEMM_SMEM, st>>>(
-        N, r0, r1, c0, c1, nchunk, mt, pA.as<__half>(), astride, pB.as<__half>(), bstride, sA.as<float>(), sastride,
-        sB.as<float>(), sbstride, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
+        N, r0, r1, c0, c1, nchunk, mt, pA.as<__half>(), astride, pB.as<__half>(), bstride, lmax, umax, w.mstride,
+        w.nblk, kcol, krow, K, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;

@@ -261,7 +261,9 @@ __global__ void __launch_bounds__(512) k_diag_factor(int N, int k, int kb, int b
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, float *__restrict__ planes,
                                                 size_t pstride, int ld, const float2 *__restrict__ dinv,
-                                                size_t dstride, const int *__restrict__ active) {
+                                                size_t dstride, const int *__restrict__ active,
+                                                float *__restrict__ lmax, float *__restrict__ umax,
+                                                size_t mstride, int nblk) {
     const int f = blockIdx.z;
     if (!active[f]) return;
     extern __shared__ float2 dyn[];
@@ -332,6 +334,38 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
                 Ai[base + (size_t)i * ld + j] = acc[a][b].y;
             }
         }
+    // maxima of the finished factor block: per column of the U block (row panel)
+    // or per row of the L block (column panel), over its 64 rows / columns
+    __shared__ float red[NB][17];
+    __syncthreads();   // M and T are no longer read
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = ty + 16 * a, j = tx + 16 * b;
+            const float v = (i < nrow && j < ncol) ? fmaxf(fabsf(acc[a][b].x), fabsf(acc[a][b].y)) : 0.f;
+            acc[a][b].x = v;
+        }
+    if (rowp) {
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            red[tx + 16 * b][ty] = fmaxf(fmaxf(acc[0][b].x, acc[1][b].x), fmaxf(acc[2][b].x, acc[3][b].x));
+    } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+            red[ty + 16 * a][tx] = fmaxf(fmaxf(acc[a][0].x, acc[a][1].x), fmaxf(acc[a][2].x, acc[a][3].x));
+    }
+    __syncthreads();
+    if (tid < NB) {
+        float m = 0.f;
+#pragma unroll
+        for (int q = 0; q < 16; q++) m = fmaxf(m, red[tid][q]);
+        if (rowp) {
+            if (tid < ncol) umax[mstride * f + (size_t)bi * ld + off + tid] = m;
+        } else {
+            if (tid < nrow) lmax[mstride * f + (size_t)(off + tid) * nblk + bi] = m;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -625,6 +659,9 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.vstride * B));
     EFIE_TRY(w.ctl.reserve(64 * (size_t)B + 64));
     EFIE_TRY(w.rpart.reserve(sizeof(double) * (size_t)B * ((N + 31) / 32)));
+    w.mstride = (size_t)w.ld * w.nblk;
+    EFIE_TRY(w.lmax.reserve(sizeof(float) * w.mstride * B));
+    EFIE_TRY(w.umax.reserve(sizeof(float) * w.mstride * B));
     EFIE_TRY(w.active.reserve(sizeof(int) * B));
     EFIE_TRY(efie_trsv_workspace(w));
     EFIE_TRY(efie_gemm_workspace(w));
@@ -707,7 +744,8 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
                 if (rest > 0) {
                     dim3 pg((rest + NB - 1) / NB, 2, B);
                     k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
-                                                        active);
+                                                        active, w.lmax.as<float>(), w.umax.as<float>(), w.mstride,
+                                                        w.nblk);
                 }
                 EFIE_CUDA(cudaGetLastError());
                 log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);

@@ -37,7 +37,11 @@ struct SolveWork {
     cudaStream_t hi = nullptr, lo = nullptr;
     cudaEvent_t ev_start = nullptr, ev_panel = nullptr, ev_rest = nullptr, ev_hi = nullptr;
     DevBuf packA2, packB2;
-    DevBuf sclA, sclB, sclA2, sclB2;   // power-of-two inverse scales of the FP16 operands (per row / column)
+    // max |Re|, |Im| of every row of each 64-column block of L (lmax[f][row][blk])
+    // and of every column of each 64-row block of U (umax[f][blk][col]), written
+    // with the factors; they give the split's power-of-two scales
+    DevBuf lmax, umax;
+    size_t mstride = 0;   // floats per frequency in lmax / umax (ld * nblk)
     SolveWork() = default;
     SolveWork(const SolveWork &) = delete;
     SolveWork &operator=(const SolveWork &) = delete;

@@ -25,19 +25,22 @@ constexpr int NB = 64;
 constexpr int DS = NB + 1;    // padded row stride of the diagonal inverse in shared memory
 constexpr int LINE = 8;       // u64 per 64-byte progress line
 
-__device__ __forceinline__ bool wait_progress(const volatile unsigned long long *ctr, unsigned long long target,
-                                              const volatile int *err) {
+// Wait until the counter reaches `target`; returns the observed value (0 on
+// timeout or error, after which every waiter returns).
+__device__ __forceinline__ unsigned long long wait_progress(const volatile unsigned long long *ctr,
+                                                            unsigned long long target, const volatile int *err) {
     long long spins = 0;
-    while (*ctr < target) {
+    unsigned long long v;
+    while ((v = *ctr) < target) {
         if (++spins > (1ll << 23)) {  // give up after ~1 s: record, let every waiter return
             atomicExch((int *)err, 2);
-            return false;
+            return 0;
         }
-        if ((spins & 63) == 0 && *err) return false;
+        if ((spins & 63) == 0 && *err) return 0;
         __nanosleep(40);
     }
     __threadfence();
-    return true;
+    return v;
 }
 
 // 16 consecutive complex entries of one row of the planes (zeros past `rows`).
@@ -78,7 +81,7 @@ __global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const floa
                                               char *ctl, const int *__restrict__ active) {
     __shared__ float2 Ds[NB * DS];
     __shared__ float2 acc[NB];
-    __shared__ float2 yj[NB];
+    __shared__ int avail_sh;
     __shared__ float2 part[4][NB];
     __shared__ int ok;
     const int tid = threadIdx.x;
@@ -114,29 +117,51 @@ __global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const floa
             const int jb0 = LOWER ? 0 : nblk - 1;
             load_tile_row(cur, Ar, Ai, rowoff + (size_t)jb0 * NB, rvalid);
         }
+        if (tid == 0) avail_sh = 0;
         __syncthreads();
+        // each thread keeps its quarter-row dot product in registers across the
+        // dependencies; the CTA synchronises only when it has to wait for a block
+        // that is not published yet (one observed count can cover many blocks)
+        float2 sdot = make_float2(0.f, 0.f);
+        int avail = 0;
         for (int q = 0; q < ndep; q++) {
             const int jb = LOWER ? q : nblk - 1 - q;
             float4 nxt[8];
             if (q + 1 < ndep) load_tile_row(nxt, Ar, Ai, rowoff + (size_t)(LOWER ? jb + 1 : jb - 1) * NB, rvalid);
-            if (tid == 0 && !wait_progress(myctr, tag | (unsigned long long)(q + 1), err)) ok = 0;
-            __syncthreads();
-            if (!ok) return;
-            // written by another CTA of this grid: read through L2 only
-            if (tid < NB) yj[tid] = (jb * NB + tid < N) ? __ldcg(out + jb * NB + tid) : make_float2(0.f, 0.f);
-            __syncthreads();
-            part[quarter][row] = dot16(cur, yj + quarter * 16);
-            __syncthreads();
-            if (tid < NB) {
-                float2 t = acc[tid];
-                t.x -= part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
-                t.y -= part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
-                acc[tid] = t;
+            if (q >= avail) {
+                if (tid == 0) {
+                    const unsigned long long v = wait_progress(myctr, tag | (unsigned long long)(q + 1), err);
+                    if (!v) ok = 0;
+                    avail_sh = (int)(v & 0xffffffffull);
+                }
+                __syncthreads();
+                if (!ok) return;
+                avail = avail_sh;
             }
+            // block jb of the solution: written by another CTA and published
+            // before `avail` was read, then never changed in this launch, so the
+            // (L1-cached) loads cannot see a stale line; a 64-entry block covers
+            // whole 128-byte lines
+            float2 y16[16];
+            const float2 *ysrc = out + jb * NB + quarter * 16;
+#pragma unroll
+            for (int c = 0; c < 16; c++)
+                y16[c] = (jb * NB + quarter * 16 + c < N) ? ysrc[c] : make_float2(0.f, 0.f);
+            const float2 t = dot16(cur, y16);
+            sdot.x += t.x;
+            sdot.y += t.y;
             if (q + 1 < ndep) {
 #pragma unroll
                 for (int i = 0; i < 8; i++) cur[i] = nxt[i];
             }
+        }
+        part[quarter][row] = sdot;
+        __syncthreads();
+        if (tid < NB) {
+            float2 t = acc[tid];
+            t.x -= part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
+            t.y -= part[0][tid].y + part[1][tid].y + part[2][tid].y + part[3][tid].y;
+            acc[tid] = t;
         }
         __syncthreads();
         // y_b = inv(diagonal block) * acc
