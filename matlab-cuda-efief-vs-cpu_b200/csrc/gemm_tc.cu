@@ -1,54 +1,67 @@
 // Trailing-matrix update of the complex64 LU on the 5th-generation tensor
 // cores: A22 -= L21 * U12.
 //
-// The complex product is realified into one real GEMM per 64-row block:
-//     [ Re ]   [ Lr  -Li ]   [ Ur ]
-//     [ Im ] = [ Li   Lr ] * [ Ui ]        (M' = 128 rows, K' = 2 kb)
-// and every operand is split into two FP16 terms after an exact power-of-two
-// scaling: each complex row of L21 by s_i and each column of U12 by t_j so
-// that the largest magnitude of the row (column) over the update's K range
-// lies in [1/2, 1); then x = hi + lo with hi = fp16(x), lo = fp16(x - hi)
-// (22 significant bits, the precision of a TF32 pair at half the bytes).  The
-// three products hi*hi + hi*lo + lo*hi accumulate in FP32 in tensor memory
-// (TMEM, kind::f16, K = 16 per instruction) and the epilogue multiplies by
-// 1/(s_i t_j), which is exact.  The update stays close to FP32 accuracy
-// normwise (the LU is then refined in FP64).
+// The complex product is written as four real products on separate real and
+// imaginary tiles,
+//     Re += Lr Ur - Li Ui        Im += Lr Ui + Li Ur,
+// with the minus sign taken by the MMA's negate-A bit, so no operand is
+// duplicated.  Every operand is split into two FP16 terms after an exact
+// power-of-two scaling: each complex row of L21 by s_i and each column of
+// U12 by t_j so that the largest magnitude of the row (column) over the
+// update's K range lies in [1/2, 1); then x = hi + lo with hi = fp16(x),
+// lo = fp16(x - hi) (22 significant bits).  The three products hi*hi + hi*lo
+// + lo*hi accumulate in FP32 in tensor memory (TMEM, kind::f16, K = 16 per
+// instruction) and the epilogue multiplies by 1/(s_i t_j), which is exact.
+// The update stays close to FP32 accuracy normwise (the LU is then refined in
+// FP64).
 //
-// Operands are packed per LU step into 64B-swizzled K-major tiles (32 FP16
-// per row) that sit contiguously in global memory, so each CTA fetches them
-// with plain bulk copies (cp.async.bulk, the TMA engine; no multicast, local
-// memory only).  One CTA computes two 128 x 256 accumulator tiles (2 x 64
-// complex rows x 256 complex columns) in the 512 TMEM columns of its SM, both
-// fed by the same B chunk, which halves the B bytes per MMA.  One elected
-// thread issues tcgen05.mma over a 3-stage shared-memory ring of K' chunks --
-// it issues chunk c's MMAs before waiting for chunk c-1's to retire, so the
-// tensor pipe always holds queued work while the bulk loads run ahead.
-// Meanwhile the other warps prefetch the CTA's rows of C into L2 (bulk
-// prefetch), and at the end all eight warps drain TMEM with tcgen05.ld -- two
-// warps per TMEM lane quarter, each taking half of the columns -- for the
-// read-modify-write epilogue on the row-major planes, reading the next 32
-// columns of C while they update the current ones.
+// Operands are packed per update into 64B-swizzled K-major tiles (32 FP16 per
+// row, 128 rows) that sit contiguously in global memory, so each CTA fetches
+// a K chunk of its operands with two plain bulk copies (cp.async.bulk, the TMA
+// engine; local memory only).  Two CTAs on the two SMs of a TPC form a
+// cluster and compute one 256 x 256 complex tile with cta_group::2 MMAs
+// (M = 256): each SM holds 128 rows of L21 (real and imaginary, hi and lo)
+// and half of the tile's 256 columns of U12, and keeps the real and the
+// imaginary accumulator of its 128 rows x 256 columns in its 512 TMEM
+// columns.  Per MMA cycle an SM thus reads half the operand bytes of a
+// realified single-SM tile.  One thread of the even CTA issues the MMAs over
+// a 3-stage ring of K chunks (chunk c's MMAs are queued before the stage of
+// chunk c-1 is refilled); the odd CTA's producer forwards the arrival of its
+// half of each chunk to the even CTA's barrier, and the MMA completions are
+// committed to the barriers of both CTAs.  Meanwhile the other warps prefetch
+// the CTA's rows of C into L2 (bulk prefetch).  At the end all eight warps
+// drain TMEM with tcgen05.ld -- four lane quarters x {real, imaginary} --,
+// scale and negate each 32 x 32 block into a 128B-swizzled shared-memory tile
+// and hand it to a bulk tensor reduction (cp.reduce.async.bulk.tensor .add),
+// so the read-modify-write of C happens in L2 and the SM never loads C; the
+// reductions drain while the next CTA on the SM runs its MMAs.  Each element
+// of C receives exactly one addition per update (deterministic); rows and
+// columns of a tile past the update's edge add exact zeros.
 // Every mbarrier wait is bounded; a timeout sets the device error flag.
 #include <cstdint>
 
+#include <cuda.h>
 #include <cuda_fp16.h>
+#include <cudaTypedefs.h>
 
 #include "solve.h"
 
 namespace {
 
 constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
-constexpr int TM = 128;          // accumulator rows (64 complex rows)
-constexpr int TN = 256;          // accumulator columns (complex columns)
-constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K' chunk)
-constexpr int NCHUNK_MAX = 2 * KMAX / KC;   // K' = 2K -> up to 16 chunks
-constexpr int A_TILE = TM * KC;       // halves per A tile (8 KB)
-constexpr int B_TILE = TN * KC;       // halves per B tile (16 KB)
-constexpr int MT = 2;            // 128-row accumulator tiles per CTA (TMEM columns: MT x 256)
-constexpr int STAGE_HALVES = MT * 2 * A_TILE + 2 * B_TILE;   // hi/lo of MT A tiles and of B: 64 KB
+constexpr int TR = 128;          // complex rows of L21 per CTA (one TMEM lane each)
+constexpr int TN = 256;          // complex columns of the pair's tile (MMA N)
+constexpr int TH = TN / 2;       // columns of U12 held by each CTA of the pair
+constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K chunk)
+constexpr int NCHUNK_MAX = KMAX / KC;
+constexpr int SUB = TR * KC;     // halves per 128 x 32 sub-tile (8 KB)
+// a packed K chunk of one 128-row (128-column) tile: re hi, re lo, im hi, im lo
+constexpr int CHUNK_HALVES = 4 * SUB;                      // 32 KB
+constexpr int STAGE_HALVES = 2 * CHUNK_HALVES;             // L chunk + U half chunk: 64 KB
 constexpr int NSTAGE = 3;
-constexpr int NBAR = 2 * NSTAGE + 1;  // full[NSTAGE], empty[NSTAGE], done
-constexpr size_t GEMM_SMEM = sizeof(__half) * NSTAGE * STAGE_HALVES + 1024 + 8 * NBAR + 16 + sizeof(float) * TN;
+constexpr int NBAR = 3 * NSTAGE + 1;  // full[], empty[], pair_full[], done
+constexpr size_t GEMM_SMEM =
+    sizeof(__half) * NSTAGE * STAGE_HALVES + 1024 + 8 * NBAR + 16 + sizeof(float) * TN;
 
 // byte offset of element (row r, k) inside a K-major 64B-swizzled tile of
 // fp16: the 16-byte chunk index (k / 8) XOR (r / 2) mod 4, 8-row atoms of 512 bytes
@@ -83,106 +96,95 @@ __device__ __forceinline__ float col_max(const float *um, int ld, int col, int b
 }
 
 // ---------------------------------------------------------------------------
-// Packing.  A: per 64-row block of L21 and K' chunk, a 128 x 32 tile (hi, lo).
-// B: per 256-column block of U12 and K' chunk, a 256 x 32 tile (hi, lo).
-// Tiles are built in shared memory in their final swizzled byte layout and
-// written out with coalesced 16-byte stores.
+// Packing.  L: per 128-row tile of L21 and K chunk, four 128 x 32 sub-tiles
+// (re hi, re lo, im hi, im lo).  U: the same per 128-column tile of U12.
+// Rows (columns) past the update's edge are zero.  Tiles are built in shared
+// memory in their final swizzled byte layout and written out with coalesced
+// 16-byte stores.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
     h = __float2half_rn(v);
     l = __float2half_rn(v - __half2float(h));
 }
 
-__global__ void __launch_bounds__(256) k_pack_a(int N, int r0, int r1, int kcol, int K, int nchunk,
+__device__ __forceinline__ void store_chunk(const __half *t, __half *dst) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(t);
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int e = threadIdx.x; e < CHUNK_HALVES / 8; e += blockDim.x) d4[e] = s4[e];
+}
+
+__global__ void __launch_bounds__(256) k_pack_l(int N, int r0, int r1, int kcol, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
                                                 const float *__restrict__ lmaxb, size_t mstride, int nblk,
                                                 __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
-    __shared__ __align__(1024) __half hi[A_TILE];
-    __shared__ __align__(1024) __half lo[A_TILE];
-    __shared__ float rscale[64];
+    __shared__ __align__(1024) __half t[CHUNK_HALVES];
+    __shared__ float rscale[TR];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
-    __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
-    if (threadIdx.x < 64) {
-        const int row = r0 + tile * 64 + threadIdx.x;
+    if (threadIdx.x < TR) {
+        const int row = r0 + tile * TR + threadIdx.x;
         rscale[threadIdx.x] =
             row < r1 ? pow2_scale(row_max(lmaxb + mstride * f, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < A_TILE; e += 256) {
+    for (int e = threadIdx.x; e < SUB; e += 256) {
         const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
-        const int kp = chunk * KC + kq;              // K' index
-        const bool second = kp >= K;
-        const int kk = second ? kp - K : kp;         // column within the L block
-        const int rl = tile * 64 + (r & 63);         // complex row within the update
-        const int row = r0 + rl;
-        float v = 0.f;
-        if (row < r1 && kk < K) {
-            const size_t o = (size_t)row * ld + kcol + kk;
-            if (r < 64) v = second ? -Ai[o] : Ar[o];     // [ Lr  -Li ]
-            else v = second ? Ar[o] : Ai[o];            // [ Li   Lr ]
-            v *= rscale[r & 63];                        // exact: a power of two
+        const int k = chunk * KC + kq;
+        const int row = r0 + tile * TR + r;
+        float vr = 0.f, vi = 0.f;
+        if (row < r1 && k < K) {
+            const size_t o = (size_t)row * ld + kcol + k;
+            vr = Ar[o] * rscale[r];                   // exact: a power of two
+            vi = Ai[o] * rscale[r];
         }
         const uint32_t off = swz(r, kq) >> 1;
-        split_half(v, hi[off], lo[off]);
+        split_half(vr, t[off], t[SUB + off]);
+        split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
     }
     __syncthreads();
-    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * A_TILE);
-    const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
-    for (int e = threadIdx.x; e < A_TILE / 8; e += 256) {
-        dst[e] = h4[e];
-        dst[A_TILE / 8 + e] = l4[e];
-    }
+    store_chunk(t, outb + ostride * f + (size_t)(tile * nchunk + chunk) * CHUNK_HALVES);
 }
 
-__global__ void __launch_bounds__(256) k_pack_b(int N, int c0, int c1, int krow, int K, int nchunk,
+__global__ void __launch_bounds__(256) k_pack_u(int N, int c0, int c1, int krow, int K, int nchunk,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
                                                 const float *__restrict__ umaxb, size_t mstride,
                                                 __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
-    extern __shared__ __align__(1024) __half dynb[];
-    __half *hi = dynb, *lo = dynb + B_TILE;
-    __shared__ float cscale[TN];
+    __shared__ __align__(1024) __half t[CHUNK_HALVES];
+    __shared__ float cscale[TH];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
-    __half *out = outb + ostride * f;
     const int tile = blockIdx.x, chunk = blockIdx.y;
-    {
-        const int col = c0 + tile * TN + threadIdx.x;   // 256 threads: one column each
+    if (threadIdx.x < TH) {
+        const int col = c0 + tile * TH + threadIdx.x;
         cscale[threadIdx.x] =
             col < c1 ? pow2_scale(col_max(umaxb + mstride * f, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < B_TILE; e += 256) {
-        const int kq = e >> 8, n = e & 255;          // consecutive threads: consecutive columns
-        const int kp = chunk * KC + kq;
-        const bool second = kp >= K;
-        const int kk = second ? kp - K : kp;
-        const int cl = tile * TN + n;
-        const int col = c0 + cl;
-        float v = 0.f;
-        if (col < c1 && kk < K) {
-            const size_t o = (size_t)(krow + kk) * ld + col;
-            v = (second ? Ai[o] : Ar[o]) * cscale[n];   // [ Ur ; Ui ], exact scaling
+    for (int e = threadIdx.x; e < SUB; e += 256) {
+        const int kq = e >> 7, n = e & (TH - 1);     // consecutive threads: consecutive columns
+        const int k = chunk * KC + kq;
+        const int col = c0 + tile * TH + n;
+        float vr = 0.f, vi = 0.f;
+        if (col < c1 && k < K) {
+            const size_t o = (size_t)(krow + k) * ld + col;
+            vr = Ar[o] * cscale[n];
+            vi = Ai[o] * cscale[n];
         }
         const uint32_t off = swz(n, kq) >> 1;
-        split_half(v, hi[off], lo[off]);
+        split_half(vr, t[off], t[SUB + off]);
+        split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
     }
     __syncthreads();
-    float4 *dst = reinterpret_cast<float4 *>(out + ((size_t)(tile * nchunk + chunk) * 2) * B_TILE);
-    const float4 *h4 = reinterpret_cast<const float4 *>(hi), *l4 = reinterpret_cast<const float4 *>(lo);
-    for (int e = threadIdx.x; e < B_TILE / 8; e += 256) {
-        dst[e] = h4[e];
-        dst[B_TILE / 8 + e] = l4[e];
-    }
+    store_chunk(t, outb + ostride * f + (size_t)(tile * nchunk + chunk) * CHUNK_HALVES);
 }
 
 // ---------------------------------------------------------------------------
-// tcgen05 / mbarrier / bulk-copy primitives (inline PTX)
+// tcgen05 / mbarrier / bulk-copy / cluster primitives (inline PTX)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -193,11 +195,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
+// try_wait with acquire at cluster scope: also orders what the peer CTA
+// released before its remote arrive
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity)
@@ -215,11 +219,49 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
     return false;
 }
 
+// address of the same shared-memory object in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// C[f][plane][y .. y+31][x .. x+31] += the 32 x 32 fp32 tile at `src`
+// (128B-swizzled rows); coordinates past the tensor's edge are skipped
+__device__ __forceinline__ void reduce_add_tile(const CUtensorMap *map, const float *src, int x, int y, int plane,
+                                                int f) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.4d.global.shared::cta.add.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(smem_u32(src)), "r"(x), "r"(y), "r"(plane), "r"(f)
+        : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ uint64_t desc_sw64(const void *smem_tile) {
@@ -233,20 +275,25 @@ __device__ __forceinline__ uint64_t desc_sw64(const void *smem_tile) {
     return d;
 }
 
-// kind::f16, D = F32, A = B = F16, both K-major, N = 256, M = 128
+// kind::f16, D = F32, A = B = F16, both K-major, M = 256 (CTA pair), N = 256;
+// bit 13 negates A
 constexpr uint32_t IDESC = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
+                           ((uint32_t)(2 * TR >> 4) << 24);
+constexpr uint32_t IDESC_NEG_A = IDESC | (1u << 13);
 
-__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
 }
 
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+// arrive on the barrier at a shared::cluster address (this CTA's or the peer's)
+// once every MMA issued so far by this thread has completed
+__device__ __forceinline__ void mma_commit(uint32_t cluster_bar) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(cluster_bar)
                  : "memory");
 }
 
@@ -264,106 +311,144 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 }
 
 // ---------------------------------------------------------------------------
-// The update kernel: grid (ceil(m/256), ceil(m/64)), 128 threads.
+// The update kernel.  C[r0:r1, c0:c1] -= (packed L) * (packed U) for the
+// pair's 256 x 256 tile; grid (2 x column tiles, row-pair tiles, frequency),
+// clusters of two CTAs along x, 256 threads.
 // ---------------------------------------------------------------------------
-// C[r0:r1, c0:c1] -= (packed A) * (packed B) for the CTA's tiles; grid
-// (column tiles, pairs of 64-row tiles, frequency), 256 threads.
-__global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int c0, int c1, int nchunk, int mt,
-                                                      const __half *__restrict__ Apackb, size_t astride,
-                                                      const __half *__restrict__ Bpackb, size_t bstride,
-                                                      const float *__restrict__ lmaxb, const float *__restrict__ umaxb,
-                                                      size_t mstride, int nblk, int kcol, int krow, int K,
-                                                      float *__restrict__ planes, size_t pstride, int ld,
-                                                      char *__restrict__ ctl, const int *__restrict__ active) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+    k_update_tc(const __grid_constant__ CUtensorMap cmap, int N, int r0, int r1, int c0, int c1, int nchunk, const __half *__restrict__ Lpackb,
+                size_t lstride, const __half *__restrict__ Upackb, size_t ustride, const float *__restrict__ lmaxb,
+                const float *__restrict__ umaxb, size_t mstride, int nblk, int kcol, int krow, int K,
+                float *__restrict__ planes, size_t pstride, int ld, char *__restrict__ ctl,
+                const int *__restrict__ active) {
     const int f = blockIdx.z;
-    if (!active[f]) return;
-    const __half *Apack = Apackb + astride * f, *Bpack = Bpackb + bstride * f;
+    if (!active[f]) return;   // both CTAs of a cluster share f
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const __half *Lpack = Lpackb + lstride * f, *Upack = Upackb + ustride * f;
     const float *lm = lmaxb + mstride * f, *um = umaxb + mstride * f;
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
     extern __shared__ uint8_t dyn_raw[];
-    // 1024-byte alignment for the swizzled tiles
+    // 1024-byte alignment for the swizzled tiles (the same offset in both CTAs)
     __half *stage = reinterpret_cast<__half *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_HALVES);  // full[], empty[], done
-    uint64_t *full = bars, *empty = bars + NSTAGE, *done = bars + 2 * NSTAGE;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_HALVES);
+    uint64_t *full = bars, *empty = bars + NSTAGE, *pfull = bars + 2 * NSTAGE, *done = bars + 3 * NSTAGE;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + NBAR);
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
-    float *col_is = reinterpret_cast<float *>(bars + 8);   // 16-byte aligned: inverse column scales of the tile
+    float *col_is = reinterpret_cast<float *>(bars + 12);   // 16-byte aligned: inverse column scales
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile_n = blockIdx.x, tile_m0 = blockIdx.y * MT;
-    const int nm = min(MT, mt - tile_m0);            // accumulator tiles of this CTA (1 or 2)
+    const int ct = blockIdx.x >> 1;                  // 256-column tile of the pair
+    const int rtile = blockIdx.y * 2 + (int)rank;    // this CTA's 128-row tile
+    const int utile = ct * 2 + (int)rank;            // this CTA's 128-column half of U
 
     if (tid == 0) {
         for (int i = 0; i < NBAR; i++) mbar_init(&bars[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *ok_sh = 1;
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(MT * TN));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
+    cluster_sync();   // barriers initialised and TMEM allocated in both CTAs
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    bool ok = true;
-    if (tid == 0) *ok_sh = 1;
     if (tid == 0) {
-        const __half *gb = Bpack + (size_t)tile_n * nchunk * 2 * B_TILE;
-        const uint32_t abytes = sizeof(__half) * 2 * A_TILE, bbytes = sizeof(__half) * 2 * B_TILE;
+        bool ok = true;
+        const __half *gl = Lpack + (size_t)rtile * nchunk * CHUNK_HALVES;
+        const __half *gu = Upack + (size_t)utile * nchunk * CHUNK_HALVES;
+        constexpr uint32_t cbytes = sizeof(__half) * CHUNK_HALVES;
         auto load = [&](int c) {
             __half *st = stage + (c % NSTAGE) * STAGE_HALVES;
-            mbar_expect_tx(&full[c % NSTAGE], nm * abytes + bbytes);
-            for (int mi = 0; mi < nm; mi++)
-                bulk_g2s(st + mi * 2 * A_TILE, Apack + ((size_t)(tile_m0 + mi) * nchunk + c) * 2 * A_TILE, abytes,
-                         &full[c % NSTAGE]);
-            bulk_g2s(st + MT * 2 * A_TILE, gb + (size_t)c * 2 * B_TILE, bbytes, &full[c % NSTAGE]);
+            mbar_expect_tx(&full[c % NSTAGE], 2 * cbytes);
+            bulk_g2s(st, gl + (size_t)c * CHUNK_HALVES, cbytes, &full[c % NSTAGE]);
+            bulk_g2s(st + CHUNK_HALVES, gu + (size_t)c * CHUNK_HALVES, cbytes, &full[c % NSTAGE]);
         };
         for (int c = 0; c < NSTAGE && c < nchunk; c++) load(c);
-        for (int c = 0; c < nchunk && ok; c++) {
-            const int sidx = c % NSTAGE;
-            if (!mbar_wait(&full[sidx], (c / NSTAGE) & 1, err)) { ok = false; break; }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const __half *st = stage + sidx * STAGE_HALVES;
-            const uint64_t bhi = desc_sw64(st + MT * 2 * A_TILE), blo = desc_sw64(st + MT * 2 * A_TILE + B_TILE);
-            for (int mi = 0; mi < nm; mi++) {
-                const uint64_t ahi = desc_sw64(st + mi * 2 * A_TILE), alo = desc_sw64(st + mi * 2 * A_TILE + A_TILE);
-                const uint32_t acc = tmem + (uint32_t)(mi * TN);
+        if (leader) {
+            const uint32_t done_me = smem_u32(done), done_peer = peer_addr(done, 1);
+            for (int c = 0; c < nchunk && ok; c++) {
+                const int sidx = c % NSTAGE;
+                const uint32_t par = (c / NSTAGE) & 1;
+                if (!mbar_wait(&full[sidx], par, err) || !mbar_wait(&pfull[sidx], par, err)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const __half *st = stage + sidx * STAGE_HALVES;
+                const uint64_t lrh = desc_sw64(st), lrl = desc_sw64(st + SUB), lih = desc_sw64(st + 2 * SUB),
+                               lil = desc_sw64(st + 3 * SUB);
+                const __half *su = st + CHUNK_HALVES;
+                const uint64_t urh = desc_sw64(su), url = desc_sw64(su + SUB), uih = desc_sw64(su + 2 * SUB),
+                               uil = desc_sw64(su + 3 * SUB);
+                const uint32_t dre = tmem, dim = tmem + TN;
 #pragma unroll
                 for (int kk = 0; kk < KC / 16; kk++) {
-                    const uint64_t adv = (uint64_t)((kk * 32) >> 4);   // 16 fp16 = 32 bytes along K
-                    // small terms first, then the leading product
-                    mma_f16(acc, alo + adv, bhi + adv, (c > 0 || kk > 0) ? 1u : 0u);
-                    mma_f16(acc, ahi + adv, blo + adv, 1u);
-                    mma_f16(acc, ahi + adv, bhi + adv, 1u);
+                    const uint64_t a = (uint64_t)((kk * 32) >> 4);   // 16 fp16 = 32 bytes along K
+                    const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
+                    // Re += Lr Ur - Li Ui; small terms first, then the leading product
+                    mma_pair(dre, lrl + a, urh + a, IDESC, acc0);
+                    mma_pair(dre, lrh + a, url + a, IDESC, 1u);
+                    mma_pair(dre, lil + a, uih + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lih + a, uil + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lih + a, uih + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lrh + a, urh + a, IDESC, 1u);
+                    // Im += Lr Ui + Li Ur
+                    mma_pair(dim, lrl + a, uih + a, IDESC, acc0);
+                    mma_pair(dim, lrh + a, uil + a, IDESC, 1u);
+                    mma_pair(dim, lil + a, urh + a, IDESC, 1u);
+                    mma_pair(dim, lih + a, url + a, IDESC, 1u);
+                    mma_pair(dim, lih + a, urh + a, IDESC, 1u);
+                    mma_pair(dim, lrh + a, uih + a, IDESC, 1u);
+                }
+                // stage sidx is free in both CTAs once these MMAs have read it
+                mma_commit(smem_u32(&empty[sidx]));
+                mma_commit(peer_addr(&empty[sidx], 1));
+                // refill the stage of chunk c - 1: its MMAs were queued ahead of chunk
+                // c's, so waiting for them leaves chunk c's MMAs on the tensor pipe
+                const int cp = c - 1;
+                if (cp >= 0 && cp + NSTAGE < nchunk) {
+                    if (!mbar_wait(&empty[cp % NSTAGE], (cp / NSTAGE) & 1, err)) { ok = false; break; }
+                    load(cp + NSTAGE);
                 }
             }
-            mma_commit(&empty[sidx]);   // stage sidx free once these MMAs have read it
-            // refill the stage of chunk c - 1: its MMAs were queued ahead of chunk
-            // c's, so waiting for them leaves chunk c's MMAs on the tensor pipe
-            const int cp = c - 1;
-            if (cp >= 0 && cp + NSTAGE < nchunk) {
-                if (!mbar_wait(&empty[cp % NSTAGE], (cp / NSTAGE) & 1, err)) { ok = false; break; }
-                load(cp + NSTAGE);
+            // all MMAs of the pair done: both CTAs' accumulators are complete
+            mma_commit(done_me);
+            mma_commit(done_peer);
+        } else {
+            // the odd CTA: forward the arrival of each chunk to the even CTA's
+            // barrier, refill a stage once the MMAs that read it are done
+            const uint32_t pf0 = peer_addr(pfull, 0);
+            for (int c = 0; c < nchunk && ok; c++) {
+                const int sidx = c % NSTAGE;
+                if (!mbar_wait(&full[sidx], (c / NSTAGE) & 1, err)) { ok = false; break; }
+                mbar_arrive_remote(pf0 + 8u * (uint32_t)sidx);
+                const int cp = c - 1;
+                if (cp >= 0 && cp + NSTAGE < nchunk) {
+                    if (!mbar_wait(&empty[cp % NSTAGE], (cp / NSTAGE) & 1, err)) { ok = false; break; }
+                    load(cp + NSTAGE);
+                }
             }
         }
-        mma_commit(done);                  // all MMAs of this CTA done
         if (!ok) *ok_sh = 0;
     } else if (warp > 0) {
         // inverse column scales of the tile into shared memory
         for (int j = tid - 32; j < TN; j += 224) {
-            const int col = c0 + tile_n * TN + j;
+            const int col = c0 + ct * TN + j;
             col_is[j] = (col < c1) ? 1.f / pow2_scale(col_max(um, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
         }
-        // C rows of this CTA into L2 while the MMAs run: (accumulator, plane, row) segments
-        const int ncol = min(TN, c1 - (c0 + tile_n * TN));
+        // C rows of this CTA into L2 while the MMAs run: (plane, row) segments
+        const int ncol = min(TN, c1 - (c0 + ct * TN));
         const uint32_t bytes = (uint32_t)((ncol * 4 + 15) & ~15);
-        for (int e = tid - 32; e < nm * 2 * 64; e += 224) {
-            const int mi = e >> 7, pl = (e >> 6) & 1, rr = e & 63;
-            const int row = r0 + (tile_m0 + mi) * 64 + rr;
+        for (int e = tid - 32; e < 2 * TR; e += 224) {
+            const int pl = e / TR, rr = e % TR;
+            const int row = r0 + rtile * TR + rr;
             if (row < r1 && ncol > 0) {
-                const float *src = (pl ? Ai : Ar) + (size_t)row * ld + c0 + tile_n * TN;
+                const float *src = (pl ? Ai : Ar) + (size_t)row * ld + c0 + ct * TN;
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
             }
         }
@@ -375,65 +460,51 @@ __global__ void __launch_bounds__(256, 1) k_update_tc(int N, int r0, int r1, int
     have = __all_sync(0xffffffffu, have) && (*ok_sh != 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (have) {
-        // TMEM lane quarter of this warp (tcgen05.ld reaches lanes 32 (warp mod 4) ...)
-        const int quarter = warp & 3;
-        const int half = quarter & 1;               // rows 0-31 or 32-63 of a complex block
-        float *plane = (quarter < 2) ? Ar : Ai;     // quarters 0,1: real part; 2,3: imaginary part
-        constexpr int NJ = TN / 32;
-        const int j0 = (warp >> 2) * (NJ / 2), j1 = j0 + NJ / 2;   // this warp's half of the columns
-        for (int mi = 0; mi < nm; mi++) {
-            const int rl = (tile_m0 + mi) * 64 + half * 32 + lane;   // complex row within the update
-            const int row = r0 + rl;
-            const bool rok = row < r1;
-            const float rs = rok ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
-            const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mi * TN);
-            float *prow = plane + (size_t)(rok ? row : r0) * ld + c0 + tile_n * TN;
-            const int ncol = c1 - (c0 + tile_n * TN);   // valid columns of this tile (may exceed TN)
-            // C of chunk j + 1 is read while chunk j is updated
-            float4 cur[8], nxt[8];
-            auto fetch = [&](int j, float4 (&d)[8]) {
-                if (rok && (j + 1) * 32 <= ncol) {
-                    const float4 *p4 = reinterpret_cast<const float4 *>(prow + j * 32);
-#pragma unroll
-                    for (int q = 0; q < 8; q++) d[q] = p4[q];
-                }
-            };
-            fetch(j0, cur);
+        const int quarter = warp & 3;               // TMEM lanes 32 quarter ... (tcgen05.ld reach of this warp)
+        const int pl = warp >> 2;                   // 0: real part, 1: imaginary part
+        const int rowq = r0 + rtile * TR + quarter * 32;   // first row of this warp's 32
+        const int ncol = c1 - (c0 + ct * TN);       // valid columns of this tile (may exceed TN)
+        if (rowq < r1) {                            // warp-uniform
+            const int row = rowq + lane;
+            const float rs = row < r1 ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
+            const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(pl * TN);
+            // the stages are free once the MMAs are done: four 4 KB tiles per warp
+            float *ring = reinterpret_cast<float *>(stage) + warp * 4 * 1024;
+            constexpr int NJ = TN / 32;
 #pragma unroll 1
-            for (int j = j0; j < j1; j++) {
-                if (j + 1 < j1) fetch(j + 1, nxt);
+            for (int j = 0; j < NJ && j * 32 < ncol; j++) {
                 uint32_t v[32];
                 tmem_ld32(tbase + j * 32, v);
-                const int col0 = j * 32;
-                if (rok && col0 < ncol) {
-                    float *p = prow + col0;
-                    if (col0 + 32 <= ncol) {
-                        float4 *p4 = reinterpret_cast<float4 *>(p);
-#pragma unroll
-                        for (int q = 0; q < 8; q++) {
-                            const float4 cs = *reinterpret_cast<const float4 *>(col_is + col0 + 4 * q);
-                            float4 a = cur[q];
-                            a.x -= __uint_as_float(v[4 * q]) * (rs * cs.x);
-                            a.y -= __uint_as_float(v[4 * q + 1]) * (rs * cs.y);
-                            a.z -= __uint_as_float(v[4 * q + 2]) * (rs * cs.z);
-                            a.w -= __uint_as_float(v[4 * q + 3]) * (rs * cs.w);
-                            p4[q] = a;
-                        }
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 32; q++)
-                            if (col0 + q < ncol) p[q] -= __uint_as_float(v[q]) * (rs * col_is[col0 + q]);
-                    }
+                float *tile = ring + (j & 3) * 1024;
+                if (j >= 4) {   // the reduction that read this tile four blocks ago is done with it
+                    if (lane == 0) bulk_wait_read<3>();
+                    __syncwarp();
                 }
+                // row `lane` of the tile; 16-byte chunk q sits at chunk q ^ (lane mod 8)
 #pragma unroll
-                for (int q = 0; q < 8; q++) cur[q] = nxt[q];
+                for (int q = 0; q < 8; q++) {
+                    const float4 cs = *reinterpret_cast<const float4 *>(col_is + j * 32 + 4 * q);
+                    const float s0 = rs * cs.x, s1 = rs * cs.y, s2 = rs * cs.z, s3 = rs * cs.w;
+                    float4 x;   // exact zeros outside the update (never 0 * inf)
+                    x.x = s0 != 0.f ? -__uint_as_float(v[4 * q]) * s0 : 0.f;
+                    x.y = s1 != 0.f ? -__uint_as_float(v[4 * q + 1]) * s1 : 0.f;
+                    x.z = s2 != 0.f ? -__uint_as_float(v[4 * q + 2]) * s2 : 0.f;
+                    x.w = s3 != 0.f ? -__uint_as_float(v[4 * q + 3]) * s3 : 0.f;
+                    *reinterpret_cast<float4 *>(tile + lane * 32 + ((q ^ (lane & 7)) << 2)) = x;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // visible to the bulk copy
+                __syncwarp();
+                if (lane == 0) reduce_add_tile(&cmap, tile, c0 + ct * TN + j * 32, rowq, pl, f);
             }
+            if (lane == 0) bulk_wait_read<0>();   // shared memory is read before the CTA exits
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
+    // both CTAs are past every access to each other's shared memory and TMEM
+    cluster_sync();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MT * TN));
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN));
     }
 }
 
@@ -445,25 +516,56 @@ efie_status efie_tc_attrs() {
     static bool done = false;
     if (done) return EFIE_OK;
     EFIE_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
-    EFIE_CUDA(cudaFuncSetAttribute(k_pack_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(__half) * 2 * B_TILE)));
     done = true;
     return EFIE_OK;
 }
 
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
 
-// Staging for the largest update of an N x N LU (per frequency slot), and the
-// kernel attributes: done when the workspace is created, so that the factor
-// sequence allocates nothing and can be captured into a CUDA graph.
+namespace {
+// packed K chunks of one frequency slot for the largest update of an N x N
+// LU: 2 ceil(N / 256) tiles of 128 rows (columns), up to 8 chunks each
+size_t pack_stride(int N) { return (size_t)2 * ((N + TN - 1) / TN) * NCHUNK_MAX * CHUNK_HALVES; }
+}  // namespace
+
+namespace {
+// the planes of every frequency slot as one float tensor [B][2][N][ld]
+// (innermost first: column, row, plane, slot), 32 x 32 boxes, 128B swizzle
+efie_status encode_planes_map(SolveWork &w) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        EFIE_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[4] = {(cuuint64_t)w.N, (cuuint64_t)w.N, 2, (cuuint64_t)w.B};
+    const cuuint64_t strides[3] = {sizeof(float) * (cuuint64_t)w.ld, sizeof(float) * (cuuint64_t)w.ld * w.N,
+                                   sizeof(float) * (cuuint64_t)w.pstride};
+    const cuuint32_t box[4] = {32, 32, 1, 1}, estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode(reinterpret_cast<CUtensorMap *>(w.planes_map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                              w.planes.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the LU planes");
+    return EFIE_OK;
+}
+}  // namespace
+
+// Staging for the largest update of an N x N LU (per frequency slot), the
+// planes' tensor map and the kernel attributes: done when the workspace is
+// created (after the planes), so that the factor sequence allocates nothing
+// and can be captured into a CUDA graph.
 efie_status efie_gemm_workspace(SolveWork &w) {
     EFIE_TRY(efie_tc_attrs());
-    const int mt0 = (w.N + 63) / 64, nt0 = (w.N + TN - 1) / TN;
-    const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
-    EFIE_TRY(w.packA.reserve(sizeof(__half) * astride * w.B));
-    EFIE_TRY(w.packB.reserve(sizeof(__half) * bstride * w.B));
-    EFIE_TRY(w.packA2.reserve(sizeof(__half) * astride * w.B));
-    EFIE_TRY(w.packB2.reserve(sizeof(__half) * bstride * w.B));
+    EFIE_TRY(encode_planes_map(w));
+    const size_t bytes = sizeof(__half) * pack_stride(w.N) * w.B;
+    EFIE_TRY(w.packA.reserve(bytes));
+    EFIE_TRY(w.packB.reserve(bytes));
+    EFIE_TRY(w.packA2.reserve(bytes));
+    EFIE_TRY(w.packB2.reserve(bytes));
     return EFIE_OK;
 }
 
@@ -483,29 +585,27 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     EFIE_TRY(efie_tc_attrs());
     const int N = w.N, B = w.B;
     cudaStream_t st = ctx->stream;
-    const int mt = (rows + 63) / 64, nt = (cols + TN - 1) / TN;
-    const int nchunk = (2 * K + KC - 1) / KC;
-    // per-frequency staging sized for the largest update of an N x N LU
-    const int mt0 = (N + 63) / 64, nt0 = (N + TN - 1) / TN;
-    const size_t astride = (size_t)mt0 * NCHUNK_MAX * 2 * A_TILE, bstride = (size_t)nt0 * NCHUNK_MAX * 2 * B_TILE;
-    DevBuf &pA = slot ? w.packA2 : w.packA, &pB = slot ? w.packB2 : w.packB;
-    EFIE_TRY(pA.reserve(sizeof(__half) * astride * B));
-    EFIE_TRY(pB.reserve(sizeof(__half) * bstride * B));
+    const int npr = (rows + TN - 1) / TN, nct = (cols + TN - 1) / TN;   // 256-row pairs, 256-column tiles
+    const int nchunk = (K + KC - 1) / KC;
+    const size_t stride = pack_stride(N);
+    DevBuf &pL = slot ? w.packA2 : w.packA, &pU = slot ? w.packB2 : w.packB;
+    EFIE_TRY(pL.reserve(sizeof(__half) * stride * B));
+    EFIE_TRY(pU.reserve(sizeof(__half) * stride * B));
     float *planes = w.planes.as<float>();
     const int *active = w.active.as<int>();
     const float *lmax = w.lmax.as<float>(), *umax = w.umax.as<float>();
     KernelLog &log = ctx->log;
     size_t tok = log.begin(st);
-    k_pack_a<<<dim3(mt, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld, lmax,
-                                                  w.mstride, w.nblk, pA.as<__half>(), astride, active);
-    k_pack_b<<<dim3(nt, nchunk, B), 256, sizeof(__half) * 2 * B_TILE, st>>>(
-        N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, umax, w.mstride, pB.as<__half>(), bstride, active);
+    k_pack_l<<<dim3(2 * npr, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld, lmax,
+                                                       w.mstride, w.nblk, pL.as<__half>(), stride, active);
+    k_pack_u<<<dim3(2 * nct, nchunk, B), 256, 0, st>>>(N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, umax,
+                                                       w.mstride, pU.as<__half>(), stride, active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
     tok = log.begin(st);
-    k_update_tc<<<dim3(nt, (mt + MT - 1) / MT, B), 256, GEMM_SMEM, st>>>(
-        N, r0, r1, c0, c1, nchunk, mt, pA.as<__half>(), astride, pB.as<__half>(), bstride, lmax, umax, w.mstride,
-        w.nblk, kcol, krow, K, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
+    k_update_tc<<<dim3(2 * nct, npr, B), 256, GEMM_SMEM, st>>>(
+        *reinterpret_cast<const CUtensorMap *>(w.planes_map), N, r0, r1, c0, c1, nchunk, pL.as<__half>(), stride, pU.as<__half>(), stride, lmax, umax, w.mstride, w.nblk,
+        kcol, krow, K, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;

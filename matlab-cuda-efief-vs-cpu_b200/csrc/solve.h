@@ -42,6 +42,10 @@ struct SolveWork {
     // with the factors; they give the split's power-of-two scales
     DevBuf lmax, umax;
     size_t mstride = 0;   // floats per frequency in lmax / umax (ld * nblk)
+    // TMA tensor map (CUtensorMap) of the planes as float [B][2][N][ld], boxes
+    // of 32 x 32: the tensor-core update adds its tiles into the factors with
+    // bulk tensor reductions
+    alignas(64) unsigned char planes_map[128] = {};
     SolveWork() = default;
     SolveWork(const SolveWork &) = delete;
     SolveWork &operator=(const SolveWork &) = delete;
