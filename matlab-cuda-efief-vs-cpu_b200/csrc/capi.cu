@@ -503,7 +503,7 @@ int choose_batch(int N, int requested, int solver) {
     freeb += efie_pool_cached(dev);   // cached blocks are available to this plan
     const double per = 26.0 * (double)N * N + 1e6;
     int B = (int)std::floor(0.35 * (double)freeb / per);
-    return std::max(1, std::min(B, 8));
+    return std::max(1, std::min(B, EFIE_MAX_BATCH));
 }
 
 // Outer LU panel width: the caller's choice, else the tuned table (wider

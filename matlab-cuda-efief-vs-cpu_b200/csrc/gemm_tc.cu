@@ -15,10 +15,11 @@
 // The update stays close to FP32 accuracy normwise (the LU is then refined in
 // FP64).
 //
-// Operands are packed per update into 64B-swizzled K-major tiles (32 FP16 per
-// row, 128 rows) that sit contiguously in global memory, so each CTA fetches
-// a K chunk of its operands with two plain bulk copies (cp.async.bulk, the TMA
-// engine; local memory only).  Two CTAs on the two SMs of a TPC form a
+// Operands are packed once per panel (the panel kernel packs the 64-wide
+// blocks of the panel chain itself) into planes of 64B-swizzled K-major rows
+// (32 FP16 per row) in which any 128 rows are contiguous, so each CTA fetches
+// a K chunk of its operands with eight plain bulk copies (cp.async.bulk, the
+// TMA engine; local memory only) from any row offset of the panel.  Two CTAs on the two SMs of a TPC form a
 // cluster and compute one 256 x 256 complex tile with cta_group::2 MMAs
 // (M = 256): each SM holds 128 rows of L21 (real and imaginary, hi and lo)
 // and half of the tile's 256 columns of U12, and keeps the real and the
@@ -51,7 +52,6 @@ namespace {
 constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
 constexpr int TR = 128;          // complex rows of L21 per CTA (one TMEM lane each)
 constexpr int TN = 256;          // complex columns of the pair's tile (MMA N)
-constexpr int TH = TN / 2;       // columns of U12 held by each CTA of the pair
 constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K chunk)
 constexpr int NCHUNK_MAX = KMAX / KC;
 constexpr int SUB = TR * KC;     // halves per 128 x 32 sub-tile (8 KB)
@@ -63,19 +63,8 @@ constexpr int NBAR = 3 * NSTAGE + 1;  // full[], empty[], pair_full[], done
 constexpr size_t GEMM_SMEM =
     sizeof(__half) * NSTAGE * STAGE_HALVES + 1024 + 8 * NBAR + 16 + sizeof(float) * TN;
 
-// byte offset of element (row r, k) inside a K-major 64B-swizzled tile of
-// fp16: the 16-byte chunk index (k / 8) XOR (r / 2) mod 4, 8-row atoms of 512 bytes
-__host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) {
-    return r * 64u + ((((k >> 3) ^ (r >> 1)) & 3u) << 4) + ((k & 7u) << 1);
-}
-
-// 2^-e with max * 2^-e in [1/2, 1) (1 for a zero maximum)
-__device__ __forceinline__ float pow2_scale(float mx) {
-    if (!(mx > 0.f)) return 1.f;
-    int e;
-    frexpf(mx, &e);
-    return ldexpf(1.f, -e);
-}
+__host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) { return efie_swz64(r, k); }
+__device__ __forceinline__ float pow2_scale(float mx) { return efie_pow2_scale(mx); }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -96,24 +85,25 @@ __device__ __forceinline__ float col_max(const float *um, int ld, int col, int b
 }
 
 // ---------------------------------------------------------------------------
-// Packing.  L: per 128-row tile of L21 and K chunk, four 128 x 32 sub-tiles
-// (re hi, re lo, im hi, im lo).  U: the same per 128-column tile of U12.
-// Rows (columns) past the update's edge are zero.  Tiles are built in shared
-// memory in their final swizzled byte layout and written out with coalesced
-// 16-byte stores.
+// Packing: a CTA builds the four components (re hi, re lo, im hi, im lo) of
+// 128 rows of L21 (columns of U12) and one K chunk in shared memory, in their
+// swizzled byte layout, and writes each as one contiguous 8 KB block of its
+// plane.  Rows (columns) past the panel's edge are zero.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
     h = __float2half_rn(v);
     l = __float2half_rn(v - __half2float(h));
 }
 
-__device__ __forceinline__ void store_chunk(const __half *t, __half *dst) {
-    const float4 *s4 = reinterpret_cast<const float4 *>(t);
-    float4 *d4 = reinterpret_cast<float4 *>(dst);
-    for (int e = threadIdx.x; e < CHUNK_HALVES / 8; e += blockDim.x) d4[e] = s4[e];
+// the four 128-row component tiles of one chunk to their planes
+__device__ __forceinline__ void store_planes(const __half *t, __half *dst, int pitch) {
+    for (int e = threadIdx.x; e < CHUNK_HALVES / 8; e += blockDim.x) {
+        const int comp = e / (SUB / 8), i = e % (SUB / 8);
+        reinterpret_cast<float4 *>(dst + (size_t)comp * pitch * KC)[i] = reinterpret_cast<const float4 *>(t)[e];
+    }
 }
 
-__global__ void __launch_bounds__(256) k_pack_l(int N, int r0, int r1, int kcol, int K, int nchunk,
+__global__ void __launch_bounds__(256) k_pack_l(int N, int r0, int r1, int kcol, int K, int pitch,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
                                                 const float *__restrict__ lmaxb, size_t mstride, int nblk,
                                                 __half *__restrict__ outb, size_t ostride,
@@ -145,30 +135,30 @@ __global__ void __launch_bounds__(256) k_pack_l(int N, int r0, int r1, int kcol,
         split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
     }
     __syncthreads();
-    store_chunk(t, outb + ostride * f + (size_t)(tile * nchunk + chunk) * CHUNK_HALVES);
+    store_planes(t, outb + ostride * f + ((size_t)chunk * 4 * pitch + (size_t)tile * TR) * KC, pitch);
 }
 
-__global__ void __launch_bounds__(256) k_pack_u(int N, int c0, int c1, int krow, int K, int nchunk,
+__global__ void __launch_bounds__(256) k_pack_u(int N, int c0, int c1, int krow, int K, int pitch,
                                                 const float *__restrict__ planes, size_t pstride, int ld,
                                                 const float *__restrict__ umaxb, size_t mstride,
                                                 __half *__restrict__ outb, size_t ostride,
                                                 const int *__restrict__ active) {
     __shared__ __align__(1024) __half t[CHUNK_HALVES];
-    __shared__ float cscale[TH];
+    __shared__ float cscale[TR];
     const int f = blockIdx.z;
     if (!active[f]) return;
     const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     const int tile = blockIdx.x, chunk = blockIdx.y;
-    if (threadIdx.x < TH) {
-        const int col = c0 + tile * TH + threadIdx.x;
+    if (threadIdx.x < TR) {
+        const int col = c0 + tile * TR + threadIdx.x;
         cscale[threadIdx.x] =
             col < c1 ? pow2_scale(col_max(umaxb + mstride * f, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < SUB; e += 256) {
-        const int kq = e >> 7, n = e & (TH - 1);     // consecutive threads: consecutive columns
+        const int kq = e >> 7, n = e & (TR - 1);     // consecutive threads: consecutive columns
         const int k = chunk * KC + kq;
-        const int col = c0 + tile * TH + n;
+        const int col = c0 + tile * TR + n;
         float vr = 0.f, vi = 0.f;
         if (col < c1 && k < K) {
             const size_t o = (size_t)(krow + k) * ld + col;
@@ -180,7 +170,7 @@ __global__ void __launch_bounds__(256) k_pack_u(int N, int c0, int c1, int krow,
         split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
     }
     __syncthreads();
-    store_chunk(t, outb + ostride * f + (size_t)(tile * nchunk + chunk) * CHUNK_HALVES);
+    store_planes(t, outb + ostride * f + ((size_t)chunk * 4 * pitch + (size_t)tile * TR) * KC, pitch);
 }
 
 // ---------------------------------------------------------------------------
@@ -316,8 +306,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 // clusters of two CTAs along x, 256 threads.
 // ---------------------------------------------------------------------------
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
-    k_update_tc(const __grid_constant__ CUtensorMap cmap, int N, int r0, int r1, int c0, int c1, int nchunk, const __half *__restrict__ Lpackb,
-                size_t lstride, const __half *__restrict__ Upackb, size_t ustride, const float *__restrict__ lmaxb,
+    k_update_tc(const __grid_constant__ CUtensorMap cmap, int N, int r0, int r1, int c0, int c1, int nchunk,
+                const __half *__restrict__ Lpackb, size_t lstride, int lpitch, int loff,
+                const __half *__restrict__ Upackb, size_t ustride, int upitch, int uoff, const float *__restrict__ lmaxb,
                 const float *__restrict__ umaxb, size_t mstride, int nblk, int kcol, int krow, int K,
                 float *__restrict__ planes, size_t pstride, int ld, char *__restrict__ ctl,
                 const int *__restrict__ active) {
@@ -359,14 +350,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
 
     if (tid == 0) {
         bool ok = true;
-        const __half *gl = Lpack + (size_t)rtile * nchunk * CHUNK_HALVES;
-        const __half *gu = Upack + (size_t)utile * nchunk * CHUNK_HALVES;
-        constexpr uint32_t cbytes = sizeof(__half) * CHUNK_HALVES;
+        // this CTA's 128 rows of each component plane of L (columns of U)
+        const __half *gl = Lpack + (size_t)(loff + rtile * TR) * KC;
+        const __half *gu = Upack + (size_t)(uoff + utile * TR) * KC;
+        constexpr uint32_t sbytes = sizeof(__half) * SUB;
         auto load = [&](int c) {
             __half *st = stage + (c % NSTAGE) * STAGE_HALVES;
-            mbar_expect_tx(&full[c % NSTAGE], 2 * cbytes);
-            bulk_g2s(st, gl + (size_t)c * CHUNK_HALVES, cbytes, &full[c % NSTAGE]);
-            bulk_g2s(st + CHUNK_HALVES, gu + (size_t)c * CHUNK_HALVES, cbytes, &full[c % NSTAGE]);
+            mbar_expect_tx(&full[c % NSTAGE], 8 * sbytes);
+            for (int comp = 0; comp < 4; comp++) {
+                bulk_g2s(st + comp * SUB, gl + (size_t)(c * 4 + comp) * lpitch * KC, sbytes, &full[c % NSTAGE]);
+                bulk_g2s(st + CHUNK_HALVES + comp * SUB, gu + (size_t)(c * 4 + comp) * upitch * KC, sbytes,
+                         &full[c % NSTAGE]);
+            }
         };
         for (int c = 0; c < NSTAGE && c < nchunk; c++) load(c);
         if (leader) {
@@ -523,12 +518,6 @@ efie_status efie_tc_attrs() {
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
 
 namespace {
-// packed K chunks of one frequency slot for the largest update of an N x N
-// LU: 2 ceil(N / 256) tiles of 128 rows (columns), up to 8 chunks each
-size_t pack_stride(int N) { return (size_t)2 * ((N + TN - 1) / TN) * NCHUNK_MAX * CHUNK_HALVES; }
-}  // namespace
-
-namespace {
 // the planes of every frequency slot as one float tensor [B][2][N][ld]
 // (innermost first: column, row, plane, slot), 32 x 32 boxes, 128B swizzle
 efie_status encode_planes_map(SolveWork &w) {
@@ -552,61 +541,102 @@ efie_status encode_planes_map(SolveWork &w) {
     if (r != CUDA_SUCCESS) return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the LU planes");
     return EFIE_OK;
 }
+
+// halves per frequency slot of a packed panel with `nchunk` K chunks
+size_t pack_stride(const SolveWork &w, int nchunk) { return (size_t)nchunk * 4 * w.ppitch * KC; }
 }  // namespace
 
-// Staging for the largest update of an N x N LU (per frequency slot), the
+// Staging for the packed panels of an N x N LU (per frequency slot), the
 // planes' tensor map and the kernel attributes: done when the workspace is
 // created (after the planes), so that the factor sequence allocates nothing
-// and can be captured into a CUDA graph.
+// and can be captured into a CUDA graph.  A panel's pitch leaves room for the
+// 256 rows a CTA pair may read past the last row of a view.
 efie_status efie_gemm_workspace(SolveWork &w) {
     EFIE_TRY(efie_tc_attrs());
     EFIE_TRY(encode_planes_map(w));
-    const size_t bytes = sizeof(__half) * pack_stride(w.N) * w.B;
-    EFIE_TRY(w.packA.reserve(bytes));
-    EFIE_TRY(w.packB.reserve(bytes));
-    EFIE_TRY(w.packA2.reserve(bytes));
-    EFIE_TRY(w.packB2.reserve(bytes));
+    w.ppitch = (w.N + 256 + TR - 1) / TR * TR;
+    const size_t outer = sizeof(__half) * pack_stride(w, NCHUNK_MAX) * w.B;
+    const size_t inpanel = sizeof(__half) * pack_stride(w, 64 / KC) * w.B;
+    for (int i = 0; i < 2; i++) {
+        EFIE_TRY(w.packL[i].reserve(outer));
+        EFIE_TRY(w.packU[i].reserve(outer));
+    }
+    EFIE_TRY(w.ipL.reserve(inpanel));
+    EFIE_TRY(w.ipU.reserve(inpanel));
     return EFIE_OK;
 }
 
+PackView efie_inpanel_view(const SolveWork &w, bool lower) {
+    PackView v;
+    v.base = (lower ? w.ipL : w.ipU).p;
+    v.stride = pack_stride(w, 64 / KC);
+    v.pitch = w.ppitch;
+    return v;
+}
+
+efie_status efie_pack_l(efie_ctx *ctx, SolveWork &w, DevBuf &buf, int r0, int r1, int kcol, int K, PackView *out) {
+    if (K <= 0 || K > KMAX || r1 <= r0) return efie_fail(EFIE_ERR_ARGS, "efie_pack_l: bad block");
+    const int nchunk = (K + KC - 1) / KC;
+    const size_t stride = pack_stride(w, nchunk);
+    if (buf.bytes < sizeof(__half) * stride * w.B) return efie_fail(EFIE_ERR_ARGS, "efie_pack_l: staging too small");
+    cudaStream_t st = ctx->stream;
+    size_t tok = ctx->log.begin(st);
+    k_pack_l<<<dim3((r1 - r0 + TR - 1) / TR, nchunk, w.B), 256, 0, st>>>(
+        w.N, r0, r1, kcol, K, w.ppitch, w.planes.as<float>(), w.pstride, w.ld, w.lmax.as<float>(), w.mstride, w.nblk,
+        buf.as<__half>(), stride, w.active.as<int>());
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_PANEL, st, tok, 0.0, 1);
+    *out = PackView{buf.p, stride, w.ppitch, 0};
+    return EFIE_OK;
+}
+
+efie_status efie_pack_u(efie_ctx *ctx, SolveWork &w, DevBuf &buf, int c0, int c1, int krow, int K, PackView *out) {
+    if (K <= 0 || K > KMAX || c1 <= c0) return efie_fail(EFIE_ERR_ARGS, "efie_pack_u: bad block");
+    const int nchunk = (K + KC - 1) / KC;
+    const size_t stride = pack_stride(w, nchunk);
+    if (buf.bytes < sizeof(__half) * stride * w.B) return efie_fail(EFIE_ERR_ARGS, "efie_pack_u: staging too small");
+    cudaStream_t st = ctx->stream;
+    size_t tok = ctx->log.begin(st);
+    k_pack_u<<<dim3((c1 - c0 + TR - 1) / TR, nchunk, w.B), 256, 0, st>>>(
+        w.N, c0, c1, krow, K, w.ppitch, w.planes.as<float>(), w.pstride, w.ld, w.umax.as<float>(), w.mstride,
+        buf.as<__half>(), stride, w.active.as<int>());
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_PANEL, st, tok, 0.0, 1);
+    *out = PackView{buf.p, stride, w.ppitch, 0};
+    return EFIE_OK;
+}
+
+bool efie_gemm_uses_tc(int rows, int cols, int K) {
+    return !g_tc_disabled && K > 0 && K <= KMAX && rows >= 64 && cols >= 64;
+}
+
 // C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] for every
-// active frequency: tensor cores when the block spans enough work, CUDA cores
-// otherwise.
+// active frequency: tensor cores from the packed views when the block spans
+// enough work, CUDA cores from the factors otherwise.
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact, int slot) {
+                             int nact, const PackView &Lv, const PackView &Uv) {
     const int rows = r1 - r0, cols = c1 - c0;
     if (rows <= 0 || cols <= 0 || K <= 0) return EFIE_OK;
-    const bool tc = !g_tc_disabled && K <= KMAX && (double)rows * cols >= 64.0 * 256.0 && cols >= 96;
-    if (!tc) {
+    if (!efie_gemm_uses_tc(rows, cols, K)) {
         for (int k0 = 0; k0 < K; k0 += 64)
             EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
         return EFIE_OK;
     }
+    if (!Lv.base || !Uv.base || (Lv.off & 7) || (Uv.off & 7) ||
+        Lv.off + (rows + TN - 1) / TN * TN > Lv.pitch || Uv.off + (cols + TN - 1) / TN * TN > Uv.pitch)
+        return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: packed operands do not cover the block");
     EFIE_TRY(efie_tc_attrs());
     const int N = w.N, B = w.B;
     cudaStream_t st = ctx->stream;
     const int npr = (rows + TN - 1) / TN, nct = (cols + TN - 1) / TN;   // 256-row pairs, 256-column tiles
     const int nchunk = (K + KC - 1) / KC;
-    const size_t stride = pack_stride(N);
-    DevBuf &pL = slot ? w.packA2 : w.packA, &pU = slot ? w.packB2 : w.packB;
-    EFIE_TRY(pL.reserve(sizeof(__half) * stride * B));
-    EFIE_TRY(pU.reserve(sizeof(__half) * stride * B));
-    float *planes = w.planes.as<float>();
-    const int *active = w.active.as<int>();
-    const float *lmax = w.lmax.as<float>(), *umax = w.umax.as<float>();
-    KernelLog &log = ctx->log;
-    size_t tok = log.begin(st);
-    k_pack_l<<<dim3(2 * npr, nchunk, B), 256, 0, st>>>(N, r0, r1, kcol, K, nchunk, planes, w.pstride, w.ld, lmax,
-                                                       w.mstride, w.nblk, pL.as<__half>(), stride, active);
-    k_pack_u<<<dim3(2 * nct, nchunk, B), 256, 0, st>>>(N, c0, c1, krow, K, nchunk, planes, w.pstride, w.ld, umax,
-                                                       w.mstride, pU.as<__half>(), stride, active);
-    EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, st, tok, 0.0, 2);
-    tok = log.begin(st);
+    size_t tok = ctx->log.begin(st);
     k_update_tc<<<dim3(2 * nct, npr, B), 256, GEMM_SMEM, st>>>(
-        *reinterpret_cast<const CUtensorMap *>(w.planes_map), N, r0, r1, c0, c1, nchunk, pL.as<__half>(), stride, pU.as<__half>(), stride, lmax, umax, w.mstride, w.nblk,
-        kcol, krow, K, planes, w.pstride, w.ld, w.ctl.as<char>(), active);
+        *reinterpret_cast<const CUtensorMap *>(w.planes_map), N, r0, r1, c0, c1, nchunk,
+        static_cast<const __half *>(Lv.base), Lv.stride, Lv.pitch, Lv.off, static_cast<const __half *>(Uv.base),
+        Uv.stride, Uv.pitch, Uv.off, w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K,
+        w.planes.as<float>(), w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
+    ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
     return EFIE_OK;
 }

@@ -21,6 +21,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "efie_internal.h"
 #include "solve.h"
 
@@ -61,192 +63,221 @@ __global__ void __launch_bounds__(256) k_z_to_planes(int N, const double2 *__res
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block bi of every frequency (blockIdx.x = f): unblocked LU without
-// pivoting of A[k:k+kb, k:k+kb] and the inverses of its unit-lower L and upper
-// U factors (kept for the panel products and the triangular solves).
-//
-// 512 threads; thread t owns row r = t / 8 and columns 8 (t mod 8) ... + 7 of
-// the block in registers (the 8 threads of a row share a warp).  Step j
-// reads the pivot row and the pivot column from shared memory; while
-// updating, the threads that hold row j + 1 and column j + 1 store them
-// (double-buffered), so a step is one barrier and one reciprocal.  Only the
-// column group that contains the pivot column needs per-column predicates.
-// The inverses follow in one 64-step sweep with the factors staged in shared
-// memory: forward substitution for L^-1 (X = I; X[r] -= l_rj X[j], r > j)
-// and backward substitution for U^-1 (Y = I; Y[j] *= 1/u_jj, then
-// Y[r] -= u_rj Y[j], r < j).  Row buffers carry one pad entry per 8 columns
-// so that the 8 column groups of a warp hit distinct banks.
+// Diagonal block bi of every frequency (blockIdx.x = f): LU without pivoting
+// of A[k:k+kb, k:k+kb] (identity beyond kb) and the inverses of its unit-lower
+// L and upper U factors (kept for the panel products and the triangular
+// solves), blocked by 16 in shared memory.  For each 16-column panel one warp
+// factors it in registers (lane l holds rows o + l and o + 32 + l; the pivot
+// row is broadcast by shuffles, so its 16 steps need no barrier), then the
+// 16-row U strip (forward substitution, one thread per column) and the
+// trailing block (one rank-16 update) follow, one barrier each.  The inverses
+// are built the same way: the four 16 x 16 diagonal blocks of L^-1 and U^-1
+// by substitution (one warp per block, one lane per column), then the
+// off-diagonal blocks block row by block row,
+//     X_ij = -X_ii sum_{j<=m<i} L_im X_mj     (L^-1, i > j, downwards)
+//     Y_ij = -Y_ii sum_{i<m<=j} U_im Y_mj     (U^-1, i < j, upwards),
+// block row r of L^-1 with block row 3 - r of U^-1: 20 barriers in all.
 // ---------------------------------------------------------------------------
-constexpr int DG = 8;                                        // columns per thread
-__device__ __forceinline__ int padc(int c) { return c + (c >> 3); }
+constexpr int SB = 16;   // sub-block of the diagonal factorisation
+constexpr size_t kDiagSmem = sizeof(float2) * (3 * NB * (NB + 1) + 2 * 3 * SB * (SB + 1));
 
 __device__ __forceinline__ void cfms(float2 &acc, float2 l, float2 u) {   // acc -= l * u
     acc.x -= l.x * u.x - l.y * u.y;
     acc.y -= l.x * u.y + l.y * u.x;
 }
 
-__global__ void __launch_bounds__(512) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
+__device__ __forceinline__ void cfma(float2 &acc, float2 l, float2 u) {   // acc += l * u
+    acc.x += l.x * u.x - l.y * u.y;
+    acc.y += l.x * u.y + l.y * u.x;
+}
+
+__device__ __forceinline__ float2 shfl2(float2 v, int src) {
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// 1 / p for complex p; `zero` when |p|^2 is not positive
+__device__ __forceinline__ float2 crecip(float2 p, bool &zero) {
+    const float den = p.x * p.x + p.y * p.y;
+    zero = !(den > 0.f);
+    const float rd = 1.0f / den;
+    return make_float2(p.x * rd, -p.y * rd);
+}
+
+__global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
                                                      size_t pstride, int ld, float2 *__restrict__ dinv,
                                                      size_t dstride, char *__restrict__ ctl,
                                                      const int *__restrict__ active) {
     const int f = blockIdx.x;
     if (!active[f]) return;
-    __shared__ float2 prow[2][72];
-    __shared__ float2 colb[2][NB];
-    __shared__ float2 LU[NB][NB + 1];
-    __shared__ float2 rdiag[NB];
-    __shared__ float2 xrow[2][72];
-    __shared__ float2 yrow[2][72];
+    extern __shared__ float2 dsm[];
+    float2(*A)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dsm);   // the block, then L\U
+    float2(*X)[NB + 1] = A + NB;                                        // L^-1
+    float2(*Y)[NB + 1] = A + 2 * NB;                                    // U^-1
+    float2(*TX)[SB][SB + 1] = reinterpret_cast<float2(*)[SB][SB + 1]>(dsm + 3 * NB * (NB + 1));
+    float2(*TY)[SB][SB + 1] = TX + 3;   // partial sums of the off-diagonal inverse blocks
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
     int *err = reinterpret_cast<int *>(ctl + 64 * f + 36);
-    const int t = threadIdx.x, r = t >> 3, c0 = (t & 7) * DG;
-    float2 a[DG];
-    if (r < kb) {
-        // 8 consecutive floats of each plane: 32-byte aligned (ld, k, c0 are multiples of 8)
-        const float4 *pr = reinterpret_cast<const float4 *>(Ar + (size_t)(k + r) * ld + k + c0);
-        const float4 *pi = reinterpret_cast<const float4 *>(Ai + (size_t)(k + r) * ld + k + c0);
-#pragma unroll
-        for (int v = 0; v < 2; v++) {
-            const float4 re = pr[v], im = pi[v];
-            a[4 * v + 0] = make_float2(re.x, im.x);
-            a[4 * v + 1] = make_float2(re.y, im.y);
-            a[4 * v + 2] = make_float2(re.z, im.z);
-            a[4 * v + 3] = make_float2(re.w, im.w);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+
+    for (int e = t; e < NB * NB; e += 256) {
+        const int r = e >> 6, c = e & 63;
+        float2 v = make_float2(r == c ? 1.f : 0.f, 0.f);   // identity beyond kb
+        if (r < kb && c < kb) {
+            const size_t o = (size_t)(k + r) * ld + k + c;
+            v = make_float2(Ar[o], Ai[o]);
         }
-#pragma unroll
-        for (int c = 0; c < DG; c++)
-            if (c0 + c >= kb) a[c] = make_float2(0.f, 0.f);   // columns past the block: zero
-    } else {
-#pragma unroll
-        for (int c = 0; c < DG; c++) a[c] = make_float2(c0 + c == r ? 1.f : 0.f, 0.f);  // identity padding
+        A[r][c] = v;
+        X[r][c] = make_float2(0.f, 0.f);
+        Y[r][c] = make_float2(0.f, 0.f);
     }
+    __syncthreads();
+
     // ---- LU without pivoting ----
-    // a column group's 8 entries are contiguous in the padded row buffers
-    const int gofs = c0 + (c0 >> 3);
-    if (r == 0) {
+    bool bad = false;
+    for (int p = 0; p < NB / SB; p++) {
+        const int o = p * SB;
+        if (warp == 0) {
+            const int i0 = o + lane, i1 = o + 32 + lane;
+            const bool h0 = i0 < NB, h1 = i1 < NB;
+            float2 a0[SB], a1[SB];
 #pragma unroll
-        for (int c = 0; c < DG; c++) prow[0][gofs + c] = a[c];
-    }
-    if (c0 == 0) colb[0][r] = a[0];
-    __syncthreads();
-    for (int j = 0; j < NB; j++) {
-        const int buf = j & 1;
-        const float2 *pb = prow[buf] + gofs;
-        float2 *pn = prow[buf ^ 1] + gofs;
-        const float2 p = prow[buf][padc(j)];
-        const float den = p.x * p.x + p.y * p.y;
-        if (t == 0 && !(den > 0.f)) atomicExch(err, 1);
-        if (r > j && c0 + DG > j) {
-            const float rd = 1.0f / den;
-            const float2 l = cmulf(colb[buf][r], make_float2(p.x * rd, -p.y * rd));
-            if (c0 > j) {
+            for (int c = 0; c < SB; c++) {
+                a0[c] = h0 ? A[i0][o + c] : make_float2(0.f, 0.f);
+                a1[c] = h1 ? A[i1][o + c] : make_float2(0.f, 0.f);
+            }
 #pragma unroll
-                for (int c = 0; c < DG; c++) cfms(a[c], l, pb[c]);
-            } else {
-                const int jc = j - c0;   // 0..7: the pivot column inside this group
+            for (int j = 0; j < SB; j++) {
+                float2 u[SB];
 #pragma unroll
-                for (int c = 0; c < DG; c++) {
-                    if (c == jc) a[c] = l;   // L entry
-                    else if (c > jc) cfms(a[c], l, pb[c]);
+                for (int c = j; c < SB; c++) u[c] = shfl2(a0[c], j);   // row o + j sits in lane j
+                bool z;
+                const float2 inv = crecip(u[j], z);
+                bad |= z;
+                if (lane > j) {
+                    const float2 l = cmulf(a0[j], inv);
+                    a0[j] = l;
+#pragma unroll
+                    for (int c = j + 1; c < SB; c++) cfms(a0[c], l, u[c]);
                 }
-            }
-            if (r == j + 1) {
+                const float2 l = cmulf(a1[j], inv);
+                a1[j] = l;
 #pragma unroll
-                for (int c = 0; c < DG; c++) pn[c] = a[c];
+                for (int c = j + 1; c < SB; c++) cfms(a1[c], l, u[c]);
             }
-            const int nc = j + 1 - c0;   // next pivot column inside this group, if 0..7
-            if (nc >= 0 && nc < DG) {
 #pragma unroll
-                for (int c = 0; c < DG; c++)
-                    if (c == nc) colb[buf ^ 1][r] = a[c];
+            for (int c = 0; c < SB; c++) {
+                if (h0) A[i0][o + c] = a0[c];
+                if (h1) A[i1][o + c] = a1[c];
+            }
+        }
+        __syncthreads();
+        const int w = NB - o - SB;   // columns (rows) right of (below) the panel
+        if (t < w) {                 // U strip: forward substitution with the panel's unit-lower block
+            const int c = o + SB + t;
+            float2 x[SB];
+#pragma unroll
+            for (int i = 0; i < SB; i++) {
+                float2 v = A[o + i][c];
+#pragma unroll
+                for (int m = 0; m < i; m++) cfms(v, A[o + i][o + m], x[m]);
+                x[i] = v;
+                A[o + i][c] = v;
+            }
+        }
+        __syncthreads();
+        for (int e = t; e < w * w; e += 256) {   // trailing block: rank-16 update
+            const int i = o + SB + e / w, c = o + SB + e % w;
+            float2 v = A[i][c];
+#pragma unroll
+            for (int m = 0; m < SB; m++) cfms(v, A[i][o + m], A[o + m][c]);
+            A[i][c] = v;
+        }
+        __syncthreads();
+    }
+
+    // ---- inverses: diagonal 16 x 16 blocks ----
+    if (lane < SB) {
+        const int c = lane;
+        if (warp < 4) {   // L^-1: unit lower, forward substitution
+            const int o = warp * SB;
+            float2 x[SB];
+#pragma unroll
+            for (int i = 0; i < SB; i++) {
+                float2 v = make_float2(i == c ? 1.f : 0.f, 0.f);
+#pragma unroll
+                for (int m = 0; m < i; m++) cfms(v, A[o + i][o + m], x[m]);
+                x[i] = v;
+                X[o + i][o + c] = v;
+            }
+        } else {          // U^-1: upper, backward substitution
+            const int o = (warp - 4) * SB;
+            float2 y[SB];
+#pragma unroll
+            for (int i = SB - 1; i >= 0; i--) {
+                float2 v = make_float2(i == c ? 1.f : 0.f, 0.f);
+#pragma unroll
+                for (int m = i + 1; m < SB; m++) cfms(v, A[o + i][o + m], y[m]);
+                bool z;
+                v = cmulf(v, crecip(A[o + i][o + i], z));
+                y[i] = v;
+                Y[o + i][o + c] = v;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- inverses: off-diagonal blocks, L^-1 row R = r with U^-1 row Q = 3 - r ----
+    for (int r = 1; r < NB / SB; r++) {
+        const int R = r, Q = NB / SB - 1 - r, nx = r * SB * SB;
+        for (int e = t; e < 2 * nx; e += 256) {
+            const bool isx = e < nx;
+            const int e2 = isx ? e : e - nx;
+            const int jb = e2 >> 8, a = (e2 >> 4) & 15, b = e2 & 15;
+            float2 v = make_float2(0.f, 0.f);
+            if (isx) {   // -sum_{jb<=m<R} L_Rm X_m,jb
+                for (int m = jb; m < R; m++)
+#pragma unroll
+                    for (int q = 0; q < SB; q++) cfms(v, A[R * SB + a][m * SB + q], X[m * SB + q][jb * SB + b]);
+                TX[jb][a][b] = v;
+            } else {     // -sum_{Q<m<=j} U_Qm Y_mj, j = Q + 1 + jb
+                const int j = Q + 1 + jb;
+                for (int m = Q + 1; m <= j; m++)
+#pragma unroll
+                    for (int q = 0; q < SB; q++) cfms(v, A[Q * SB + a][m * SB + q], Y[m * SB + q][j * SB + b]);
+                TY[jb][a][b] = v;
+            }
+        }
+        __syncthreads();
+        for (int e = t; e < 2 * nx; e += 256) {
+            const bool isx = e < nx;
+            const int e2 = isx ? e : e - nx;
+            const int jb = e2 >> 8, a = (e2 >> 4) & 15, b = e2 & 15;
+            float2 v = make_float2(0.f, 0.f);
+            if (isx) {
+#pragma unroll
+                for (int q = 0; q < SB; q++) cfma(v, X[R * SB + a][R * SB + q], TX[jb][q][b]);
+                X[R * SB + a][jb * SB + b] = v;
+            } else {
+#pragma unroll
+                for (int q = 0; q < SB; q++) cfma(v, Y[Q * SB + a][Q * SB + q], TY[jb][q][b]);
+                Y[Q * SB + a][(Q + 1 + jb) * SB + b] = v;
             }
         }
         __syncthreads();
     }
-    // factors: back to the planes and into shared memory
-#pragma unroll
-    for (int c = 0; c < DG; c++) LU[r][c0 + c] = a[c];
-    if (r < kb) {
-        float4 *pr = reinterpret_cast<float4 *>(Ar + (size_t)(k + r) * ld + k + c0);
-        float4 *pi = reinterpret_cast<float4 *>(Ai + (size_t)(k + r) * ld + k + c0);
-        if (c0 + DG <= kb) {
-#pragma unroll
-            for (int v = 0; v < 2; v++) {
-                pr[v] = make_float4(a[4 * v].x, a[4 * v + 1].x, a[4 * v + 2].x, a[4 * v + 3].x);
-                pi[v] = make_float4(a[4 * v].y, a[4 * v + 1].y, a[4 * v + 2].y, a[4 * v + 3].y);
-            }
-        } else {
-            float *sr = Ar + (size_t)(k + r) * ld + k + c0, *si = Ai + (size_t)(k + r) * ld + k + c0;
-#pragma unroll
-            for (int c = 0; c < DG; c++)
-                if (c0 + c < kb) {
-                    sr[c] = a[c].x;
-                    si[c] = a[c].y;
-                }
+
+    // ---- factors back to the planes, inverses to their slots ----
+    for (int e = t; e < NB * NB; e += 256) {
+        const int r = e >> 6, c = e & 63;
+        if (r < kb && c < kb) {
+            const size_t o = (size_t)(k + r) * ld + k + c;
+            Ar[o] = A[r][c].x;
+            Ai[o] = A[r][c].y;
         }
+        Linv[e] = X[r][c];
+        Uinv[e] = Y[r][c];
     }
-    __syncthreads();
-    if (t < NB) {
-        const float2 u = LU[t][t];
-        const float rd = 1.0f / (u.x * u.x + u.y * u.y);
-        rdiag[t] = make_float2(u.x * rd, -u.y * rd);
-    }
-    // ---- L^-1 (forward) and U^-1 (backward) in one sweep ----
-    float2 x[DG], y[DG];
-#pragma unroll
-    for (int c = 0; c < DG; c++) {
-        x[c] = make_float2(c0 + c == r ? 1.f : 0.f, 0.f);
-        y[c] = x[c];
-    }
-    __syncthreads();
-    for (int s = 0; s < NB; s++) {
-        const int jl = s, ju = NB - 1 - s, buf = s & 1;
-        float2 *xb = xrow[buf] + gofs, *yb = yrow[buf] + gofs;
-        if (r == ju) {
-            const float2 dv = rdiag[ju];
-#pragma unroll
-            for (int c = 0; c < DG; c++) {
-                y[c] = cmulf(y[c], dv);
-                yb[c] = y[c];
-            }
-        }
-        if (r == jl) {
-#pragma unroll
-            for (int c = 0; c < DG; c++) xb[c] = x[c];
-        }
-        __syncthreads();
-        // row jl of L^-1 is zero right of the diagonal, row ju of U^-1 left of it
-        if (r > jl && c0 <= jl) {
-            const float2 lr = LU[r][jl];
-            const int lim = jl - c0;   // columns c <= lim of this group
-            if (lim >= DG - 1) {
-#pragma unroll
-                for (int c = 0; c < DG; c++) cfms(x[c], lr, xb[c]);
-            } else {
-#pragma unroll
-                for (int c = 0; c < DG; c++)
-                    if (c <= lim) cfms(x[c], lr, xb[c]);
-            }
-        }
-        if (r < ju && c0 + DG - 1 >= ju) {
-            const float2 ur = LU[r][ju];
-            const int lim = ju - c0;   // columns c >= lim of this group
-            if (lim <= 0) {
-#pragma unroll
-                for (int c = 0; c < DG; c++) cfms(y[c], ur, yb[c]);
-            } else {
-#pragma unroll
-                for (int c = 0; c < DG; c++)
-                    if (c >= lim) cfms(y[c], ur, yb[c]);
-            }
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < DG; c++) {
-        Linv[r * NB + c0 + c] = x[c];
-        Uinv[r * NB + c0 + c] = y[c];
-    }
+    if (t == 0 && bad) atomicExch(err, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -263,7 +294,9 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
                                                 size_t pstride, int ld, const float2 *__restrict__ dinv,
                                                 size_t dstride, const int *__restrict__ active,
                                                 float *__restrict__ lmax, float *__restrict__ umax,
-                                                size_t mstride, int nblk) {
+                                                size_t mstride, int nblk, __half *__restrict__ ipl,
+                                                __half *__restrict__ ipu, size_t ipstride, int ippitch,
+                                                int emit) {
     const int f = blockIdx.z;
     if (!active[f]) return;
     extern __shared__ float2 dyn[];
@@ -337,34 +370,72 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     // maxima of the finished factor block: per column of the U block (row panel)
     // or per row of the L block (column panel), over its 64 rows / columns
     __shared__ float red[NB][17];
+    __shared__ float mx[NB];
     __syncthreads();   // M and T are no longer read
+    float mag[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) {
             const int i = ty + 16 * a, j = tx + 16 * b;
-            const float v = (i < nrow && j < ncol) ? fmaxf(fabsf(acc[a][b].x), fabsf(acc[a][b].y)) : 0.f;
-            acc[a][b].x = v;
+            mag[a][b] = (i < nrow && j < ncol) ? fmaxf(fabsf(acc[a][b].x), fabsf(acc[a][b].y)) : 0.f;
         }
     if (rowp) {
 #pragma unroll
         for (int b = 0; b < 4; b++)
-            red[tx + 16 * b][ty] = fmaxf(fmaxf(acc[0][b].x, acc[1][b].x), fmaxf(acc[2][b].x, acc[3][b].x));
+            red[tx + 16 * b][ty] = fmaxf(fmaxf(mag[0][b], mag[1][b]), fmaxf(mag[2][b], mag[3][b]));
     } else {
 #pragma unroll
         for (int a = 0; a < 4; a++)
-            red[ty + 16 * a][tx] = fmaxf(fmaxf(acc[a][0].x, acc[a][1].x), fmaxf(acc[a][2].x, acc[a][3].x));
+            red[ty + 16 * a][tx] = fmaxf(fmaxf(mag[a][0], mag[a][1]), fmaxf(mag[a][2], mag[a][3]));
     }
     __syncthreads();
     if (tid < NB) {
         float m = 0.f;
 #pragma unroll
         for (int q = 0; q < 16; q++) m = fmaxf(m, red[tid][q]);
+        mx[tid] = m;
         if (rowp) {
             if (tid < ncol) umax[mstride * f + (size_t)bi * ld + off + tid] = m;
         } else {
             if (tid < nrow) lmax[mstride * f + (size_t)(off + tid) * nblk + bi] = m;
         }
+    }
+    if (!emit) return;
+    // the block as tensor-core operand of the panel chain's updates (K = 64):
+    // rows of L (columns of U) scaled by the power of two of their maximum,
+    // split into FP16 hi + lo, in the packed layout [chunk][re hi, re lo,
+    // im hi, im lo][row][32] with the 64-byte swizzle, staged in T's memory
+    __syncthreads();
+    __half *pk = reinterpret_cast<__half *>(&T[0][0]);   // 2 chunks x 4 components x 64 rows x 32: 32 KB
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = ty + 16 * a, j = tx + 16 * b;
+            const int prow = rowp ? j : i, kidx = rowp ? i : j;
+            const float sc = efie_pow2_scale(mx[prow]);
+            const int chunk = kidx >> 5, kq = kidx & 31;
+            const int o = chunk * 4 * NB * 32 + (int)(efie_swz64(prow, kq) >> 1);
+            __half h, l;
+            const float vr = acc[a][b].x * sc, vi = acc[a][b].y * sc;
+            h = __float2half_rn(vr);
+            l = __float2half_rn(vr - __half2float(h));
+            pk[o] = h;
+            pk[o + NB * 32] = l;
+            h = __float2half_rn(vi);
+            l = __float2half_rn(vi - __half2float(h));
+            pk[o + 2 * NB * 32] = h;
+            pk[o + 3 * NB * 32] = l;
+        }
+    __syncthreads();
+    // eight 64-row component blocks (4 KB each) to their planes, at the pack
+    // row of this tile (rows / columns from k + kb on)
+    __half *dst = (rowp ? ipu : ipl) + ipstride * f + (size_t)(off - k - kb) * 32;
+    for (int e = tid; e < 8 * NB * 32 / 8; e += 256) {
+        const int blk = e / (NB * 32 / 8), q = e % (NB * 32 / 8);
+        reinterpret_cast<float4 *>(dst + (size_t)blk * ippitch * 32)[q] =
+            reinterpret_cast<const float4 *>(pk + blk * NB * 32)[q];
     }
 }
 
@@ -629,6 +700,7 @@ efie_status set_smem_attrs() {
     static bool done = false;
     if (done) return EFIE_OK;
     EFIE_CUDA(cudaFuncSetAttribute(k_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
+    EFIE_CUDA(cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
     done = true;
     return EFIE_OK;
@@ -730,43 +802,55 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     EFIE_CUDA(cudaStreamWaitEvent(w.hi, w.ev_start, 0));
     const int KB = w.kb_outer;
     bool rest_pending = false;   // ev_rest holds the record of the previous D^rest
+    const PackView ipl = efie_inpanel_view(w, true), ipu = efie_inpanel_view(w, false);
     {
         OnStream on(ctx, w.hi);
         cudaStream_t s = w.hi;
-        for (int K0 = 0; K0 < N; K0 += KB) {
+        for (int K0 = 0, P = 0; K0 < N; K0 += KB, P++) {
             const int Kend = std::min(N, K0 + KB), K1 = std::min(N, Kend + KB);
-            // F_P: the panel chain
+            // F_P: the panel chain; the panel kernel packs each 64-wide block
+            // for the chain's two updates (K = 64)
             for (int k = K0; k < Kend; k += NB) {
                 const int bi = k / NB, kb = std::min(NB, N - k);
                 const int s1 = k + kb, rest = N - s1;
+                const bool inpanel = s1 < Kend;
                 tok = log.begin(s);
-                k_diag_factor<<<B, 512, 0, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
+                k_diag_factor<<<B, 256, kDiagSmem, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
                 if (rest > 0) {
                     dim3 pg((rest + NB - 1) / NB, 2, B);
                     k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
                                                         active, w.lmax.as<float>(), w.umax.as<float>(), w.mstride,
-                                                        w.nblk);
+                                                        w.nblk, w.ipL.as<__half>(), w.ipU.as<__half>(), ipl.stride,
+                                                        ipl.pitch, inpanel ? 1 : 0);
                 }
                 EFIE_CUDA(cudaGetLastError());
                 log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
-                if (s1 < Kend) {
+                if (inpanel) {
                     // rows of this panel below the block, every column to the right
-                    EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact));
+                    EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact, ipl, ipu));
                     // rows below the panel, the panel's remaining columns
-                    EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, s1, Kend, k, k, kb, nact));
+                    EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, s1, Kend, k, k, kb, nact, ipl.at(Kend - s1), ipu));
                 }
             }
             if (Kend >= N) break;
+            // L and U of the panel packed once (staging of this panel's parity)
+            // for D_P^next and D_P^rest; D_P^rest finishes before panel P + 2's
+            // packs, which follow D_{P+1}^next on this stream
+            const int K = Kend - K0;
+            PackView Lp, Up;
+            EFIE_TRY(efie_pack_l(ctx, w, w.packL[P & 1], Kend, N, K0, K, &Lp));
+            EFIE_TRY(efie_pack_u(ctx, w, w.packU[P & 1], Kend, N, K0, K, &Up));
             EFIE_CUDA(cudaEventRecord(w.ev_panel, s));
             // D_P^next on the critical stream, after D_{P-1}^rest
             if (rest_pending) EFIE_CUDA(cudaStreamWaitEvent(s, w.ev_rest, 0));
-            EFIE_TRY(efie_gemm_update(ctx, w, Kend, K1, Kend, N, K0, K0, Kend - K0, nact));
-            EFIE_TRY(efie_gemm_update(ctx, w, K1, N, Kend, K1, K0, K0, Kend - K0, nact));
-            // D_P^rest on the low-priority stream, after F_P
+            EFIE_TRY(efie_gemm_update(ctx, w, Kend, K1, Kend, N, K0, K0, K, nact, Lp, Up));
+            EFIE_TRY(efie_gemm_update(ctx, w, K1, N, Kend, K1, K0, K0, K, nact, Lp.at(K1 - Kend), Up));
+            // D_P^rest on the low-priority stream, after F_P and the packs
             if (K1 < N) {
                 OnStream on_lo(ctx, w.lo);
                 EFIE_CUDA(cudaStreamWaitEvent(w.lo, w.ev_panel, 0));
-                EFIE_TRY(efie_gemm_update(ctx, w, K1, N, K1, N, K0, K0, Kend - K0, nact, 1));
+                EFIE_TRY(efie_gemm_update(ctx, w, K1, N, K1, N, K0, K0, K, nact, Lp.at(K1 - Kend),
+                                          Up.at(K1 - Kend)));
                 EFIE_CUDA(cudaEventRecord(w.ev_rest, w.lo));
                 rest_pending = true;
             }

@@ -1,9 +1,27 @@
 // Mixed-precision solver, batched over frequencies (solve.cu, trsv.cu, gemm_tc.cu).
 #pragma once
 
+#include <cstdint>
+
 #include "efie_internal.h"
 
 constexpr int EFIE_MAX_BATCH = 16;
+
+// Byte offset of element (row r, k) inside a K-major 64B-swizzled FP16 tile
+// (the tensor-core operand layout): 16-byte chunk (k / 8) XOR (r / 2) mod 4,
+// 8-row atoms of 512 bytes.
+__host__ __device__ __forceinline__ uint32_t efie_swz64(uint32_t r, uint32_t k) {
+    return r * 64u + ((((k >> 3) ^ (r >> 1)) & 3u) << 4) + ((k & 7u) << 1);
+}
+
+// The split's exact scale 2^-e of a row (column) with largest magnitude mx:
+// mx * 2^-e in [1/2, 1); 1 for a zero maximum.
+__device__ __forceinline__ float efie_pow2_scale(float mx) {
+    if (!(mx > 0.f)) return 1.f;
+    int e;
+    frexpf(mx, &e);
+    return ldexpf(1.f, -e);
+}
 
 struct SolveWork {
     int N = 0, ld = 0, nblk = 0;
@@ -21,7 +39,11 @@ struct SolveWork {
     DevBuf ctl;      // per f 64 bytes: red[3] @0, counter @24, conv @28, skip @32, err @36
     DevBuf rpart;    // residual-norm partial sums: double [B][ceil(N/32)]
     DevBuf active;   // int[B]: slot holds a frequency of this batch
-    DevBuf packA, packB;  // tensor-core operand staging (FP16 hi/lo tiles)
+    // tensor-core operands, FP16 hi/lo packed once per panel (see PackView):
+    // the outer panel's L and U by parity of the panel (packL[2], packU[2]),
+    // the 64-wide block of the panel chain written by the panel kernel (ipL, ipU)
+    DevBuf packL[2], packU[2], ipL, ipU;
+    int ppitch = 0;       // packed rows (columns) per component plane
     // flexible GMRES (gmres.cu): Krylov basis V [M+1][B][N] and preconditioned
     // vectors Zm [M][B][N] in complex128, the new vector w [B][N], partial
     // sums and per-frequency Arnoldi state
@@ -32,11 +54,9 @@ struct SolveWork {
     bool zsym = false;
     DevBuf spart;
     // look-ahead LU: the panel chain runs on `hi` (highest priority) while the
-    // bulk of each deferred trailing update runs on `lo`, with its own operand
-    // staging (packA2/packB2)
+    // bulk of each deferred trailing update runs on `lo`
     cudaStream_t hi = nullptr, lo = nullptr;
     cudaEvent_t ev_start = nullptr, ev_panel = nullptr, ev_rest = nullptr, ev_hi = nullptr;
-    DevBuf packA2, packB2;
     // max |Re|, |Im| of every row of each 64-column block of L (lmax[f][row][blk])
     // and of every column of each 64-row block of U (umax[f][blk][col]), written
     // with the factors; they give the split's power-of-two scales
@@ -99,11 +119,35 @@ efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const d
 efie_status efie_trsv_workspace(SolveWork &w);
 efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int epoch);
 
+// A view of packed tensor-core operands.  A panel of L (rows) or U (columns)
+// is packed as half [B][nchunk][4][pitch][32]: per K chunk of 32 the
+// components re hi, re lo, im hi, im lo (x = hi + lo after an exact
+// power-of-two scaling of the row of L / column of U), each a plane of
+// `pitch` rows of 32 K values in the 64-byte swizzle of the MMA operands, so
+// that any 128 rows starting at a multiple of 8 are one contiguous 8 KB
+// block.  The view's row 0 is row `off` of the packed panel.
+struct PackView {
+    const void *base = nullptr;   // __half, slot 0
+    size_t stride = 0;            // halves per frequency slot
+    int pitch = 0;
+    int off = 0;
+    PackView at(int o) const { PackView v = *this; v.off = off + o; return v; }
+};
+// Pack rows [r0, r1) of L over columns [kcol, kcol + K) (U: columns [c0, c1)
+// over rows [krow, krow + K)) into `buf`; the view starts at r0 (c0).
+efie_status efie_pack_l(efie_ctx *ctx, SolveWork &w, DevBuf &buf, int r0, int r1, int kcol, int K, PackView *out);
+efie_status efie_pack_u(efie_ctx *ctx, SolveWork &w, DevBuf &buf, int c0, int c1, int krow, int K, PackView *out);
+// The views of the 64-wide block packed by the panel kernel (rows / columns
+// from s1 = k + 64 on).
+PackView efie_inpanel_view(const SolveWork &w, bool lower);
 // C[r0:r1, c0:c1] -= L[r0:r1, kcol:kcol+K] * U[krow:krow+K, c0:c1] for every
-// active frequency: tensor cores when the block is large enough (K <= 256),
-// CUDA cores otherwise (efie_update_simt, K <= 64 per call).
+// active frequency: on the tensor cores from the packed views Lv (rows r0..)
+// and Uv (columns c0..) when the block is large enough (K <= 256), else on
+// CUDA cores from the factors (efie_update_simt, K <= 64 per call).
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact, int slot = 0);
+                             int nact, const PackView &Lv, const PackView &Uv);
+// whether efie_gemm_update takes the tensor-core path for this block
+bool efie_gemm_uses_tc(int rows, int cols, int K);
 efie_status efie_update_simt(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
                              int nact);
 extern "C" void efie_debug_disable_tensor_cores(int disable);
