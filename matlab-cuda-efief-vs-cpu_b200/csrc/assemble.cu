@@ -42,18 +42,52 @@ __device__ __forceinline__ size_t pair_slot(int t1, int t2, int Nt, bool sym) {
     return (size_t)hi * (size_t)(hi + 1) / 2 + (size_t)lo;
 }
 
-// Triangle-pair moments, component-major: component c (S0, S1x, S1y, S1z, S2x,
-// S2y, S2z, S3; complex) of pair slot q at p[c * stride + q].  Consecutive
-// threads handle consecutive slots, so every store and every gather load is
-// a coalesced run of 16-byte values.
+// Triangle-pair moments of the pair (t1, t2), t1 the triangle of rho and t2
+// that of rho': S0 = int G, S1 = int G rho, S2 = int G rho', S3 = int G
+// rho.rho' (complex; rho, rho' relative to each triangle's origin), stored
+// component-major at p[c * stride + q] for pair slot q, so consecutive
+// threads (consecutive slots) store and load coalesced runs of 16 bytes.
+//
+// Edge-combination form (tri_d set): an RWG side on triangle t contributes
+// c (rho - d) with d one of at most three free-vertex vectors of t (its slot
+// l), so the pair's whole contribution to an entry is c_m c_n Q[l1][l2] with
+//     Q[l1][l2] = alpha (S3 - d2.S1 - d1.S2 + (d1.d2) S0) + beta 4 S0,
+// nine complex values per pair, p[(3 l1 + l2) * stride + q]: the gather then
+// reads one value per triangle pair instead of eight.  Otherwise the eight
+// moments themselves (c = S0, S1x, S1y, S1z, S2x, S2y, S2z, S3).
 struct MomStore {
     double2 *p;
     size_t stride;
+    const double4 *tri_d;   // [Nt][3] free-vertex vectors per slot, or null
+    double alr, ali, ber, bei;
 };
 
-__device__ __forceinline__ void store_mom(MomStore M, size_t slot, const double *a) {
+__device__ __forceinline__ void store_mom(const MomStore &M, size_t slot, int t1, int t2, const double *a) {
+    if (!M.tri_d) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) M.p[(size_t)i * M.stride + slot] = make_double2(a[2 * i], a[2 * i + 1]);
+        for (int i = 0; i < 8; i++) M.p[(size_t)i * M.stride + slot] = make_double2(a[2 * i], a[2 * i + 1]);
+        return;
+    }
+    const double s0r = 4.0 * a[0], s0i = 4.0 * a[1];
+    const double bsr = M.ber * s0r - M.bei * s0i, bsi = M.ber * s0i + M.bei * s0r;   // beta 4 S0
+#pragma unroll
+    for (int l1 = 0; l1 < 3; l1++) {
+        const double4 d1 = M.tri_d[3 * (size_t)t1 + l1];
+        // S3 - d1.S2 and S1 - d1 S0
+        const double ar = a[14] - (d1.x * a[8] + d1.y * a[10] + d1.z * a[12]);
+        const double ai = a[15] - (d1.x * a[9] + d1.y * a[11] + d1.z * a[13]);
+        const double bxr = a[2] - d1.x * a[0], bxi = a[3] - d1.x * a[1];
+        const double byr = a[4] - d1.y * a[0], byi = a[5] - d1.y * a[1];
+        const double bzr = a[6] - d1.z * a[0], bzi = a[7] - d1.z * a[1];
+#pragma unroll
+        for (int l2 = 0; l2 < 3; l2++) {
+            const double4 d2 = M.tri_d[3 * (size_t)t2 + l2];
+            const double ivr = ar - (d2.x * bxr + d2.y * byr + d2.z * bzr);
+            const double ivi = ai - (d2.x * bxi + d2.y * byi + d2.z * bzi);
+            M.p[(size_t)(3 * l1 + l2) * M.stride + slot] =
+                make_double2((M.alr * ivr - M.ali * ivi) + bsr, (M.alr * ivi + M.ali * ivr) + bsi);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -123,7 +157,7 @@ __global__ void __launch_bounds__(256) k_regular_moments(
         m[14] += w * (pq.x * t1r[0] + pq.y * t1r[1] + pq.z * t1r[2]);
         m[15] += w * (pq.x * t1i[0] + pq.y * t1i[1] + pq.z * t1i[2]);
     }
-    store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
+    store_mom(mom, pair_slot(t1, t2, Nt, sym), t1, t2, m);
 }
 
 // Generic point count (any Nq a prepack may carry).
@@ -159,7 +193,7 @@ __global__ void __launch_bounds__(256) k_regular_moments_any(
             m[14] += gr * dd; m[15] += gi * dd;
         }
     }
-    store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
+    store_mom(mom, pair_slot(t1, t2, Nt, sym), t1, t2, m);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -218,7 +252,7 @@ __global__ void __launch_bounds__(256) k_near_moments(
     }
 #pragma unroll
     for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
-    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, sym), m);
+    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, sym), t1, t2, m);
 }
 
 // ---------------------------------------------------------------------------
@@ -255,7 +289,7 @@ __global__ void __launch_bounds__(256) k_self_moments(
     }
 #pragma unroll
     for (int i = 0; i < 16; i++) m[i] = warp_sum(m[i]);
-    if (lane == 0) store_mom(mom, pair_slot(t, t, Nt, sym), m);
+    if (lane == 0) store_mom(mom, pair_slot(t, t, Nt, sym), t, t, m);
 }
 
 // ---------------------------------------------------------------------------
@@ -379,7 +413,7 @@ __global__ void __launch_bounds__(256) k_singular_moments(
             m[i + 6] = s;
         }
     }
-    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, true), m);
+    if (lane == 0) store_mom(mom, pair_slot(t1, t2, Nt, true), t1, t2, m);
 }
 
 // ---------------------------------------------------------------------------
@@ -425,22 +459,64 @@ __device__ __forceinline__ double2 z_entry(int m, int n, int Ne, int Nt, bool sy
     return make_double2(zr, zi);
 }
 
+// The same sum from the edge-combination form: etl[side][e] = 4 t + slot of
+// the RWG side (-1: none), ec[side][e] its coefficient c.
+__device__ __forceinline__ double2 z_entry_combo(int m, int n, int Ne, int Nt, bool sym, const int *__restrict__ etl,
+                                                 const double *__restrict__ ec, const MomStore mom) {
+    double zr = 0.0, zi = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+        const int tm = etl[a * Ne + m];
+        if (tm < 0) continue;
+        const double cm = ec[a * Ne + m];
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const int tn = etl[b * Ne + n];
+            if (tn < 0) continue;
+            const int t1 = tm >> 2, l1 = tm & 3, t2 = tn >> 2, l2 = tn & 3;
+            // stored for (t2, t1) when t1 > t2 in the symmetric regime: the
+            // integrand is symmetric, so the value sits at the swapped slots
+            const bool sw = sym && t1 > t2;
+            const int comp = sw ? 3 * l2 + l1 : 3 * l1 + l2;
+            const double2 q = __ldg(mom.p + (size_t)comp * mom.stride + pair_slot(t1, t2, Nt, sym));
+            const double cc = cm * ec[b * Ne + n];
+            zr += cc * q.x;
+            zi += cc * q.y;
+        }
+    }
+    return make_double2(zr, zi);
+}
+
+struct EdgeData {
+    const int *etri;      // triangle per RWG side (eight-moment form)
+    const double4 *ecd;   // free vertex - origin, c
+    const int *etl;       // 4 t + slot per RWG side (edge-combination form)
+    const double *ec;     // c per RWG side
+};
+
+template <bool COMBO>
+__device__ __forceinline__ double2 z_any(int m, int n, int Ne, int Nt, bool sym, const EdgeData &E,
+                                         const MomStore &mom) {
+    if (COMBO) return z_entry_combo(m, n, Ne, Nt, sym, E.etl, E.ec, mom);
+    return z_entry(m, n, Ne, Nt, sym, E.etri, E.ecd, mom, mom.alr, mom.ali, mom.ber, mom.bei);
+}
+
 // Thread per entry, m fastest (column-major Z, coalesced stores).
-__global__ void __launch_bounds__(256) k_gather_z(
-    int Ne, int Nt, bool sym, const int *__restrict__ etri, const double4 *__restrict__ ecd,
-    const MomStore mom, double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+template <bool COMBO>
+__global__ void __launch_bounds__(256) k_gather_z(int Ne, int Nt, bool sym, const EdgeData E, const MomStore mom,
+                                                  double2 *__restrict__ Z) {
     const int m = blockIdx.x * 64 + (threadIdx.x & 63);
     const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
     if (m >= Ne || n >= Ne) return;
-    Z[(size_t)m + (size_t)Ne * n] = z_entry(m, n, Ne, Nt, sym, etri, ecd, mom, alr, ali, ber, bei);
+    Z[(size_t)m + (size_t)Ne * n] = z_any<COMBO>(m, n, Ne, Nt, sym, E, mom);
 }
 
 // Symmetric Z (symmetric pair regimes): only 32x32 tiles with bm <= bn are
 // evaluated; an off-diagonal tile is also stored transposed through shared
 // memory, so Z(n,m) is a bit-exact copy of Z(m,n).
-__global__ void __launch_bounds__(256) k_gather_z_sym(
-    int Ne, int Nt, const int *__restrict__ etri, const double4 *__restrict__ ecd, const MomStore mom,
-    double alr, double ali, double ber, double bei, double2 *__restrict__ Z) {
+template <bool COMBO>
+__global__ void __launch_bounds__(256) k_gather_z_sym(int Ne, int Nt, const EdgeData E, const MomStore mom,
+                                                      double2 *__restrict__ Z) {
     const int bm = blockIdx.x, bn = blockIdx.y;
     if (bm > bn) return;
     __shared__ double2 tile[32][33];
@@ -450,7 +526,7 @@ __global__ void __launch_bounds__(256) k_gather_z_sym(
         const int n = bn * 32 + j;
         double2 z = make_double2(0.0, 0.0);
         if (m < Ne && n < Ne) {
-            z = z_entry(m, n, Ne, Nt, true, etri, ecd, mom, alr, ali, ber, bei);
+            z = z_any<COMBO>(m, n, Ne, Nt, true, E, mom);
             Z[(size_t)m + (size_t)Ne * n] = z;
         }
         tile[j][tx] = z;
@@ -583,6 +659,41 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     EFIE_TRY(up(g.origin, origin.data(), sizeof(double4) * Nt));
     EFIE_TRY(up(g.edge_tri, etri.data(), sizeof(int) * etri.size()));
     EFIE_TRY(up(g.edge_cd, ecd.data(), sizeof(double4) * ecd.size()));
+    // free-vertex slots of the edge-combination moments: the distinct vectors
+    // v - o of the RWG sides on each triangle (bitwise), at most three for a
+    // mesh whose RWG free vertices are vertices of their triangles; otherwise
+    // the eight-moment form is kept
+    {
+        std::vector<double4> trid(3 * (size_t)Nt, make_double4(0, 0, 0, 0));
+        std::vector<int> nslot(Nt, 0), etl(2 * (size_t)Ne, -1);
+        std::vector<double> ec(2 * (size_t)Ne, 0.0);
+        bool combo = true;
+        for (size_t i = 0; i < 2 * (size_t)Ne && combo; i++) {
+            const int t = etri[i];
+            if (t < 0) continue;
+            const double4 d = ecd[i];
+            int l = 0;
+            while (l < nslot[t] && !(trid[3 * (size_t)t + l].x == d.x && trid[3 * (size_t)t + l].y == d.y &&
+                                     trid[3 * (size_t)t + l].z == d.z))
+                l++;
+            if (l == nslot[t]) {
+                if (l == 3) {
+                    combo = false;
+                    break;
+                }
+                trid[3 * (size_t)t + l] = make_double4(d.x, d.y, d.z, 0.0);
+                nslot[t]++;
+            }
+            etl[i] = 4 * t + l;
+            ec[i] = d.w;
+        }
+        g.combo = combo;
+        if (combo) {
+            EFIE_TRY(up(g.tri_d, trid.data(), sizeof(double4) * trid.size()));
+            EFIE_TRY(up(g.edge_tl, etl.data(), sizeof(int) * etl.size()));
+            EFIE_TRY(up(g.edge_c, ec.data(), sizeof(double) * ec.size()));
+        }
+    }
 
     std::vector<uint8_t> mask((size_t)Nt * Nt, 0);
     if (scheme == EFIE_SCHEME_REF) {
@@ -690,7 +801,8 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     }
     EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
-    EFIE_TRY(g.moments.reserve(sizeof(double2) * 8 * g.npairs));   // 8 component planes of npairs
+    // component planes of npairs: 9 edge combinations or the 8 moments
+    EFIE_TRY(g.moments.reserve(sizeof(double2) * (g.combo ? 9 : 8) * g.npairs));
     return EFIE_OK;
 }
 
@@ -698,7 +810,8 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int Nt = g.Nt, Ne = g.Ne;
-    const MomStore mom{g.moments.as<double2>(), g.npairs};
+    const MomStore mom{g.moments.as<double2>(), g.npairs, g.combo ? g.tri_d.as<double4>() : nullptr,
+                       ph.alr, ph.ali, ph.ber, ph.bei};
     dim3 grid((Nt + 31) / 32, (Nt + 7) / 8);
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
@@ -747,14 +860,16 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     log.end(EFIE_K_NEARSELF, s, tok, qpe, nl);
     }
     tok = log.begin(s);
+    const EdgeData E{g.edge_tri.as<int>(), g.edge_cd.as<double4>(), g.edge_tl.as<int>(), g.edge_c.as<double>()};
+    double2 *Zd = static_cast<double2 *>(Z);
     if (g.symmetric) {
         dim3 gs((Ne + 31) / 32, (Ne + 31) / 32);
-        k_gather_z_sym<<<gs, 256, 0, s>>>(Ne, Nt, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr, ph.ali,
-                                          ph.ber, ph.bei, static_cast<double2 *>(Z));
+        if (g.combo) k_gather_z_sym<true><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd);
+        else k_gather_z_sym<false><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd);
     } else {
         dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
-        k_gather_z<<<gg, 256, 0, s>>>(Ne, Nt, false, g.edge_tri.as<int>(), g.edge_cd.as<double4>(), mom, ph.alr,
-                                      ph.ali, ph.ber, ph.bei, static_cast<double2 *>(Z));
+        if (g.combo) k_gather_z<true><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
+        else k_gather_z<false><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
     }
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_GATHER, s, tok, 16.0 * (double)Ne * Ne);

@@ -169,8 +169,12 @@ struct GeomDev {
     DevBuf tri_vtx;           // double4[3*Nt] vertices relative to origin (extraction scheme)
     DevBuf adj_list;          // int2[] vertex-adjacent pairs t1 < t2 (extraction scheme)
     int n_adj = 0;
-    DevBuf moments;           // double2[8][npairs]: component-major triangle-pair moments
+    DevBuf moments;           // double2[9 or 8][npairs]: component-major pair values (assemble.cu)
     size_t npairs = 0;
+    bool combo = false;       // edge-combination form (9 values per pair) in use
+    DevBuf tri_d;             // double4[3*Nt] free-vertex vectors per triangle slot
+    DevBuf edge_tl;           // int32[2*Ne] 4 t + slot per RWG side (-1 = none)
+    DevBuf edge_c;            // double[2*Ne] RWG coefficient c per side
 };
 
 // Per-frequency physics: k = w sqrt(mu eps) (principal branch), alpha = j w mu,

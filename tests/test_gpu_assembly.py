@@ -89,6 +89,28 @@ def test_asymmetric_near_matrix():
     assert _rel(Z, Zo) < TOL_Z
 
 
+def test_rwg_free_vertex_off_its_triangle():
+    """A copy of an RWG whose free vertex is moved by 1e-9 of the mesh size
+    leaves four distinct free vertices on a triangle: the assembly falls back
+    from the nine edge-combination values per triangle pair to the eight
+    moments, and stays exact against the oracle."""
+    p = eo.build_problem(small_design("grid"))
+    r = {k: np.array(v, copy=True) for k, v in p["rwg"].items()}
+    e = 5
+    for key in ("edge", "plusTri", "minusTri", "plusSign", "minusSign", "rp", "rm", "Ap", "Am", "len", "center",
+                "zSign"):
+        r[key] = np.asfortranarray(np.concatenate([r[key], r[key][e:e + 1]]))
+    r["rp"][-1] += 1e-9 * np.abs(p["V"]).max()
+    r["Ne"] = np.int64(r["Ne"] + 1)
+    p = dict(p, rwg=r)
+    d = p["design"]
+    omega, k, _, _ = eo.physics(2.3e9, d.mu, d.eps)
+    Z, _ = _gg(p, k, omega)
+    Zo = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
+    assert Z.shape == (r["Ne"], r["Ne"])
+    assert _rel(Z, Zo) < TOL_Z
+
+
 def test_gassemble_matches_oracle_and_reference():
     m = pkg()
     d = small_design("grid")
