@@ -17,7 +17,7 @@ import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned.json")
-BATCHES = (2, 4, 8)
+BATCHES = (4, 8, 16)
 PANELS = (64, 128, 256)
 
 
