@@ -160,6 +160,93 @@ __global__ void __launch_bounds__(256) k_regular_moments(
     store_mom(mom, pair_slot(t1, t2, Nt, sym), t1, t2, m);
 }
 
+// Several frequencies at once (F = 2..4, equally spaced: k_f = k0 + f dk).
+// Per point pair R, 1/(4 pi R) and the weights are shared, e^{-j k0 R} and
+// e^{-j dk R} take one sincos (and exp for lossy media) each, and every
+// further frequency costs one complex multiplication: e^{-j k_f R} =
+// e^{-j k0 R} (e^{-j dk R})^f.  The pair values go to each frequency's store.
+struct MomStores {
+    MomStore s[4];
+};
+
+template <int NQ, int F>
+__global__ void __launch_bounds__(256) k_regular_moments_mf(
+    int Nt, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
+    const uint8_t *__restrict__ skip, double kr0, double ki0, double dkr, double dki, MomStores ms) {
+    __shared__ double4 sp[8][NQ];
+    __shared__ double4 so[8];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int t1 = blockIdx.x * 32 + tx;
+    const int t2b = blockIdx.y * 8;
+    if (sym && blockIdx.x * 32 > t2b + 7) return;  // whole tile below the diagonal
+    for (int i = threadIdx.x; i < 8 * NQ; i += blockDim.x) {
+        int tt = t2b + i / NQ;
+        sp[i / NQ][i % NQ] = tt < Nt ? pts[(size_t)tt * NQ + i % NQ] : make_double4(0, 0, 0, 0);
+    }
+    if (threadIdx.x < 8) {
+        int tt = t2b + threadIdx.x;
+        so[threadIdx.x] = tt < Nt ? origin[tt] : make_double4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    const int t2 = t2b + ty;
+    if (t1 >= Nt || t2 >= Nt) return;
+    if (sym && t1 > t2) return;
+    if (skip[(size_t)t1 + (size_t)Nt * t2]) return;
+    double4 p1[NQ];
+#pragma unroll
+    for (int p = 0; p < NQ; p++) p1[p] = pts[(size_t)t1 * NQ + p];
+    const double4 o1 = origin[t1], o2 = so[ty];
+    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
+    double m[F][16];
+#pragma unroll
+    for (int f = 0; f < F; f++)
+#pragma unroll
+        for (int i = 0; i < 16; i++) m[f][i] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NQ; q++) {
+        const double4 pq = sp[ty][q];
+        const double ax = dox - pq.x, ay = doy - pq.y, az = doz - pq.z;
+#pragma unroll
+        for (int p = 0; p < NQ; p++) {
+            const double dx = ax + p1[p].x, dy = ay + p1[p].y, dz = az + p1[p].z;
+            double R = sqrt(dx * dx + dy * dy + dz * dz);
+            R = fmax(R, 1e-15);
+            double inv = p1[p].w * pq.w / (4.0 * kPi * R);
+            double s0, c0, ss, cs;
+            sincos(kr0 * R, &s0, &c0);
+            sincos(dkr * R, &ss, &cs);
+            if (ki0 != 0.0) inv *= exp(ki0 * R);
+            double esr = cs, esi = -ss;   // e^{-j dk R}
+            if (dki != 0.0) {
+                const double e = exp(dki * R);
+                esr *= e;
+                esi *= e;
+            }
+            double gr = c0 * inv, gi = -s0 * inv;
+            const double dd = p1[p].x * pq.x + p1[p].y * pq.y + p1[p].z * pq.z;
+#pragma unroll
+            for (int f = 0; f < F; f++) {
+                m[f][0] += gr; m[f][1] += gi;
+                m[f][2] += gr * p1[p].x; m[f][3] += gi * p1[p].x;
+                m[f][4] += gr * p1[p].y; m[f][5] += gi * p1[p].y;
+                m[f][6] += gr * p1[p].z; m[f][7] += gi * p1[p].z;
+                m[f][8] += gr * pq.x; m[f][9] += gi * pq.x;
+                m[f][10] += gr * pq.y; m[f][11] += gi * pq.y;
+                m[f][12] += gr * pq.z; m[f][13] += gi * pq.z;
+                m[f][14] += gr * dd; m[f][15] += gi * dd;
+                if (f + 1 < F) {
+                    const double nr = gr * esr - gi * esi;
+                    gi = gr * esi + gi * esr;
+                    gr = nr;
+                }
+            }
+        }
+    }
+    const size_t slot = pair_slot(t1, t2, Nt, sym);
+#pragma unroll
+    for (int f = 0; f < F; f++) store_mom(ms.s[f], slot, t1, t2, m[f]);
+}
+
 // Generic point count (any Nq a prepack may carry).
 __global__ void __launch_bounds__(256) k_regular_moments_any(
     int Nt, int Nq, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
@@ -801,24 +888,78 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     }
     EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
-    // component planes of npairs: 9 edge combinations or the 8 moments
-    EFIE_TRY(g.moments.reserve(sizeof(double2) * (g.combo ? 9 : 8) * g.npairs));
+    // component planes of npairs (9 edge combinations or the 8 moments) for up
+    // to four frequencies assembled together, within a quarter of free memory
+    const size_t per = sizeof(double2) * (g.combo ? 9 : 8) * g.npairs;
+    size_t freeb = 0, totalb = 0;
+    g.mf = 1;
+    if ((g.Nq == 3 || g.Nq == 7) && cudaMemGetInfo(&freeb, &totalb) == cudaSuccess)
+        for (int f = 4; f >= 2; f--)
+            if (f * per <= freeb / 4) {
+                g.mf = f;
+                break;
+            }
+    EFIE_TRY(g.moments.reserve(per * g.mf));
     return EFIE_OK;
 }
+
+namespace {
+
+// the pair-value store of frequency slot j of the geometry's moment buffer
+MomStore mom_store(const GeomDev &g, const Physics &ph, int j) {
+    const size_t planes = g.combo ? 9 : 8;
+    return MomStore{g.moments.as<double2>() + (size_t)j * planes * g.npairs, g.npairs,
+                    g.combo ? g.tri_d.as<double4>() : nullptr, ph.alr, ph.ali, ph.ber, ph.bei};
+}
+
+double regular_pairs(const GeomDev &g) {
+    // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
+    const double all = g.symmetric ? 0.5 * (double)g.Nt * (g.Nt + 1) : (double)g.Nt * g.Nt;
+    return g.scheme == EFIE_SCHEME_EXTRACT ? all - (double)g.n_adj : all - (double)g.n_near - (double)g.Nt;
+}
+
+template <int F>
+void launch_regular_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, const MomStores &ms) {
+    dim3 grid((g.Nt + 31) / 32, (g.Nt + 7) / 8);
+    const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
+    const uint8_t *skip = g.near_mask.as<uint8_t>();
+    const double dkr = (ph[F - 1].kr - ph[0].kr) / (F - 1), dki = (ph[F - 1].ki - ph[0].ki) / (F - 1);
+    switch (g.Nq) {
+    case 3:
+        k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
+                                                        dki, ms);
+        break;
+    case 7:
+        k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
+                                                        dki, ms);
+        break;
+    }
+}
+
+// k_f = k0 + f dk within 1e-12 |k_f| for f < n
+bool equally_spaced(const Physics *ph, int n) {
+    if (n < 2) return false;
+    const double dkr = (ph[n - 1].kr - ph[0].kr) / (n - 1), dki = (ph[n - 1].ki - ph[0].ki) / (n - 1);
+    for (int f = 1; f < n - 1; f++) {
+        const double er = ph[0].kr + f * dkr - ph[f].kr, ei = ph[0].ki + f * dki - ph[f].ki;
+        if (std::hypot(er, ei) > 1e-12 * std::hypot(ph[f].kr, ph[f].ki)) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z);
 
 efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
-    const int Nt = g.Nt, Ne = g.Ne;
-    const MomStore mom{g.moments.as<double2>(), g.npairs, g.combo ? g.tri_d.as<double4>() : nullptr,
-                       ph.alr, ph.ali, ph.ber, ph.bei};
+    const int Nt = g.Nt;
+    const MomStore mom = mom_store(g, ph, 0);
     dim3 grid((Nt + 31) / 32, (Nt + 7) / 8);
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
-    // regular pairs evaluated: all pairs (or t1 <= t2) minus near/self ones
-    const double all = g.symmetric ? 0.5 * (double)Nt * (Nt + 1) : (double)Nt * Nt;
-    const double n_regular = g.scheme == EFIE_SCHEME_EXTRACT ? all - (double)g.n_adj
-                                                             : all - (double)g.n_near - (double)Nt;
+    const double n_regular = regular_pairs(g);
     size_t tok = log.begin(s);
     switch (g.Nq) {
     case 1: k_regular_moments<1><<<grid, 256, 0, s>>>(Nt, g.symmetric, org, pts, skip, ph.kr, ph.ki, mom); break;
@@ -830,7 +971,44 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     }
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_QUAD, s, tok, n_regular * (double)g.Nq * g.Nq);
-    tok = log.begin(s);
+    return efie_assemble_finish(ctx, g, ph, 0, Z);
+}
+
+// Frequencies of a batch: equally spaced runs of up to g.mf frequencies share
+// one regular-pair launch (the Nq = 3 and 7 rules), then each frequency's
+// near/self or singular pairs and gather run on its own store.
+efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z) {
+    int f0 = 0;
+    while (f0 < nf) {
+        int n = std::min(g.mf, nf - f0);
+        while (n > 1 && !equally_spaced(ph + f0, n)) n--;
+        if (n < 2 || (g.Nq != 3 && g.Nq != 7)) {
+            EFIE_TRY(efie_assemble_device(ctx, g, ph[f0], Z[f0]));
+            f0++;
+            continue;
+        }
+        MomStores ms{};
+        for (int j = 0; j < n; j++) ms.s[j] = mom_store(g, ph[f0 + j], j);
+        size_t tok = ctx->log.begin(ctx->stream);
+        if (n == 2) launch_regular_mf<2>(g, ctx->stream, ph + f0, ms);
+        else if (n == 3) launch_regular_mf<3>(g, ctx->stream, ph + f0, ms);
+        else launch_regular_mf<4>(g, ctx->stream, ph + f0, ms);
+        EFIE_CUDA(cudaGetLastError());
+        ctx->log.end(EFIE_K_QUAD, ctx->stream, tok, n * regular_pairs(g) * (double)g.Nq * g.Nq);
+        for (int j = 0; j < n; j++) EFIE_TRY(efie_assemble_finish(ctx, g, ph[f0 + j], j, Z[f0 + j]));
+        f0 += n;
+    }
+    return EFIE_OK;
+}
+
+// Near/self (or singular) pairs of one frequency into store j, then its gather.
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z) {
+    cudaStream_t s = ctx->stream;
+    KernelLog &log = ctx->log;
+    const int Nt = g.Nt, Ne = g.Ne;
+    const MomStore mom = mom_store(g, ph, j);
+    const double4 *org = g.origin.as<double4>();
+    size_t tok = log.begin(s);
     int nl = 0;
     double qpe = 0;
     if (g.scheme == EFIE_SCHEME_EXTRACT) {

@@ -626,11 +626,19 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         const int nb = std::min(B, Nf - f0);
         int active[EFIE_MAX_BATCH] = {0};
         for (int f = 0; f < nb; f++) active[f] = 1;
-        for (int f = 0; f < nb && rc == EFIE_OK; f++) {
-            const Physics ph = efie_physics(freqs[f0 + f], p->mu, p->eps);
-            void *Zf = p->Z.as<efie_c128>() + NN * f;
-            if (p->centroid) rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph, Zf, p->scratch);
-            else rc = efie_assemble_device(ctx, p->g, ph, Zf);
+        {
+            Physics ph[EFIE_MAX_BATCH];
+            void *Zf[EFIE_MAX_BATCH];
+            for (int f = 0; f < nb; f++) {
+                ph[f] = efie_physics(freqs[f0 + f], p->mu, p->eps);
+                Zf[f] = p->Z.as<efie_c128>() + NN * f;
+            }
+            if (p->centroid) {
+                for (int f = 0; f < nb && rc == EFIE_OK; f++)
+                    rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph[f], Zf[f], p->scratch);
+            } else {
+                rc = efie_assemble_batch(ctx, p->g, ph, nb, Zf);
+            }
         }
         if (rc != EFIE_OK) break;
         bool fallback[EFIE_MAX_BATCH] = {false};

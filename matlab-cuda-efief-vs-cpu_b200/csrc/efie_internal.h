@@ -172,6 +172,7 @@ struct GeomDev {
     DevBuf moments;           // double2[9 or 8][npairs]: component-major pair values (assemble.cu)
     size_t npairs = 0;
     bool combo = false;       // edge-combination form (9 values per pair) in use
+    int mf = 1;               // frequencies whose pair values fit the moment buffer together
     DevBuf tri_d;             // double4[3*Nt] free-vertex vectors per triangle slot
     DevBuf edge_tl;           // int32[2*Ne] 4 t + slot per RWG side (-1 = none)
     DevBuf edge_c;            // double[2*Ne] RWG coefficient c per side
@@ -189,6 +190,9 @@ Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
                              int rule_order, GeomDev &g);
 efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/);
+// nf frequencies of a batch into Z[0 .. nf-1] (equally spaced runs share the
+// regular-pair evaluation)
+efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z);
 efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, double selfAlpha,
                                           const Physics &ph, void *Z, DevBuf &scratch);
 #endif

@@ -108,6 +108,30 @@ def test_plan_reuse_and_currents():
     plan.close()
 
 
+@pytest.mark.parametrize("spacing", ["even", "uneven"])
+def test_multi_frequency_assembly_matches_oracle(spacing):
+    """Equally spaced frequencies of a batch share one regular-pair launch
+    (e^{-jk_f R} by recurrence in f); unevenly spaced ones are assembled one by
+    one.  The currents solve the oracle's Z of each frequency to 1e-9."""
+    m = pkg()
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    r = p["rwg"]
+    freqs = np.linspace(d.freqs[0], d.freqs[-1], 4)
+    if spacing == "uneven":
+        freqs[1] *= 1.001
+    plan = m.SweepPlan(p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"],
+                       r["rp"], r["rm"], r["Ap"], r["Am"], r["len"], p["prepack"], d.mu, d.eps, p["patchEdge"],
+                       p["groundEdge"], d.V0, p["spread"], d.Z0, opts=m.sweep_opts(batch=4))
+    _, _, I = plan.run(freqs, return_currents=True)
+    plan.close()
+    for j, f in enumerate(freqs):
+        omega, k, _, _ = eo.physics(f, d.mu, d.eps)
+        Z = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
+        x = I[:, j]
+        assert np.linalg.norm(p["b"] - Z @ x) / np.linalg.norm(p["b"]) < 1e-9
+
+
 @pytest.mark.parametrize("batch", [1, 2, 4])
 def test_batched_sweep_matches_unbatched(batch):
     """Frequencies solved together (ragged last batch) give the same Zin."""
@@ -142,7 +166,8 @@ def test_gmres_converges_where_classical_refinement_stalls():
 def test_graph_replay_matches_eager_launches():
     """The mixed factorization replayed from a captured CUDA graph (timing off)
     gives bit-identical results to eager launches (timing on), and later
-    batches of the same plan replay the graph."""
+    batches of the same plan replay the graph (the reversed sweep within the
+    refinement tolerance)."""
     m = pkg()
     d = config1_design("grid")
     p = eo.build_problem(d)
@@ -166,4 +191,7 @@ def test_graph_replay_matches_eager_launches():
     finally:
         nat.check(nat.lib().efie_ctx_set_stream(nat.context(), None))
     assert np.array_equal(Zg, Ze) and np.array_equal(Sg, Se)
-    assert np.array_equal(Zg2, Zg[::-1])
+    # in reverse order the frequencies share their regular-pair launches with
+    # other neighbours (e^{-jk_f R} by recurrence from the group's first
+    # frequency): Z moves in its last bits, Zin within the GMRES tolerance
+    assert np.abs(Zg2 - Zg[::-1]).max() <= 1e-8 * np.abs(Zg).max()
