@@ -17,7 +17,7 @@ import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned.json")
-BATCHES = (4, 8, 16)
+BATCHES = (8, 16, 32)
 PANELS = (64, 128, 256)
 
 
