@@ -12,6 +12,7 @@
 //   Ivec = c_m c_n [S3 - d_n.S1 - d_m.S2 + (d_m.d_n) S0],  Isca = 4 c_m c_n S0
 // with d = v - o.  Pair regimes follow Z_entry (CPU_FAST.m:48-54): self when
 // t1 == t2, near when nearMat(t1,t2), else regular.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -670,6 +671,21 @@ __global__ void __launch_bounds__(256) k_centroid_z(int Ne, const Side *__restri
     Z[(size_t)m + (size_t)Ne * n] = make_double2(zr, zi);
 }
 
+// The pair mask (1 = near, adjacent or self: not a regular pair) from the
+// pair list, on a zeroed mask: entry (t1, t2) and, for a symmetric list, (t2, t1).
+__global__ void k_mask_pairs(int Nt, int n, const int2 *__restrict__ list, bool both, uint8_t *__restrict__ mask) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 pr = list[i];
+    mask[(size_t)pr.x + (size_t)Nt * pr.y] = 1;
+    if (both) mask[(size_t)pr.y + (size_t)Nt * pr.x] = 1;
+}
+
+__global__ void k_mask_self(int Nt, uint8_t *__restrict__ mask) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < Nt) mask[(size_t)t * (Nt + 1)] = 1;
+}
+
 }  // namespace
 
 Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps) {
@@ -782,7 +798,9 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
         }
     }
 
-    std::vector<uint8_t> mask((size_t)Nt * Nt, 0);
+    // the pair list whose entries (and diagonal) the device mask marks
+    std::vector<int2> list;
+    bool mask_both = true;
     if (scheme == EFIE_SCHEME_REF) {
         const int Nq = pre->Nq, Nq2 = pre->Nq2, NsS = pre->NsS, NsN = pre->NsN;
         g.Nq = Nq;
@@ -817,23 +835,35 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
         EFIE_TRY(up(g.self_pts, selfp.data(), sizeof(double4) * selfp.size()));
         EFIE_TRY(up(g.self_a, pre->self_a, sizeof(double) * (size_t)Nt * NsS));
         EFIE_TRY(up(g.aeq, pre->aeqTri, sizeof(double) * Nt));
-        // pair regimes; symmetric storage only if nearMat is symmetric
-        bool sym = true;
-        for (int t2 = 0; t2 < Nt && sym; t2++)
-            for (int t1 = 0; t1 < t2; t1++)
-                if ((pre->nearMat[(size_t)t1 + (size_t)Nt * t2] != 0) != (pre->nearMat[(size_t)t2 + (size_t)Nt * t1] != 0)) {
-                    sym = false;
-                    break;
-                }
-        g.symmetric = sym;
-        std::vector<int2> list;
-        for (int t2 = 0; t2 < Nt; t2++)
-            for (int t1 = 0; t1 < Nt; t1++) {
-                const bool self = t1 == t2;
-                const bool nr = !self && pre->nearMat[(size_t)t1 + (size_t)Nt * t2] != 0;
-                mask[(size_t)t1 + (size_t)Nt * t2] = (self || nr) ? 1 : 0;
-                if (nr && (!sym || t1 < t2)) list.push_back(make_int2(t1, t2));
+        // near pairs (t1 != t2, nearMat nonzero) column by column, skipping
+        // zero bytes eight at a time: nearMat is almost all zeros
+        std::vector<int2> all;
+        for (int t2 = 0; t2 < Nt; t2++) {
+            const uint8_t *col = pre->nearMat + (size_t)Nt * t2;
+            int t1 = 0;
+            for (; t1 + 8 <= Nt; t1 += 8) {
+                uint64_t w;
+                std::memcpy(&w, col + t1, 8);
+                if (!w) continue;
+                for (int j = 0; j < 8; j++)
+                    if (col[t1 + j] && t1 + j != t2) all.push_back(make_int2(t1 + j, t2));
             }
+            for (; t1 < Nt; t1++)
+                if (col[t1] && t1 != t2) all.push_back(make_int2(t1, t2));
+        }
+        // pair regimes; symmetric storage only if nearMat is symmetric: every
+        // (t1, t2) of the list has its (t2, t1)
+        std::vector<int64_t> keys(all.size());
+        for (size_t i = 0; i < all.size(); i++) keys[i] = (int64_t)all[i].x * Nt + all[i].y;
+        std::sort(keys.begin(), keys.end());
+        bool sym = true;
+        for (size_t i = 0; i < all.size() && sym; i++)
+            sym = std::binary_search(keys.begin(), keys.end(), (int64_t)all[i].y * Nt + all[i].x);
+        g.symmetric = sym;
+        // the near list in column order (t1 < t2 when symmetric)
+        for (const int2 &pr : all)
+            if (!sym || pr.x < pr.y) list.push_back(pr);
+        mask_both = sym;
         g.n_near = (int)list.size();
         EFIE_TRY(up(g.near_list, list.data(), sizeof(int2) * (list.empty() ? 1 : list.size())));
     } else if (scheme == EFIE_SCHEME_EXTRACT) {
@@ -867,7 +897,6 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
         std::vector<std::vector<int>> vt(Nv);
         for (int t = 0; t < Nt; t++)
             for (int j = 0; j < 3; j++) vt[mesh->F[t + (size_t)j * Nt] - 1].push_back(t);
-        std::vector<int2> list;
         std::vector<int> seen(Nt, -1);
         for (int t1 = 0; t1 < Nt; t1++) {
             for (int j = 0; j < 3; j++)
@@ -875,8 +904,6 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
                     if (t2 >= t1 && seen[t2] != t1) {
                         seen[t2] = t1;
                         list.push_back(make_int2(t1, t2));
-                        mask[(size_t)t1 + (size_t)Nt * t2] = 1;
-                        mask[(size_t)t2 + (size_t)Nt * t1] = 1;
                     }
         }
         g.symmetric = true;
@@ -886,7 +913,20 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     } else {
         return efie_fail(EFIE_ERR_ARGS, "unknown scheme");
     }
-    EFIE_TRY(up(g.near_mask, mask.data(), mask.size()));
+    // the pair mask is built on the device from the list: zeros, the list's
+    // entries (both orientations when symmetric), the diagonal
+    {
+        const size_t nn = (size_t)Nt * Nt;
+        EFIE_TRY(g.near_mask.reserve(nn));
+        EFIE_CUDA(cudaMemsetAsync(g.near_mask.p, 0, nn, ctx->stream));
+        DevBuf &lst = scheme == EFIE_SCHEME_REF ? g.near_list : g.adj_list;
+        const int n = (int)list.size();
+        if (n > 0)
+            k_mask_pairs<<<(n + 255) / 256, 256, 0, ctx->stream>>>(Nt, n, lst.as<int2>(), mask_both,
+                                                                   g.near_mask.as<uint8_t>());
+        k_mask_self<<<(Nt + 255) / 256, 256, 0, ctx->stream>>>(Nt, g.near_mask.as<uint8_t>());
+        EFIE_CUDA(cudaGetLastError());
+    }
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
     // component planes of npairs (9 edge combinations or the 8 moments) for up
     // to four frequencies assembled together, within a quarter of free memory
