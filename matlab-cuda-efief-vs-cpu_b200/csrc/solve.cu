@@ -725,7 +725,11 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     const size_t pbytes = sizeof(float) * w.pstride * B;
     if (pbytes > w.planes.bytes) {
         EFIE_TRY(w.planes.reserve(pbytes));
-        EFIE_CUDA(cudaMemset(w.planes.p, 0, pbytes));  // padding columns stay zero
+        // the padding columns N .. ld-1 of every row stay zero (the triangular
+        // solves' aligned loads read them); every other entry is written per batch
+        if (w.ld > N)
+            EFIE_CUDA(cudaMemset2D(w.planes.as<float>() + N, sizeof(float) * w.ld, 0, sizeof(float) * (w.ld - N),
+                                   (size_t)2 * N * B));
     }
     EFIE_TRY(w.dinv.reserve(sizeof(float2) * w.dstride * B));
     EFIE_TRY(w.vec.reserve(sizeof(float2) * 3 * (size_t)w.vstride * B));
