@@ -309,7 +309,7 @@ def run_ours(args):
     B = args.batch or len(freqs)
     # frequency slots of the plan: automatic, but no more than the points of a step
     opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
-                        batch=B if B < 8 else 0)
+                        batch=B if B < 8 else 0, lu_nb=args.lu_nb)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -364,10 +364,10 @@ def run_ours(args):
         fr = batch(args.warmup + s)
         t0 = time.perf_counter()
         if args.scheme == "ref":
-            m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver))
+            m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb))
         else:
             # plan create (host mesh upload) + run + destroy through the C ABI
-            p2 = m.SweepPlan(*pargs, *inp["tail"], opts=m.sweep_opts(solver=args.solver, scheme="extract"),
+            p2 = m.SweepPlan(*pargs, *inp["tail"], opts=m.sweep_opts(solver=args.solver, scheme="extract", lu_nb=args.lu_nb),
                              rule_order=RULE[args.scheme])
             p2.run(fr)
             p2.close()
@@ -565,6 +565,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=300, help="cfg4: training epochs")
     ap.add_argument("--batch", type=int, default=0, help="frequency points per step (0 = the whole sweep)")
     ap.add_argument("--solver", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--lu-nb", type=int, default=0, choices=[0, 64, 128, 256, 512],
+                    help="outer LU panel width (0: the library's choice)")
     ap.add_argument("--scheme", choices=["ref", "extract"], default="ref",
                     help="ref: the reference's cached subdivision + softening; extract: Dunavant 7-point rule "
                          "+ analytic 1/R extraction")

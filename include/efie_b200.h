@@ -162,7 +162,7 @@ typedef struct efie_sweep_opts {
     int32_t scheme;          /* efie_scheme; default EFIE_SCHEME_REF            */
     double refine_tol;       /* relative residual target; default 1e-10         */
     int32_t refine_max_iter; /* default 30                                      */
-    int32_t lu_nb;           /* outer LU panel width 64/128/256 (0 = tuned)     */
+    int32_t lu_nb;           /* outer LU panel width 64/128/256/512 (0 = tuned) */
     int32_t timing;          /* 1 = record per-phase CUDA-event timings         */
     int32_t batch;           /* frequencies solved together (0 = automatic)     */
     int32_t refine_method;   /* efie_refine_method; default EFIE_REFINE_GMRES    */

@@ -18,7 +18,7 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned.json")
 BATCHES = (8, 16, 32)
-PANELS = (64, 128, 256)
+PANELS = (128, 256, 512)
 
 
 def _key(Ne, sms):

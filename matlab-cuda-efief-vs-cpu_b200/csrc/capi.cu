@@ -510,8 +510,8 @@ int choose_batch(int N, int requested, int solver) {
 // panels cut trailing-matrix traffic; narrower ones keep fewer terms per
 // tensor-core accumulation).
 int choose_panel(int N, int requested) {
-    if (requested == 64 || requested == 128 || requested == 256) return requested;
-    return N >= 4096 ? 256 : 128;
+    if (requested == 64 || requested == 128 || requested == 256 || requested == 512) return requested;
+    return N >= 4096 ? 512 : 128;
 }
 
 efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c128 eps, int pe, int ge, double V0,

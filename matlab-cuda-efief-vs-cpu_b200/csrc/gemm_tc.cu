@@ -49,7 +49,7 @@
 
 namespace {
 
-constexpr int KMAX = 256;        // largest complex K of one update (the outer LU block)
+constexpr int KMAX = 512;        // largest complex K of one update (the outer LU block)
 constexpr int TR = 128;          // complex rows of L21 per CTA (one TMEM lane each)
 constexpr int TN = 256;          // complex columns of the pair's tile (MMA N)
 constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K chunk)

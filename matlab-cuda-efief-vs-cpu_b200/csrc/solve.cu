@@ -712,8 +712,8 @@ int efie_solve_nb() { return NB; }
 
 efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(set_smem_attrs());
-    if (kb_outer != 64 && kb_outer != 128 && kb_outer != 256)
-        return efie_fail(EFIE_ERR_ARGS, "LU panel width must be 64, 128 or 256");
+    if (kb_outer != 64 && kb_outer != 128 && kb_outer != 256 && kb_outer != 512)
+        return efie_fail(EFIE_ERR_ARGS, "LU panel width must be 64, 128, 256 or 512");
     w.kb_outer = kb_outer;
     w.N = N;
     w.B = B;

@@ -132,6 +132,19 @@ def test_multi_frequency_assembly_matches_oracle(spacing):
         assert np.linalg.norm(p["b"] - Z @ x) / np.linalg.norm(p["b"]) < 1e-9
 
 
+@pytest.mark.parametrize("lu_nb", [128, 256, 512])
+def test_panel_widths_match_oracle(lu_nb):
+    """Every outer panel width of the two-level LU (the K of the tensor-core
+    trailing updates) reaches the refinement target and the oracle's Zin."""
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    freqs = d.freqs[:4]
+    Zb, _, st = _sweep(p, freqs, "mixed", lu_nb=lu_nb)
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zb - Zo) / np.abs(Zo)).max() <= 1e-6
+    assert st["n_fp64_fallback"] == 0 and st["max_relres"] <= 1e-10
+
+
 @pytest.mark.parametrize("batch", [1, 2, 4])
 def test_batched_sweep_matches_unbatched(batch):
     """Frequencies solved together (ragged last batch) give the same Zin."""
