@@ -602,9 +602,12 @@ __global__ void __launch_bounds__(256) k_gather_z(int Ne, int Nt, bool sym, cons
 // Symmetric Z (symmetric pair regimes): only 32x32 tiles with bm <= bn are
 // evaluated; an off-diagonal tile is also stored transposed through shared
 // memory, so Z(n,m) is a bit-exact copy of Z(m,n).
+// With pr set, the tile is also written as the complex64 working matrix of
+// the mixed solver: FP32 planes re = pr[m * ld + n], im = pr[(Ne + m) * ld + n]
+// (row-major, both triangles), coalesced through the same shared-memory tile.
 template <bool COMBO>
 __global__ void __launch_bounds__(256) k_gather_z_sym(int Ne, int Nt, const EdgeData E, const MomStore mom,
-                                                      double2 *__restrict__ Z) {
+                                                      double2 *__restrict__ Z, float *__restrict__ pr, int ld) {
     const int bm = blockIdx.x, bn = blockIdx.y;
     if (bm > bn) return;
     __shared__ double2 tile[32][33];
@@ -619,8 +622,30 @@ __global__ void __launch_bounds__(256) k_gather_z_sym(int Ne, int Nt, const Edge
         }
         tile[j][tx] = z;
     }
-    if (bm == bn) return;
+    if (bm == bn && !pr) return;
     __syncthreads();
+    if (pr) {
+        float *pi = pr + (size_t)ld * Ne;
+        // row m = bm * 32 + j of the planes, columns n = bn * 32 + tx
+        for (int j = ty; j < 32; j += 8) {
+            const int mm = bm * 32 + j, nn = bn * 32 + tx;
+            if (mm < Ne && nn < Ne) {
+                const double2 v = tile[tx][j];
+                pr[(size_t)mm * ld + nn] = (float)v.x;
+                pi[(size_t)mm * ld + nn] = (float)v.y;
+            }
+        }
+        if (bm != bn)   // row n = bn * 32 + j, columns m = bm * 32 + tx: Z(n, m) = Z(m, n)
+            for (int j = ty; j < 32; j += 8) {
+                const int nn = bn * 32 + j, mm = bm * 32 + tx;
+                if (mm < Ne && nn < Ne) {
+                    const double2 v = tile[j][tx];
+                    pr[(size_t)nn * ld + mm] = (float)v.x;
+                    pi[(size_t)nn * ld + mm] = (float)v.y;
+                }
+            }
+    }
+    if (bm == bn) return;
     for (int j = ty; j < 32; j += 8) {
         const int mm = bm * 32 + j, nn = bn * 32 + tx;
         if (mm < Ne && nn < Ne) Z[(size_t)nn + (size_t)Ne * mm] = tile[tx][j];
@@ -989,9 +1014,9 @@ bool equally_spaced(const Physics *ph, int n) {
 
 }  // namespace
 
-efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z);
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld);
 
-efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z) {
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z, float *pr, int ld) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int Nt = g.Nt;
@@ -1011,19 +1036,23 @@ efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, v
     }
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_QUAD, s, tok, n_regular * (double)g.Nq * g.Nq);
-    return efie_assemble_finish(ctx, g, ph, 0, Z);
+    return efie_assemble_finish(ctx, g, ph, 0, Z, pr, ld);
 }
 
 // Frequencies of a batch: equally spaced runs of up to g.mf frequencies share
 // one regular-pair launch (the Nq = 3 and 7 rules), then each frequency's
 // near/self or singular pairs and gather run on its own store.
-efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z) {
+efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z,
+                                const PlanesOut *po) {
+    if (po && !g.symmetric) return efie_fail(EFIE_ERR_ARGS, "complex64 planes need the symmetric gather");
+    auto planes = [&](int f) { return po ? po->p + po->pstride * f : nullptr; };
+    const int ld = po ? po->ld : 0;
     int f0 = 0;
     while (f0 < nf) {
         int n = std::min(g.mf, nf - f0);
         while (n > 1 && !equally_spaced(ph + f0, n)) n--;
         if (n < 2 || (g.Nq != 3 && g.Nq != 7)) {
-            EFIE_TRY(efie_assemble_device(ctx, g, ph[f0], Z[f0]));
+            EFIE_TRY(efie_assemble_device(ctx, g, ph[f0], Z[f0], planes(f0), ld));
             f0++;
             continue;
         }
@@ -1035,14 +1064,15 @@ efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, in
         else launch_regular_mf<4>(g, ctx->stream, ph + f0, ms);
         EFIE_CUDA(cudaGetLastError());
         ctx->log.end(EFIE_K_QUAD, ctx->stream, tok, n * regular_pairs(g) * (double)g.Nq * g.Nq);
-        for (int j = 0; j < n; j++) EFIE_TRY(efie_assemble_finish(ctx, g, ph[f0 + j], j, Z[f0 + j]));
+        for (int j = 0; j < n; j++)
+            EFIE_TRY(efie_assemble_finish(ctx, g, ph[f0 + j], j, Z[f0 + j], planes(f0 + j), ld));
         f0 += n;
     }
     return EFIE_OK;
 }
 
 // Near/self (or singular) pairs of one frequency into store j, then its gather.
-efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z) {
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int Nt = g.Nt, Ne = g.Ne;
@@ -1082,15 +1112,15 @@ efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, i
     double2 *Zd = static_cast<double2 *>(Z);
     if (g.symmetric) {
         dim3 gs((Ne + 31) / 32, (Ne + 31) / 32);
-        if (g.combo) k_gather_z_sym<true><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd);
-        else k_gather_z_sym<false><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd);
+        if (g.combo) k_gather_z_sym<true><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd, pr, ld);
+        else k_gather_z_sym<false><<<gs, 256, 0, s>>>(Ne, Nt, E, mom, Zd, pr, ld);
     } else {
         dim3 gg((Ne + 63) / 64, (Ne + 3) / 4);
         if (g.combo) k_gather_z<true><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
         else k_gather_z<false><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
     }
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_GATHER, s, tok, 16.0 * (double)Ne * Ne);
+    log.end(EFIE_K_GATHER, s, tok, (pr ? 24.0 : 16.0) * (double)Ne * Ne);
     return EFIE_OK;
 }
 

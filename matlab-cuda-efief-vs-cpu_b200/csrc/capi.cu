@@ -576,6 +576,8 @@ extern "C" efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, co
     // a symmetric gather writes Z(n,m) as a copy of Z(m,n): the refinement's
     // products then read only the upper triangle
     if (s == EFIE_OK) p->sw.zsym = p->g.symmetric;
+    // the symmetric gather also writes the mixed solver's complex64 planes
+    if (s == EFIE_OK) p->sw.planes_from_assembly = p->opts.solver == EFIE_SOLVER_MIXED && p->g.symmetric;
     if (s == EFIE_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         s = efie_fail(EFIE_ERR_CUDA, "geometry upload failed");
     if (s != EFIE_OK) {
@@ -637,7 +639,8 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 for (int f = 0; f < nb && rc == EFIE_OK; f++)
                     rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph[f], Zf[f], p->scratch);
             } else {
-                rc = efie_assemble_batch(ctx, p->g, ph, nb, Zf);
+                const PlanesOut po{p->sw.planes.as<float>(), p->sw.pstride, p->sw.ld};
+                rc = efie_assemble_batch(ctx, p->g, ph, nb, Zf, p->sw.planes_from_assembly ? &po : nullptr);
             }
         }
         if (rc != EFIE_OK) break;

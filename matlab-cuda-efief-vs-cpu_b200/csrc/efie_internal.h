@@ -189,10 +189,21 @@ Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
 // assemble.cu
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
                              int rule_order, GeomDev &g);
-efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/);
+// pr (optional, symmetric gather only): also write the complex64 working
+// matrix of the mixed solver as FP32 planes, re at pr[m * ld + n], im at
+// pr[(Ne + m) * ld + n]
+efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z /*c128 Ne*Ne*/,
+                                 float *pr = nullptr, int ld = 0);
+// the planes of frequency slot f at p + pstride * f
+struct PlanesOut {
+    float *p;
+    size_t pstride;
+    int ld;
+};
 // nf frequencies of a batch into Z[0 .. nf-1] (equally spaced runs share the
-// regular-pair evaluation)
-efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z);
+// regular-pair evaluation), and into the planes of slots 0 .. nf-1 when po is set
+efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, int nf, void *const *Z,
+                                const PlanesOut *po = nullptr);
 efie_status efie_assemble_centroid_device(efie_ctx *ctx, const efie_mesh *mesh, double selfAlpha,
                                           const Physics &ph, void *Z, DevBuf &scratch);
 #endif

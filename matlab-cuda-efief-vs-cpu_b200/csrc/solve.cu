@@ -797,10 +797,13 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     char *ctl = w.ctl.as<char>();
     const int *active = w.active.as<int>();
     dim3 tg((N + 31) / 32, (N + 31) / 32, B);
-    size_t tok = log.begin(s0);
-    k_z_to_planes<<<tg, 256, 0, s0>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
-    EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_PANEL, s0, tok, 24.0 * (double)N * N * nact);
+    size_t tok = 0;
+    if (!w.planes_from_assembly) {
+        tok = log.begin(s0);
+        k_z_to_planes<<<tg, 256, 0, s0>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
+        EFIE_CUDA(cudaGetLastError());
+        log.end(EFIE_K_PANEL, s0, tok, 24.0 * (double)N * N * nact);
+    }
     float2 *dinv = w.dinv.as<float2>();
     EFIE_CUDA(cudaEventRecord(w.ev_start, s0));
     EFIE_CUDA(cudaStreamWaitEvent(w.hi, w.ev_start, 0));

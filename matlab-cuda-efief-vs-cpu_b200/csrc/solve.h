@@ -52,6 +52,9 @@ struct SolveWork {
     // Z is bit-exactly symmetric (symmetric gather): matrix-vector products read
     // only its upper triangle (128 x 128 tiles, partial vectors in spart)
     bool zsym = false;
+    // the assembly writes the complex64 planes of each batch itself (symmetric
+    // gather): the factorization starts without converting Z
+    bool planes_from_assembly = false;
     DevBuf spart;
     // look-ahead LU: the panel chain runs on `hi` (highest priority) while the
     // bulk of each deferred trailing update runs on `lo`
