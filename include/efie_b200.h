@@ -306,6 +306,16 @@ efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32
 /* 1 disables the tensor-core trailing update process-wide (CUDA-core path). */
 void efie_debug_disable_tensor_cores(int disable);
 
+/* 1 makes the mixed LU of a symmetric Z factor it as a general matrix
+ * (every trailing update over the full block) instead of L D L^T with U
+ * formed from L, process-wide.  No counterpart in the reference. */
+void efie_debug_disable_symmetric_lu(int disable);
+
+/* Outer panel width of efie_lu_selftest: 64/128/256/512 (anything else:
+ * 256, the default), process-wide.  A bit-exactly symmetric A takes the
+ * symmetric factorization unless efie_debug_disable_symmetric_lu(1). */
+void efie_debug_set_selftest_panel(int lu_nb);
+
 /* ---------------------------------------------------------------------- */
 /* Centroid assembly without device allocation                             */
 /* ---------------------------------------------------------------------- */

@@ -657,6 +657,31 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                                       p->opts.refine_max_iter, active, &rr);
             if (rc != EFIE_OK) break;
             S->refine_iters_max = std::max(S->refine_iters_max, rr.iters);
+            if (p->sw.zsym && p->sw.sym_lu && p->opts.refine_method == EFIE_REFINE_GMRES) {
+                // a frequency that missed the target with the L D L^T factors
+                // is factored again as a general matrix (eager launches, from
+                // Z) before the complex128 fallback
+                int retry[EFIE_MAX_BATCH] = {0};
+                int nr = 0;
+                for (int f = 0; f < nb; f++)
+                    if (!rr.converged[f] || rr.err[f]) retry[f] = 1, nr++;
+                if (nr > 0) {
+                    RefineResult r2;
+                    const bool pfa = p->sw.planes_from_assembly;
+                    p->sw.sym_lu = false;
+                    p->sw.planes_from_assembly = false;
+                    rc = efie_mixed_factor(ctx, p->sw, p->Z.p, NN, retry);
+                    if (rc == EFIE_OK)
+                        rc = efie_mixed_gmres(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
+                                              p->opts.refine_max_iter, retry, &r2);
+                    p->sw.sym_lu = true;
+                    p->sw.planes_from_assembly = pfa;
+                    if (rc != EFIE_OK) break;
+                    S->refine_iters_max = std::max(S->refine_iters_max, r2.iters);
+                    for (int f = 0; f < nb; f++)
+                        if (retry[f]) rr.relres[f] = r2.relres[f], rr.converged[f] = r2.converged[f], rr.err[f] = r2.err[f];
+                }
+            }
             for (int f = 0; f < nb; f++) {
                 if (!rr.converged[f] || rr.err[f]) {
                     // zero pivot, timeout or stalled refinement: complex128 LU for this frequency
@@ -783,13 +808,30 @@ extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh 
 // ---------------------------------------------------------------------------
 // Self-test of the complex64 LU (no pivoting) used by the mixed solver.
 // ---------------------------------------------------------------------------
+static int g_selftest_nb = 256;
+extern "C" void efie_debug_set_selftest_panel(int lu_nb) {
+    g_selftest_nb = (lu_nb == 64 || lu_nb == 128 || lu_nb == 256 || lu_nb == 512) ? lu_nb : 256;
+}
+
 extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores,
                                         efie_c128 *LU) {
     if (!ctx || N < 1 || !A || !LU) return efie_fail(EFIE_ERR_ARGS, "efie_lu_selftest: bad arguments");
     DeviceGuard dg(ctx->device);
     ctx->log.reset(false);
     SolveWork w;
-    EFIE_TRY(efie_mixed_workspace(w, N, 1, 256));
+    EFIE_TRY(efie_mixed_workspace(w, N, 1, g_selftest_nb));
+    // a bit-exactly symmetric A takes the symmetric factorization, as a
+    // sweep's Z from the symmetric gather does
+    bool sym = true;
+    for (int j = 0; j < N && sym; j++)
+        for (int i = j + 1; i < N; i++) {
+            const efie_c128 a = A[(size_t)i + (size_t)N * j], b = A[(size_t)j + (size_t)N * i];
+            if (a.re != b.re || a.im != b.im) {
+                sym = false;
+                break;
+            }
+        }
+    w.zsym = sym;
     DevBuf dA;
     EFIE_TRY(dA.reserve(sizeof(efie_c128) * (size_t)N * N));
     EFIE_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(efie_c128) * (size_t)N * N, cudaMemcpyHostToDevice, ctx->stream));

@@ -300,6 +300,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Column tiles of row pair p in the lower-triangle mode: those whose first
+// column block of width kb does not lie right of the pair's last row block.
+__host__ __device__ __forceinline__ int tri_cols(int p, int nct, int kb) {
+    const int qr = (p * TN + TN - 1) / kb;
+    const int n = ((qr + 1) * kb + TN - 1) / TN;
+    return n < nct ? n : nct;
+}
+
 // ---------------------------------------------------------------------------
 // The update kernel.  C[r0:r1, c0:c1] -= (packed L) * (packed U) for the
 // pair's 256 x 256 tile; grid (2 x column tiles, row-pair tiles, frequency),
@@ -311,9 +319,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 const __half *__restrict__ Upackb, size_t ustride, int upitch, int uoff, const float *__restrict__ lmaxb,
                 const float *__restrict__ umaxb, size_t mstride, int nblk, int kcol, int krow, int K,
                 float *__restrict__ planes, size_t pstride, int ld, char *__restrict__ ctl,
-                const int *__restrict__ active) {
+                const int *__restrict__ active, int tri_kb) {
     const int f = blockIdx.z;
     if (!active[f]) return;   // both CTAs of a cluster share f
+    int ct = blockIdx.x >> 1;   // 256-column tile of the pair
+    int rp = blockIdx.y;        // 256-row tile of the pair
+    if (tri_kb > 0) {
+        // lower tiles of a square block in row order (both CTAs of the pair
+        // map the same x to the same tile)
+        const int npr = (r1 - r0 + TN - 1) / TN, nct = (c1 - c0 + TN - 1) / TN;
+        rp = 0;
+        while (rp < npr - 1) {
+            const int nc = tri_cols(rp, nct, tri_kb);
+            if (ct < nc) break;
+            ct -= nc;
+            rp++;
+        }
+        if (ct >= tri_cols(rp, nct, tri_kb)) return;
+    }
     const uint32_t rank = cluster_rank();
     const bool leader = rank == 0;
     const __half *Lpack = Lpackb + lstride * f, *Upack = Upackb + ustride * f;
@@ -329,8 +352,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
     float *col_is = reinterpret_cast<float *>(bars + 12);   // 16-byte aligned: inverse column scales
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ct = blockIdx.x >> 1;                  // 256-column tile of the pair
-    const int rtile = blockIdx.y * 2 + (int)rank;    // this CTA's 128-row tile
+    const int rtile = rp * 2 + (int)rank;            // this CTA's 128-row tile
     const int utile = ct * 2 + (int)rank;            // this CTA's 128-column half of U
 
     if (tid == 0) {
@@ -614,9 +636,11 @@ bool efie_gemm_uses_tc(int rows, int cols, int K) {
 // active frequency: tensor cores from the packed views when the block spans
 // enough work, CUDA cores from the factors otherwise.
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact, const PackView &Lv, const PackView &Uv) {
+                             int nact, const PackView &Lv, const PackView &Uv, int tri_kb) {
     const int rows = r1 - r0, cols = c1 - c0;
     if (rows <= 0 || cols <= 0 || K <= 0) return EFIE_OK;
+    if (tri_kb > 0 && (r0 != c0 || r1 != c1 || tri_kb % 64))
+        return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: the lower-triangle mode takes a square block");
     if (!efie_gemm_uses_tc(rows, cols, K)) {
         for (int k0 = 0; k0 < K; k0 += 64)
             EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
@@ -630,13 +654,25 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     cudaStream_t st = ctx->stream;
     const int npr = (rows + TN - 1) / TN, nct = (cols + TN - 1) / TN;   // 256-row pairs, 256-column tiles
     const int nchunk = (K + KC - 1) / KC;
+    // work: the entries the update must produce (in the lower-triangle mode
+    // those of column blocks <= row block, not the tiles' overhang)
+    dim3 grid(2 * nct, npr, B);
+    double entries = (double)rows * cols;
+    if (tri_kb > 0) {
+        int ntiles = 0;
+        for (int p = 0; p < npr; p++) ntiles += tri_cols(p, nct, tri_kb);
+        grid = dim3(2 * ntiles, 1, B);
+        entries = 0;
+        for (int q0 = 0; q0 < rows; q0 += tri_kb)
+            entries += (double)std::min(tri_kb, rows - q0) * std::min(cols, q0 + tri_kb);
+    }
     size_t tok = ctx->log.begin(st);
-    k_update_tc<<<dim3(2 * nct, npr, B), 256, GEMM_SMEM, st>>>(
+    k_update_tc<<<grid, 256, GEMM_SMEM, st>>>(
         *reinterpret_cast<const CUtensorMap *>(w.planes_map), N, r0, r1, c0, c1, nchunk,
         static_cast<const __half *>(Lv.base), Lv.stride, Lv.pitch, Lv.off, static_cast<const __half *>(Uv.base),
         Uv.stride, Uv.pitch, Uv.off, w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K,
-        w.planes.as<float>(), w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>());
+        w.planes.as<float>(), w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>(), tri_kb);
     EFIE_CUDA(cudaGetLastError());
-    ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
+    ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * entries * K * nact);
     return EFIE_OK;
 }

@@ -106,7 +106,7 @@ __device__ __forceinline__ float2 crecip(float2 p, bool &zero) {
 __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int bi, float *__restrict__ planes,
                                                      size_t pstride, int ld, float2 *__restrict__ dinv,
                                                      size_t dstride, char *__restrict__ ctl,
-                                                     const int *__restrict__ active) {
+                                                     const int *__restrict__ active, int sym) {
     const int f = blockIdx.x;
     if (!active[f]) return;
     extern __shared__ float2 dsm[];
@@ -124,7 +124,9 @@ __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int b
         const int r = e >> 6, c = e & 63;
         float2 v = make_float2(r == c ? 1.f : 0.f, 0.f);   // identity beyond kb
         if (r < kb && c < kb) {
-            const size_t o = (size_t)(k + r) * ld + k + c;
+            // symmetric Z: the lower triangle, mirrored
+            const int rr = (sym && c > r) ? c : r, cc = (sym && c > r) ? r : c;
+            const size_t o = (size_t)(k + rr) * ld + k + cc;
             v = make_float2(Ar[o], Ai[o]);
         }
         A[r][c] = v;
@@ -149,11 +151,18 @@ __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int b
 #pragma unroll
             for (int j = 0; j < SB; j++) {
                 float2 u[SB];
+                // row o + j sits in lane j; symmetric Z (L D L^T): the row is
+                // the column below the pivot, row o + c in lane c
+                u[j] = shfl2(a0[j], j);
 #pragma unroll
-                for (int c = j; c < SB; c++) u[c] = shfl2(a0[c], j);   // row o + j sits in lane j
+                for (int c = j + 1; c < SB; c++) u[c] = sym == 1 ? shfl2(a0[j], c) : shfl2(a0[c], j);
                 bool z;
                 const float2 inv = crecip(u[j], z);
                 bad |= z;
+                if (sym == 1 && lane == j) {
+#pragma unroll
+                    for (int c = j + 1; c < SB; c++) a0[c] = u[c];
+                }
                 if (lane > j) {
                     const float2 l = cmulf(a0[j], inv);
                     a0[j] = l;
@@ -173,7 +182,11 @@ __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int b
         }
         __syncthreads();
         const int w = NB - o - SB;   // columns (rows) right of (below) the panel
-        if (t < w) {                 // U strip: forward substitution with the panel's unit-lower block
+        if (sym == 1 && t < w) {     // U strip of L D L^T: U[o + i][c] = d_i L[c][o + i]
+            const int c = o + SB + t;
+#pragma unroll
+            for (int i = 0; i < SB; i++) A[o + i][c] = cmulf(A[o + i][o + i], A[c][o + i]);
+        } else if (t < w) {          // U strip: forward substitution with the panel's unit-lower block
             const int c = o + SB + t;
             float2 x[SB];
 #pragma unroll
@@ -266,6 +279,16 @@ __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int b
         __syncthreads();
     }
 
+    if (sym == 1) {
+        // U = D L^T: U^-1 = L^-T D^-1 from L^-1, so that U^-1 L^-1 is
+        // symmetric as the inverse of a symmetric block is
+        for (int e = t; e < NB * NB; e += 256) {
+            const int r = e >> 6, c = e & 63;
+            bool z;
+            Y[r][c] = r <= c ? cmulf(X[c][r], crecip(A[c][c], z)) : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+    }
     // ---- factors back to the planes, inverses to their slots ----
     for (int e = t; e < NB * NB; e += 256) {
         const int r = e >> 6, c = e & 63;
@@ -280,10 +303,48 @@ __global__ void __launch_bounds__(256) k_diag_factor(int N, int k, int kb, int b
     if (t == 0 && bad) atomicExch(err, 1);
 }
 
+// A finished 64 x 64 factor block (thread (ty, tx) holds rows ty + 16 a,
+// columns tx + 16 b) as tensor-core operand of the panel chain's updates
+// (K = 64): rows of L (columns of U when ublk) scaled by the power of two of
+// their maximum mx, split into FP16 hi + lo, in the packed layout
+// [chunk][re hi, re lo, im hi, im lo][row][32] with the 64-byte swizzle,
+// staged in `pk` (32 KB of shared memory), then the eight 64-row component
+// blocks (4 KB each) to their planes at `dst`.
+__device__ __forceinline__ void emit_block(const float2 (&acc)[4][4], bool ublk, const float *mx, __half *pk,
+                                           __half *dst, int ippitch, int tid, int ty, int tx) {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = ty + 16 * a, j = tx + 16 * b;
+            const int prow = ublk ? j : i, kidx = ublk ? i : j;
+            const float sc = efie_pow2_scale(mx[prow]);
+            const int chunk = kidx >> 5, kq = kidx & 31;
+            const int o = chunk * 4 * NB * 32 + (int)(efie_swz64(prow, kq) >> 1);
+            __half h, l;
+            const float vr = acc[a][b].x * sc, vi = acc[a][b].y * sc;
+            h = __float2half_rn(vr);
+            l = __float2half_rn(vr - __half2float(h));
+            pk[o] = h;
+            pk[o + NB * 32] = l;
+            h = __float2half_rn(vi);
+            l = __float2half_rn(vi - __half2float(h));
+            pk[o + 2 * NB * 32] = h;
+            pk[o + 3 * NB * 32] = l;
+        }
+    __syncthreads();
+    for (int e = tid; e < 8 * NB * 32 / 8; e += 256) {
+        const int blk = e / (NB * 32 / 8), q = e % (NB * 32 / 8);
+        reinterpret_cast<float4 *>(dst + (size_t)blk * ippitch * 32)[q] =
+            reinterpret_cast<const float4 *>(pk + blk * NB * 32)[q];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Panels: U12 = Linv * A12 (row panel) and L21 = A21 * Uinv (column panel).
 // One 64x64 tile per CTA, in place.  blockIdx.y: 0 row panel, 1 column panel;
-// blockIdx.z: frequency.  Thread (ty, tx) = (t / 16, t mod 16) computes rows
+// blockIdx.z: frequency.  Symmetric Z (sym): column panel CTAs only, each
+// also forming its tile of the row panel, U12 = Linv * A21^T.  Thread (ty, tx) = (t / 16, t mod 16) computes rows
 // ty + 16a and columns tx + 16b (a, b < 4): the 16 threads of a half-warp
 // read 16 consecutive complex entries of a shared-memory row, which is
 // conflict-free for 64-bit loads.  Tiles are loaded with float4 reads of
@@ -296,26 +357,32 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
                                                 float *__restrict__ lmax, float *__restrict__ umax,
                                                 size_t mstride, int nblk, __half *__restrict__ ipl,
                                                 __half *__restrict__ ipu, size_t ipstride, int ippitch,
-                                                int emit) {
+                                                int emit, int sym, int kend) {
     const int f = blockIdx.z;
     if (!active[f]) return;
+    // symmetric Z: the factorization keeps only the lower part; the column
+    // panel's tiles also form the row panel, U[k.., j] = L_kk^-1 A[j, k..]^T
     extern __shared__ float2 dyn[];
     float2(*M)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);               // the inverse
     float2(*T)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));  // the panel tile
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     const float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
     const int tid = threadIdx.x;
-    const bool rowp = blockIdx.y == 0;
+    const bool rowp = !sym && blockIdx.y == 0;
     const int off = k + kb + blockIdx.x * NB;
     if (off >= N) return;
     const int ext = min(NB, N - off);
-    const float4 *inv4 = reinterpret_cast<const float4 *>(rowp ? Linv : Uinv);   // 2 complex per float4
-    for (int e = tid; e < NB * NB / 2; e += 256) {
-        const float4 v = inv4[e];
-        const int i = (2 * e) / NB, j = (2 * e) % NB;
-        M[i][j] = make_float2(v.x, v.y);
-        M[i][j + 1] = make_float2(v.z, v.w);
-    }
+    const bool utrans = sym != 0;
+    auto load_inverse = [&](const float2 *src) {
+        const float4 *inv4 = reinterpret_cast<const float4 *>(src);   // 2 complex per float4
+        for (int e = tid; e < NB * NB / 2; e += 256) {
+            const float4 v = inv4[e];
+            const int i = (2 * e) / NB, j = (2 * e) % NB;
+            M[i][j] = make_float2(v.x, v.y);
+            M[i][j + 1] = make_float2(v.z, v.w);
+        }
+    };
+    load_inverse((rowp || utrans) ? Linv : Uinv);
     // tile rows: row panel rows k..k+kb (columns off..off+ext); column panel rows off..off+ext (columns k..k+kb)
     const int nrow = rowp ? kb : ext, ncol = rowp ? ext : kb;
     const size_t base = rowp ? (size_t)k * ld + off : (size_t)off * ld + k;
@@ -333,6 +400,61 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     }
     __syncthreads();
     const int ty = tid >> 4, tx = tid & 15;
+    if (utrans) {
+        // U[k + i][off + j] = sum_q Linv[i][q] T[j][q], with its column maxima
+        __shared__ float ured[NB][17];
+        float2 au[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) au[a][b] = make_float2(0.f, 0.f);
+#pragma unroll 4
+        for (int q = 0; q < NB; q++) {
+            float2 x[4], y[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                x[a] = M[ty + 16 * a][q];
+                y[a] = T[tx + 16 * a][q];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) cfma(au[a][b], x[a], y[b]);
+        }
+        float cm[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int i = ty + 16 * a, j = tx + 16 * b;
+                if (i < kb && j < ext) {
+                    const size_t o = (size_t)(k + i) * ld + off + j;
+                    Ar[o] = au[a][b].x;
+                    Ai[o] = au[a][b].y;
+                    cm[b] = fmaxf(cm[b], fmaxf(fabsf(au[a][b].x), fabsf(au[a][b].y)));
+                }
+            }
+#pragma unroll
+        for (int b = 0; b < 4; b++) ured[tx + 16 * b][ty] = cm[b];
+        __syncthreads();   // M is no longer read
+        __shared__ float umx[NB];
+        if (tid < NB) {
+            float m = 0.f;
+#pragma unroll
+            for (int q = 0; q < 16; q++) m = fmaxf(m, ured[tid][q]);
+            umx[tid] = m;
+            if (tid < ext) umax[mstride * f + (size_t)bi * ld + off + tid] = m;
+        }
+        if (emit && off < kend) {
+            // the U block inside the outer panel: operand of the panel chain's update
+            __syncthreads();
+            emit_block(au, true, umx, reinterpret_cast<__half *>(&M[0][0]),
+                       ipu + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
+        }
+        __syncthreads();
+        load_inverse(Uinv);
+        __syncthreads();
+    }
     float2 acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
@@ -402,41 +524,9 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
         }
     }
     if (!emit) return;
-    // the block as tensor-core operand of the panel chain's updates (K = 64):
-    // rows of L (columns of U) scaled by the power of two of their maximum,
-    // split into FP16 hi + lo, in the packed layout [chunk][re hi, re lo,
-    // im hi, im lo][row][32] with the 64-byte swizzle, staged in T's memory
-    __syncthreads();
-    __half *pk = reinterpret_cast<__half *>(&T[0][0]);   // 2 chunks x 4 components x 64 rows x 32: 32 KB
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const int i = ty + 16 * a, j = tx + 16 * b;
-            const int prow = rowp ? j : i, kidx = rowp ? i : j;
-            const float sc = efie_pow2_scale(mx[prow]);
-            const int chunk = kidx >> 5, kq = kidx & 31;
-            const int o = chunk * 4 * NB * 32 + (int)(efie_swz64(prow, kq) >> 1);
-            __half h, l;
-            const float vr = acc[a][b].x * sc, vi = acc[a][b].y * sc;
-            h = __float2half_rn(vr);
-            l = __float2half_rn(vr - __half2float(h));
-            pk[o] = h;
-            pk[o + NB * 32] = l;
-            h = __float2half_rn(vi);
-            l = __float2half_rn(vi - __half2float(h));
-            pk[o + 2 * NB * 32] = h;
-            pk[o + 3 * NB * 32] = l;
-        }
-    __syncthreads();
-    // eight 64-row component blocks (4 KB each) to their planes, at the pack
-    // row of this tile (rows / columns from k + kb on)
-    __half *dst = (rowp ? ipu : ipl) + ipstride * f + (size_t)(off - k - kb) * 32;
-    for (int e = tid; e < 8 * NB * 32 / 8; e += 256) {
-        const int blk = e / (NB * 32 / 8), q = e % (NB * 32 / 8);
-        reinterpret_cast<float4 *>(dst + (size_t)blk * ippitch * 32)[q] =
-            reinterpret_cast<const float4 *>(pk + blk * NB * 32)[q];
-    }
+    __syncthreads();   // T is no longer read: the staging of the pack
+    emit_block(acc, rowp, mx, reinterpret_cast<__half *>(&T[0][0]),
+               (rowp ? ipu : ipl) + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
 }
 
 // ---------------------------------------------------------------------------
@@ -678,9 +768,10 @@ __global__ void __launch_bounds__(1024) k_port(int N, const double2 *__restrict_
     }
 }
 
-__global__ void k_fill_c128(size_t n, double2 *__restrict__ dst, double2 v) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = v;
+// x_f = 0 for the active slots f (grid (N / 256, B)); the others keep theirs
+__global__ void k_zero_active(int N, double2 *__restrict__ x, const int *__restrict__ active) {
+    const int f = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (active[f] && i < N) x[(size_t)N * f + i] = make_double2(0.0, 0.0);
 }
 
 __global__ void k_init_ctl(int B, char *__restrict__ ctl, double bnorm, const int *__restrict__ active) {
@@ -789,6 +880,9 @@ struct OnStream {
 // low-priority stream after F_P, so F_{P+1} overlaps D_P^rest (they touch
 // disjoint parts of the matrix; D_P^next waits for D_{P-1}^rest, whose
 // region contains it).
+static int g_sym_lu_disabled = 0;
+extern "C" void efie_debug_disable_symmetric_lu(int disable) { g_sym_lu_disabled = disable; }
+
 efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, int nact) {
     cudaStream_t s0 = ctx->stream;
     KernelLog &log = ctx->log;
@@ -808,6 +902,13 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     EFIE_CUDA(cudaEventRecord(w.ev_start, s0));
     EFIE_CUDA(cudaStreamWaitEvent(w.hi, w.ev_start, 0));
     const int KB = w.kb_outer;
+    // symmetric Z: every update keeps the lower part only (and the outer
+    // panels' diagonal blocks); the diagonal blocks are factored from their
+    // lower triangle and the row panel is formed from the column panel's
+    // tiles, U[k.., j] = L_kk^-1 A[j, k..]^T, so that L and U follow from
+    // the same (lower) data
+    const bool sym = w.zsym && w.sym_lu && g_sym_lu_disabled != 1;
+    const bool symtri = sym && g_sym_lu_disabled != 2;
     bool rest_pending = false;   // ev_rest holds the record of the previous D^rest
     const PackView ipl = efie_inpanel_view(w, true), ipu = efie_inpanel_view(w, false);
     {
@@ -822,17 +923,21 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
                 const int s1 = k + kb, rest = N - s1;
                 const bool inpanel = s1 < Kend;
                 tok = log.begin(s);
-                k_diag_factor<<<B, 256, kDiagSmem, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active);
+                k_diag_factor<<<B, 256, kDiagSmem, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride, ctl, active,
+                                                        sym ? (g_sym_lu_disabled == 3 ? 2 : 1) : 0);
                 if (rest > 0) {
-                    dim3 pg((rest + NB - 1) / NB, 2, B);
+                    dim3 pg((rest + NB - 1) / NB, sym ? 1 : 2, B);
                     k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
                                                         active, w.lmax.as<float>(), w.umax.as<float>(), w.mstride,
                                                         w.nblk, w.ipL.as<__half>(), w.ipU.as<__half>(), ipl.stride,
-                                                        ipl.pitch, inpanel ? 1 : 0);
+                                                        ipl.pitch, inpanel ? 1 : 0, sym ? 1 : 0, Kend);
                 }
                 EFIE_CUDA(cudaGetLastError());
                 log.end(EFIE_K_PANEL, s, tok, 0.0, rest > 0 ? 2 : 1);
-                if (inpanel) {
+                if (inpanel && sym) {
+                    // every row below the block, the panel's remaining columns
+                    EFIE_TRY(efie_gemm_update(ctx, w, s1, N, s1, Kend, k, k, kb, nact, ipl, ipu));
+                } else if (inpanel) {
                     // rows of this panel below the block, every column to the right
                     EFIE_TRY(efie_gemm_update(ctx, w, s1, Kend, s1, N, k, k, kb, nact, ipl, ipu));
                     // rows below the panel, the panel's remaining columns
@@ -850,14 +955,19 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
             EFIE_CUDA(cudaEventRecord(w.ev_panel, s));
             // D_P^next on the critical stream, after D_{P-1}^rest
             if (rest_pending) EFIE_CUDA(cudaStreamWaitEvent(s, w.ev_rest, 0));
-            EFIE_TRY(efie_gemm_update(ctx, w, Kend, K1, Kend, N, K0, K0, K, nact, Lp, Up));
-            EFIE_TRY(efie_gemm_update(ctx, w, K1, N, Kend, K1, K0, K0, K, nact, Lp.at(K1 - Kend), Up));
+            if (symtri) {
+                // the next panel's columns (its diagonal block in full)
+                EFIE_TRY(efie_gemm_update(ctx, w, Kend, N, Kend, K1, K0, K0, K, nact, Lp, Up));
+            } else {
+                EFIE_TRY(efie_gemm_update(ctx, w, Kend, K1, Kend, N, K0, K0, K, nact, Lp, Up));
+                EFIE_TRY(efie_gemm_update(ctx, w, K1, N, Kend, K1, K0, K0, K, nact, Lp.at(K1 - Kend), Up));
+            }
             // D_P^rest on the low-priority stream, after F_P and the packs
             if (K1 < N) {
                 OnStream on_lo(ctx, w.lo);
                 EFIE_CUDA(cudaStreamWaitEvent(w.lo, w.ev_panel, 0));
                 EFIE_TRY(efie_gemm_update(ctx, w, K1, N, K1, N, K0, K0, K, nact, Lp.at(K1 - Kend),
-                                          Up.at(K1 - Kend)));
+                                          Up.at(K1 - Kend), symtri ? KB : 0));
                 EFIE_CUDA(cudaEventRecord(w.ev_rest, w.lo));
                 rest_pending = true;
             }
@@ -895,8 +1005,7 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
     for (int f = 0; f < B; f++) nact += active_host[f] ? 1 : 0;
     const double zbytes = 16.0 * (double)N * N, lubytes = 8.0 * (double)N * N;
     size_t tok = log.begin(s);
-    k_fill_c128<<<(unsigned)(((size_t)N * B + 255) / 256), 256, 0, s>>>((size_t)N * B, static_cast<double2 *>(x),
-                                                                        make_double2(0.0, 0.0));
+    k_zero_active<<<dim3((N + 255) / 256, B), 256, 0, s>>>(N, static_cast<double2 *>(x), w.active.as<int>());
     k_init_ctl<<<(B + 63) / 64, 64, 0, s>>>(B, ctl, bnorm, w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
     log.end(EFIE_K_OTHER, s, tok, 0.0, 2);
@@ -979,8 +1088,7 @@ efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm)
     cudaStream_t s = ctx->stream;
     const int N = w.N, B = w.B;
     size_t tok = ctx->log.begin(s);
-    k_fill_c128<<<(unsigned)(((size_t)N * B + 255) / 256), 256, 0, s>>>((size_t)N * B, static_cast<double2 *>(x),
-                                                                        make_double2(0.0, 0.0));
+    k_zero_active<<<dim3((N + 255) / 256, B), 256, 0, s>>>(N, static_cast<double2 *>(x), w.active.as<int>());
     k_init_ctl<<<(B + 63) / 64, 64, 0, s>>>(B, w.ctl.as<char>(), bnorm, w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
     ctx->log.end(EFIE_K_OTHER, s, tok, 0.0, 2);

@@ -52,6 +52,10 @@ struct SolveWork {
     // Z is bit-exactly symmetric (symmetric gather): matrix-vector products read
     // only its upper triangle (128 x 128 tiles, partial vectors in spart)
     bool zsym = false;
+    // with zsym, the complex64 LU is L D L^T from the lower part (about half
+    // the trailing-update work); false: the general LU (the retry of a
+    // frequency whose refinement missed its target)
+    bool sym_lu = true;
     // the assembly writes the complex64 planes of each batch itself (symmetric
     // gather): the factorization starts without converting Z
     bool planes_from_assembly = false;
@@ -113,7 +117,8 @@ efie_status efie_true_residual(efie_ctx *ctx, SolveWork &w, const void *Z, size_
 // efie_true_residual.
 efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, const void *b, double tol, void *rout,
                                  int nact);
-// x = 0 and fresh control blocks (||b|| = bnorm) for every slot.
+// x = 0 for the active slots (the others keep theirs) and fresh control
+// blocks (||b|| = bnorm) for every slot.
 efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
                              int ge, double V0, double Z0, void *out);
@@ -147,10 +152,15 @@ PackView efie_inpanel_view(const SolveWork &w, bool lower);
 // active frequency: on the tensor cores from the packed views Lv (rows r0..)
 // and Uv (columns c0..) when the block is large enough (K <= 256), else on
 // CUDA cores from the factors (efie_update_simt, K <= 64 per call).
+// tri_kb > 0 (a square block, r0 == c0): only the 256 x 256 tensor-core tiles
+// that reach the block's lower triangle at tri_kb granularity (column block
+// <= row block of width tri_kb, from r0), i.e. what a symmetric factorization
+// with outer panels of tri_kb columns still reads.
 efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
-                             int nact, const PackView &Lv, const PackView &Uv);
+                             int nact, const PackView &Lv, const PackView &Uv, int tri_kb = 0);
 // whether efie_gemm_update takes the tensor-core path for this block
 bool efie_gemm_uses_tc(int rows, int cols, int K);
 efie_status efie_update_simt(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0, int c1, int kcol, int krow, int K,
                              int nact);
 extern "C" void efie_debug_disable_tensor_cores(int disable);
+extern "C" void efie_debug_disable_symmetric_lu(int disable);

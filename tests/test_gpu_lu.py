@@ -54,3 +54,39 @@ def test_lu_efie_matrix():
     U = torch.triu(torch.from_numpy(tc.astype(np.complex64)))
     R = (L.cuda() @ U.cuda()).cpu().numpy()
     assert np.linalg.norm(R - Z) / np.linalg.norm(Z) <= 1e-5
+
+
+@pytest.mark.parametrize("lu_nb", [128, 256, 512])
+def test_lu_symmetric_matches_general(lu_nb):
+    """A bit-exactly symmetric Z (the symmetric gather's) is factored as
+    L D L^T: the trailing updates form only the lower part and the outer
+    panels' diagonal blocks, and the row panel comes from the lower part
+    transposed; the diagonal blocks are factored as L D L^T with
+    U^-1 = L^-T D^-1.  Its factors reproduce Z about as closely as the
+    general factorization's (within 4x of its worst entry), in the upper and
+    the lower triangle alike."""
+    nat = importlib.import_module("matlab-cuda-efief-vs-cpu_b200._native")
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    omega, k, _, _ = eo.physics(2.5e9, d.mu, d.eps)
+    Z = oc.assemble_z(p["rwg"], p["prepack"], k, omega, d.mu, d.eps)
+    Z = np.triu(Z) + np.triu(Z, 1).T
+    assert np.array_equal(Z, Z.T)
+    nat.lib().efie_debug_set_selftest_panel(lu_nb)
+    try:
+        sym = _lu(Z, True)
+        nat.lib().efie_debug_disable_symmetric_lu(1)
+        gen = _lu(Z, True)
+    finally:
+        nat.lib().efie_debug_disable_symmetric_lu(0)
+        nat.lib().efie_debug_set_selftest_panel(0)
+    n = Z.shape[0]
+    zmax = np.abs(Z).max()
+
+    def errs(LU):
+        E = np.abs((np.tril(LU, -1) + np.eye(n)) @ np.triu(LU) - Z) / zmax
+        return np.tril(E).max(), np.triu(E, 1).max()
+
+    es, eg = errs(sym), errs(gen)
+    assert max(eg) <= 5e-5
+    assert max(es) <= 4 * max(eg), (es, eg)
