@@ -372,7 +372,6 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     const int off = k + kb + blockIdx.x * NB;
     if (off >= N) return;
     const int ext = min(NB, N - off);
-    const bool utrans = sym != 0;
     auto load_inverse = [&](const float2 *src) {
         const float4 *inv4 = reinterpret_cast<const float4 *>(src);   // 2 complex per float4
         for (int e = tid; e < NB * NB / 2; e += 256) {
@@ -382,7 +381,7 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
             M[i][j + 1] = make_float2(v.z, v.w);
         }
     };
-    load_inverse((rowp || utrans) ? Linv : Uinv);
+    load_inverse((rowp || sym) ? Linv : Uinv);
     // tile rows: row panel rows k..k+kb (columns off..off+ext); column panel rows off..off+ext (columns k..k+kb)
     const int nrow = rowp ? kb : ext, ncol = rowp ? ext : kb;
     const size_t base = rowp ? (size_t)k * ld + off : (size_t)off * ld + k;
@@ -400,10 +399,15 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     }
     __syncthreads();
     const int ty = tid >> 4, tx = tid & 15;
-    if (utrans) {
-        // U[k + i][off + j] = sum_q Linv[i][q] T[j][q], with its column maxima
-        __shared__ float ured[NB][17];
-        float2 au[4][4];
+    if (sym) {
+        // U[k + i][off + j] = sum_q Linv[i][q] T[j][q] (T: rows off.. of the
+        // lower part), and with U^-1 = L^-T D^-1 the column panel follows
+        // from it exactly: L[off + j][k + i] = U[i][j] / d_i
+        __shared__ float ured[NB][17], lred[NB][17];
+        __shared__ float umx[NB], lmx[NB];
+        __shared__ float2 rdiag[NB];
+        if (tid < NB) rdiag[tid] = Uinv[tid * NB + tid];   // 1 / d_i
+        float2 au[4][4], al[4][4];
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -421,39 +425,59 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
 #pragma unroll
                 for (int b = 0; b < 4; b++) cfma(au[a][b], x[a], y[b]);
         }
-        float cm[4] = {0.f, 0.f, 0.f, 0.f};
+        __syncthreads();   // M, T and rdiag: M and T are free from here
+        float cu[4] = {0.f, 0.f, 0.f, 0.f}, cl[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int b = 0; b < 4; b++) {
                 const int i = ty + 16 * a, j = tx + 16 * b;
+                al[a][b] = cmulf(au[a][b], rdiag[i]);
+                T[j][i] = al[a][b];   // L tile, row j
                 if (i < kb && j < ext) {
                     const size_t o = (size_t)(k + i) * ld + off + j;
                     Ar[o] = au[a][b].x;
                     Ai[o] = au[a][b].y;
-                    cm[b] = fmaxf(cm[b], fmaxf(fabsf(au[a][b].x), fabsf(au[a][b].y)));
+                    cu[b] = fmaxf(cu[b], fmaxf(fabsf(au[a][b].x), fabsf(au[a][b].y)));
+                    cl[b] = fmaxf(cl[b], fmaxf(fabsf(al[a][b].x), fabsf(al[a][b].y)));
                 }
             }
 #pragma unroll
-        for (int b = 0; b < 4; b++) ured[tx + 16 * b][ty] = cm[b];
-        __syncthreads();   // M is no longer read
-        __shared__ float umx[NB];
-        if (tid < NB) {
-            float m = 0.f;
-#pragma unroll
-            for (int q = 0; q < 16; q++) m = fmaxf(m, ured[tid][q]);
-            umx[tid] = m;
-            if (tid < ext) umax[mstride * f + (size_t)bi * ld + off + tid] = m;
+        for (int b = 0; b < 4; b++) {
+            ured[tx + 16 * b][ty] = cu[b];
+            lred[tx + 16 * b][ty] = cl[b];
         }
-        if (emit && off < kend) {
-            // the U block inside the outer panel: operand of the panel chain's update
-            __syncthreads();
+        __syncthreads();
+        // L rows off.. (columns k..k+kb): consecutive threads, consecutive columns
+        for (int e = tid; e < NB * NB; e += 256) {
+            const int r = e >> 6, c = e & (NB - 1);
+            if (r < ext && c < kb) {
+                const size_t o = (size_t)(off + r) * ld + k + c;
+                Ar[o] = T[r][c].x;
+                Ai[o] = T[r][c].y;
+            }
+        }
+        if (tid < NB) {
+            float mu = 0.f, ml = 0.f;
+#pragma unroll
+            for (int q = 0; q < 16; q++) mu = fmaxf(mu, ured[tid][q]), ml = fmaxf(ml, lred[tid][q]);
+            umx[tid] = mu;
+            lmx[tid] = ml;
+            if (tid < ext) {
+                umax[mstride * f + (size_t)bi * ld + off + tid] = mu;
+                lmax[mstride * f + (size_t)(off + tid) * nblk + bi] = ml;
+            }
+        }
+        __syncthreads();   // T (the L staging) is free
+        if (!emit) return;
+        // operands of the panel chain's update: L rows (columns of the U
+        // tile) always, the U block when its columns lie inside the panel
+        emit_block(al, true, lmx, reinterpret_cast<__half *>(&T[0][0]),
+                   ipl + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
+        if (off < kend)
             emit_block(au, true, umx, reinterpret_cast<__half *>(&M[0][0]),
                        ipu + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
-        }
-        __syncthreads();
-        load_inverse(Uinv);
-        __syncthreads();
+        return;
     }
     float2 acc[4][4];
 #pragma unroll
