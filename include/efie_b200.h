@@ -316,6 +316,12 @@ void efie_debug_disable_symmetric_lu(int disable);
  * symmetric factorization unless efie_debug_disable_symmetric_lu(1). */
 void efie_debug_set_selftest_panel(int lu_nb);
 
+/* 1 makes efie_plan_run take its batches in frequency order with every
+ * refinement starting from zero, instead of coarse to fine with initial
+ * guesses interpolated from the solved neighbours (mixed solver, GMRES, more
+ * than one batch), process-wide.  No counterpart in the reference. */
+void efie_debug_disable_warm_start(int disable);
+
 /* ---------------------------------------------------------------------- */
 /* Centroid assembly without device allocation                             */
 /* ---------------------------------------------------------------------- */

@@ -116,6 +116,7 @@ SIGNATURES = {
     "efie_debug_disable_tensor_cores": (None, [C.c_int]),
     "efie_debug_disable_symmetric_lu": (None, [C.c_int]),
     "efie_debug_set_selftest_panel": (None, [C.c_int]),
+    "efie_debug_disable_warm_start": (None, [C.c_int]),
     "efie_gassemble_zv_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_int32] + [_P] * 12 +
                                   [c128, C.c_double, C.c_double, c128, c_double_p, _P, _P]),
     "efie_mlp_config_default": (None, [_P]),

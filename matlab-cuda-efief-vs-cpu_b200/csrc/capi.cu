@@ -404,6 +404,7 @@ struct efie_plan {
     std::vector<int32_t> hF, hpt, hmt, hps, hms;
     efie_mesh cmesh{};
     DevBuf Z, b, x, wport, out, scratch, ipiv, info, lwork;
+    DevBuf xall;   // solutions of a sweep by sorted frequency (initial guesses of later batches)
     int lwork_elems = -1;
     SolveWork sw;
     // the mixed factorization as a CUDA graph (captured on the first untimed
@@ -601,6 +602,9 @@ extern "C" void efie_plan_destroy(efie_plan *p) {
     delete p;
 }
 
+static bool g_warm_start_disabled = false;
+extern "C" void efie_debug_disable_warm_start(int disable) { g_warm_start_disabled = disable != 0; }
+
 extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t Nf, efie_c128 *Zin, efie_c128 *S11,
                                      efie_c128 *I, efie_sweep_stats *st) {
     if (!p) return efie_fail(EFIE_ERR_ARGS, "null plan");
@@ -624,15 +628,48 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     const bool mixed = p->opts.solver == EFIE_SOLVER_MIXED;
     const int B = p->B;
     efie_status rc = EFIE_OK;
-    for (int f0 = 0; f0 < Nf && rc == EFIE_OK; f0 += B) {
-        const int nb = std::min(B, Nf - f0);
+    // as few batches as B allows, of balanced sizes (each batch pays the
+    // latency of its panel chain once).  The mixed solver with GMRES takes
+    // them coarse to fine: batch b holds the frequencies at sorted positions
+    // q = r_b (mod nbat), residues in van der Corput order, so every later
+    // frequency starts its refinement from the interpolation of its solved
+    // neighbours instead of from zero.
+    const int nbat = (Nf + B - 1) / B;
+    const bool warm = mixed && !p->centroid && nbat > 1 && p->opts.refine_method == EFIE_REFINE_GMRES &&
+                      !g_warm_start_disabled;
+    std::vector<int> ord(Nf), bstart(nbat + 1, 0), posq(Nf);   // processing index -> original, sorted position
+    std::vector<double> fsorted(Nf);
+    std::vector<char> solved(Nf, 0);
+    {
+        std::vector<int> srt(Nf);
+        for (int i = 0; i < Nf; i++) srt[i] = i;
+        if (warm) std::stable_sort(srt.begin(), srt.end(), [&](int a, int b) { return freqs[a] < freqs[b]; });
+        for (int i = 0; i < Nf; i++) fsorted[i] = freqs[srt[i]];
+        int n = 0, P = 1, bits = 0;
+        while (P < nbat) P <<= 1, bits++;
+        for (int i = 0, b = 0; i < (warm ? P : nbat); i++) {
+            if (warm) {
+                int r = 0;
+                for (int t = 0; t < bits; t++) r |= ((i >> t) & 1) << (bits - 1 - t);
+                if (r >= nbat) continue;
+                for (int q = r; q < Nf; q += nbat) posq[n] = q, ord[n++] = srt[q];
+            } else {
+                const int nb = Nf / nbat + (b < Nf % nbat ? 1 : 0);
+                for (int f = 0; f < nb; f++) posq[n] = n, ord[n] = srt[n], n++;
+            }
+            bstart[++b] = n;
+        }
+    }
+    if (warm) EFIE_TRY(p->xall.reserve(sizeof(efie_c128) * (size_t)N * Nf));
+    for (int bi = 0; bi < nbat && rc == EFIE_OK; bi++) {
+        const int f0 = bstart[bi], nb = bstart[bi + 1] - f0;
         int active[EFIE_MAX_BATCH] = {0};
         for (int f = 0; f < nb; f++) active[f] = 1;
         {
             Physics ph[EFIE_MAX_BATCH];
             void *Zf[EFIE_MAX_BATCH];
             for (int f = 0; f < nb; f++) {
-                ph[f] = efie_physics(freqs[f0 + f], p->mu, p->eps);
+                ph[f] = efie_physics(freqs[ord[f0 + f]], p->mu, p->eps);
                 Zf[f] = p->Z.as<efie_c128>() + NN * f;
             }
             if (p->centroid) {
@@ -649,12 +686,34 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             rc = plan_factor(p, active, nb);
             if (rc != EFIE_OK) break;
             RefineResult rr;
+            const bool guess = warm && bi > 0;
+            if (guess) {
+                // linear in frequency between the nearest solved neighbours
+                // (the nearest one alone at the ends of the band)
+                GuessSpec g;
+                for (int f = 0; f < nb; f++) {
+                    const int q = posq[f0 + f];
+                    int l = q - 1, r = q + 1;
+                    while (l >= 0 && !solved[l]) l--;
+                    while (r < Nf && !solved[r]) r++;
+                    if (l < 0) l = r, r = Nf;
+                    g.il[f] = l;
+                    g.ir[f] = r < Nf ? r : -1;
+                    g.wl[f] = 1.0, g.wr[f] = 0.0;
+                    if (r < Nf && fsorted[r] > fsorted[l]) {
+                        g.wr[f] = (fsorted[q] - fsorted[l]) / (fsorted[r] - fsorted[l]);
+                        g.wl[f] = 1.0 - g.wr[f];
+                    }
+                }
+                rc = efie_interp_guess(ctx, N, nb, p->x.p, p->xall.p, g);
+                if (rc != EFIE_OK) break;
+            }
             if (p->opts.refine_method == EFIE_REFINE_CLASSICAL)
                 rc = efie_mixed_refine(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
                                        p->opts.refine_max_iter, active, &rr);
             else
                 rc = efie_mixed_gmres(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
-                                      p->opts.refine_max_iter, active, &rr);
+                                      p->opts.refine_max_iter, active, &rr, guess);
             if (rc != EFIE_OK) break;
             S->refine_iters_max = std::max(S->refine_iters_max, rr.iters);
             if (p->sw.zsym && p->sw.sym_lu && p->opts.refine_method == EFIE_REFINE_GMRES) {
@@ -704,9 +763,17 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                               p->centroid ? EFIE_PORT_EDGE_DIFF : p->opts.port_model, p->pe - 1, p->ge - 1, p->V0,
                               p->Z0, p->out.as<efie_c128>() + 2 * f0);
         if (rc != EFIE_OK) break;
-        if (I) {
-            cudaError_t e = cudaMemcpyAsync(I + (size_t)f0 * N, p->x.p, sizeof(efie_c128) * N * nb,
-                                            cudaMemcpyDeviceToHost, ctx->stream);
+        for (int f = 0; f < nb && rc == EFIE_OK; f++) {
+            const efie_c128 *xf = p->x.as<efie_c128>() + (size_t)N * f;
+            cudaError_t e = cudaSuccess;
+            if (warm) {
+                solved[posq[f0 + f]] = 1;
+                e = cudaMemcpyAsync(p->xall.as<efie_c128>() + (size_t)N * posq[f0 + f], xf, sizeof(efie_c128) * N,
+                                    cudaMemcpyDeviceToDevice, ctx->stream);
+            }
+            if (I && e == cudaSuccess)
+                e = cudaMemcpyAsync(I + (size_t)ord[f0 + f] * N, xf, sizeof(efie_c128) * N, cudaMemcpyDeviceToHost,
+                                    ctx->stream);
             if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
         }
     }
@@ -721,15 +788,15 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         if (e != cudaSuccess) rc = efie_fail(EFIE_ERR_CUDA, cudaGetErrorString(e));
         else {
             for (int fi = 0; fi < Nf; fi++) {
-                Zin[fi] = res[2 * fi];
-                S11[fi] = res[2 * fi + 1];
+                Zin[ord[fi]] = res[2 * fi];
+                S11[ord[fi]] = res[2 * fi + 1];
             }
+            int bad = -1;
             for (int fi = 0; fi < Nf; fi++)
-                if (info[fi] != 0) {
-                    rc = efie_fail(EFIE_ERR_SINGULAR, "Z is singular at frequency index " + std::to_string(fi + 1) +
-                                                          " (getrf info " + std::to_string(info[fi]) + ").");
-                    break;
-                }
+                if (info[fi] != 0 && (bad < 0 || ord[fi] < ord[bad])) bad = fi;
+            if (bad >= 0)
+                rc = efie_fail(EFIE_ERR_SINGULAR, "Z is singular at frequency index " + std::to_string(ord[bad] + 1) +
+                                                      " (getrf info " + std::to_string(info[bad]) + ").");
         }
     } else {
         cudaStreamSynchronize(ctx->stream);

@@ -475,7 +475,8 @@ efie_status gm_workspace(SolveWork &w) {
 }  // namespace
 
 efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
-                             double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res) {
+                             double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res,
+                             bool x0_given) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int N = w.N, B = w.B;
@@ -500,8 +501,8 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
         log.end(EFIE_K_RESIDUAL, s, tk, 8.0 * (double)N * N * nact, 2);
         return efie_residual_finish(ctx, w, wv, b, tol, V, nact);
     };
-    EFIE_TRY(efie_refine_init(ctx, w, x, bnorm));
-    // r0 = b (x = 0): the residual also stores it at V slot 0
+    EFIE_TRY(efie_refine_init(ctx, w, x, bnorm, !x0_given));
+    // r0 = b - Z x0 (b for x0 = 0): the residual also stores it at V slot 0
     EFIE_TRY(residual());
     std::vector<char> hctl(64 * (size_t)B);
     std::vector<int> hstop(B);

@@ -1108,14 +1108,39 @@ efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, con
     return EFIE_OK;
 }
 
-efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm) {
+efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm, bool zero_x) {
     cudaStream_t s = ctx->stream;
     const int N = w.N, B = w.B;
     size_t tok = ctx->log.begin(s);
-    k_zero_active<<<dim3((N + 255) / 256, B), 256, 0, s>>>(N, static_cast<double2 *>(x), w.active.as<int>());
+    if (zero_x)
+        k_zero_active<<<dim3((N + 255) / 256, B), 256, 0, s>>>(N, static_cast<double2 *>(x), w.active.as<int>());
     k_init_ctl<<<(B + 63) / 64, 64, 0, s>>>(B, w.ctl.as<char>(), bnorm, w.active.as<int>());
     EFIE_CUDA(cudaGetLastError());
-    ctx->log.end(EFIE_K_OTHER, s, tok, 0.0, 2);
+    ctx->log.end(EFIE_K_OTHER, s, tok, 0.0, zero_x ? 2 : 1);
+    return EFIE_OK;
+}
+
+namespace {
+__global__ void k_interp_guess(int N, double2 *__restrict__ x, const double2 *__restrict__ xs, GuessSpec g) {
+    const int f = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double2 a = xs[(size_t)N * g.il[f] + i];
+    double2 v = a;
+    if (g.ir[f] >= 0) {
+        const double2 c = xs[(size_t)N * g.ir[f] + i];
+        v = make_double2(g.wl[f] * a.x + g.wr[f] * c.x, g.wl[f] * a.y + g.wr[f] * c.y);
+    }
+    x[(size_t)N * f + i] = v;
+}
+}  // namespace
+
+efie_status efie_interp_guess(efie_ctx *ctx, int N, int n, void *x, const void *xs, const GuessSpec &g) {
+    if (n <= 0) return EFIE_OK;
+    size_t tok = ctx->log.begin(ctx->stream);
+    k_interp_guess<<<dim3((N + 255) / 256, n), 256, 0, ctx->stream>>>(N, static_cast<double2 *>(x),
+                                                                     static_cast<const double2 *>(xs), g);
+    EFIE_CUDA(cudaGetLastError());
+    ctx->log.end(EFIE_K_OTHER, ctx->stream, tok, 0.0);
     return EFIE_OK;
 }
 

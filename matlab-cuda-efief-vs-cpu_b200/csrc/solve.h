@@ -106,8 +106,10 @@ efie_status efie_mixed_refine(efie_ctx *ctx, SolveWork &w, const void *Z, size_t
 // Flexible GMRES on Z x = b with the complex64 LU as right preconditioner;
 // the Arnoldi process and every vector are complex128.  Same contract as
 // efie_mixed_refine (x starts at 0; res->iters counts matrix-vector products).
+// x0_given: the active slots of x hold initial guesses (x = 0 otherwise).
 efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const void *b, void *x,
-                             double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res);
+                             double bnorm, double tol, int max_iter, const int *active_host, RefineResult *res,
+                             bool x0_given = false);
 // r = b - Z x for every frequency of the batch (complex128), its complex64
 // copy in w.vec, ||r|| / ||b|| and the convergence flags in w.ctl; r is also
 // stored at rout + N f when rout is not null.
@@ -119,7 +121,14 @@ efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, con
                                  int nact);
 // x = 0 for the active slots (the others keep theirs) and fresh control
 // blocks (||b|| = bnorm) for every slot.
-efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm);
+efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm, bool zero_x = true);
+// x_f = wl_f xs[il_f] + wr_f xs[ir_f] for the slots f < n (complex128
+// vectors of N; ir_f < 0: x_f = xs[il_f]).
+struct GuessSpec {
+    int il[EFIE_MAX_BATCH], ir[EFIE_MAX_BATCH];
+    double wl[EFIE_MAX_BATCH], wr[EFIE_MAX_BATCH];
+};
+efie_status efie_interp_guess(efie_ctx *ctx, int N, int n, void *x, const void *xs, const GuessSpec &g);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
                              int ge, double V0, double Z0, void *out);
 

@@ -208,3 +208,36 @@ def test_graph_replay_matches_eager_launches():
     # other neighbours (e^{-jk_f R} by recurrence from the group's first
     # frequency): Z moves in its last bits, Zin within the GMRES tolerance
     assert np.abs(Zg2 - Zg[::-1]).max() <= 1e-8 * np.abs(Zg).max()
+
+
+def test_coarse_to_fine_batches_with_interpolated_guesses():
+    """Several batches of the mixed solver run coarse to fine (sorted
+    positions by residue, van der Corput order) and start GMRES from the
+    interpolation of solved neighbours.  Unsorted input frequencies come back
+    in their own order, currents included, and match the same sweep with
+    every refinement started from zero and the oracle."""
+    m = pkg()
+    nat = __import__(m.__name__ + "._native", fromlist=["x"])
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    r = p["rwg"]
+    args = [p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"], r["rm"],
+            r["Ap"], r["Am"], r["len"], p["prepack"], d.mu, d.eps, p["patchEdge"], p["groundEdge"], d.V0, p["spread"],
+            d.Z0]
+    freqs = np.linspace(d.freqs[0], d.freqs[-1], 13)
+    perm = np.random.default_rng(5).permutation(len(freqs))
+    plan = m.SweepPlan(*args, opts=m.sweep_opts(batch=3))
+    Zw, Sw, Iw = plan.run(freqs[perm], return_currents=True)
+    nat.lib().efie_debug_disable_warm_start(1)
+    try:
+        Zc, Sc, Ic = plan.run(freqs, return_currents=True)
+    finally:
+        nat.lib().efie_debug_disable_warm_start(0)
+    plan.close()
+    assert (np.abs(Zw - Zc[perm]) / np.abs(Zc[perm])).max() <= 1e-7
+    Zo, _ = _oracle(p, freqs[perm])
+    assert (np.abs(Zw - Zo) / np.abs(Zo)).max() <= 1e-6
+    for j in (0, 7, 12):
+        omega, k, _, _ = eo.physics(freqs[perm[j]], d.mu, d.eps)
+        Z = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
+        assert np.linalg.norm(p["b"] - Z @ Iw[:, j]) / np.linalg.norm(p["b"]) < 1e-9
