@@ -602,6 +602,42 @@ extern "C" void efie_plan_destroy(efie_plan *p) {
     delete p;
 }
 
+// Initial guess of the frequency at sorted position q: the Lagrange
+// interpolant in frequency through the (up to) three nearest solved
+// neighbours, the two nearest on one side and one on the other where both
+// sides have some (a quadratic through points 1-2 grid steps away), else the
+// nearest one or two on the one side.
+static void guess_weights(int q, const std::vector<double> &fs, const std::vector<char> &solved, GuessSpec &g,
+                          int f) {
+    const int Nf = (int)fs.size();
+    int nodes[3], n = 0;
+    int l = q - 1, r = q + 1;
+    auto next_l = [&]() { while (l >= 0 && !solved[l]) l--; };
+    auto next_r = [&]() { while (r < Nf && !solved[r]) r++; };
+    next_l();
+    next_r();
+    while (n < 3 && (l >= 0 || r < Nf)) {
+        const bool take_l = l >= 0 && (r >= Nf || q - l <= r - q);
+        if (take_l) nodes[n++] = l--, next_l();
+        else nodes[n++] = r++, next_r();
+    }
+    for (int t = 0; t < 3; t++) g.idx[t][f] = -1, g.w[t][f] = 0.0;
+    // one-sided nodes: keep the nearest only (no extrapolation)
+    bool below = false, above = false;
+    for (int t = 0; t < n; t++) (nodes[t] < q ? below : above) = true;
+    if (!(below && above)) n = std::min(n, 1);
+    for (int t = 0; t < n; t++)
+        for (int u = 0; u < t; u++)
+            if (fs[nodes[t]] == fs[nodes[u]]) n = 1;   // repeated frequencies: the nearest alone
+    for (int t = 0; t < n; t++) {
+        double w = 1.0;
+        for (int u = 0; u < n; u++)
+            if (u != t) w *= (fs[q] - fs[nodes[u]]) / (fs[nodes[t]] - fs[nodes[u]]);
+        g.idx[t][f] = nodes[t];
+        g.w[t][f] = w;
+    }
+}
+
 static bool g_warm_start_disabled = false;
 extern "C" void efie_debug_disable_warm_start(int disable) { g_warm_start_disabled = disable != 0; }
 
@@ -688,23 +724,8 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
             RefineResult rr;
             const bool guess = warm && bi > 0;
             if (guess) {
-                // linear in frequency between the nearest solved neighbours
-                // (the nearest one alone at the ends of the band)
                 GuessSpec g;
-                for (int f = 0; f < nb; f++) {
-                    const int q = posq[f0 + f];
-                    int l = q - 1, r = q + 1;
-                    while (l >= 0 && !solved[l]) l--;
-                    while (r < Nf && !solved[r]) r++;
-                    if (l < 0) l = r, r = Nf;
-                    g.il[f] = l;
-                    g.ir[f] = r < Nf ? r : -1;
-                    g.wl[f] = 1.0, g.wr[f] = 0.0;
-                    if (r < Nf && fsorted[r] > fsorted[l]) {
-                        g.wr[f] = (fsorted[q] - fsorted[l]) / (fsorted[r] - fsorted[l]);
-                        g.wl[f] = 1.0 - g.wr[f];
-                    }
-                }
+                for (int f = 0; f < nb; f++) guess_weights(posq[f0 + f], fsorted, solved, g, f);
                 rc = efie_interp_guess(ctx, N, nb, p->x.p, p->xall.p, g);
                 if (rc != EFIE_OK) break;
             }

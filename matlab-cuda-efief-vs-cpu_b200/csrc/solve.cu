@@ -1124,11 +1124,13 @@ namespace {
 __global__ void k_interp_guess(int N, double2 *__restrict__ x, const double2 *__restrict__ xs, GuessSpec g) {
     const int f = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const double2 a = xs[(size_t)N * g.il[f] + i];
-    double2 v = a;
-    if (g.ir[f] >= 0) {
-        const double2 c = xs[(size_t)N * g.ir[f] + i];
-        v = make_double2(g.wl[f] * a.x + g.wr[f] * c.x, g.wl[f] * a.y + g.wr[f] * c.y);
+    double2 v = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+        if (g.idx[t][f] < 0) continue;
+        const double2 a = xs[(size_t)N * g.idx[t][f] + i];
+        v.x += g.w[t][f] * a.x;
+        v.y += g.w[t][f] * a.y;
     }
     x[(size_t)N * f + i] = v;
 }

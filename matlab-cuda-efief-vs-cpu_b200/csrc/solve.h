@@ -122,11 +122,11 @@ efie_status efie_residual_finish(efie_ctx *ctx, SolveWork &w, const void *y, con
 // x = 0 for the active slots (the others keep theirs) and fresh control
 // blocks (||b|| = bnorm) for every slot.
 efie_status efie_refine_init(efie_ctx *ctx, SolveWork &w, void *x, double bnorm, bool zero_x = true);
-// x_f = wl_f xs[il_f] + wr_f xs[ir_f] for the slots f < n (complex128
-// vectors of N; ir_f < 0: x_f = xs[il_f]).
+// x_f = sum_t w[t][f] xs[idx[t][f]] over the terms t < 3 with idx >= 0, for
+// the slots f < n (complex128 vectors of N).
 struct GuessSpec {
-    int il[EFIE_MAX_BATCH], ir[EFIE_MAX_BATCH];
-    double wl[EFIE_MAX_BATCH], wr[EFIE_MAX_BATCH];
+    int idx[3][EFIE_MAX_BATCH];
+    double w[3][EFIE_MAX_BATCH];
 };
 efie_status efie_interp_guess(efie_ctx *ctx, int N, int n, void *x, const void *xs, const GuessSpec &g);
 efie_status efie_port_reduce(efie_ctx *ctx, int N, int B, const void *x, const double *wport, int model, int pe,
