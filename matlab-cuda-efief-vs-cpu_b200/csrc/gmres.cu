@@ -444,6 +444,12 @@ __global__ void __launch_bounds__(ST) k_symv_reduce(int N, int nb, const double2
 
 inline unsigned cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
+// the stop flags of the batch in one array (one read-back per poll)
+__global__ void k_gm_stop_flags(int B, const GmState *__restrict__ st, int *__restrict__ out) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < B) out[f] = st[f].stop;
+}
+
 efie_status symv(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const double2 *x, double2 *y,
                  const int *flags, int fstride) {
     const int nb = (w.N + ST - 1) / ST;
@@ -465,6 +471,7 @@ efie_status gm_workspace(SolveWork &w) {
     EFIE_TRY(w.gw.reserve(sizeof(double2) * NB));
     EFIE_TRY(w.gpart.reserve(sizeof(double2) * (size_t)w.B * w.gnch * (GM_M + 1) + sizeof(double) * w.B * w.gnch));
     EFIE_TRY(w.gst.reserve(sizeof(GmState) * w.B));
+    EFIE_TRY(w.gflags.reserve(sizeof(int) * w.B));
     if (w.zsym) {
         const int nb = (w.N + ST - 1) / ST;
         EFIE_TRY(w.spart.reserve(sizeof(double2) * ((size_t)nb * (nb + 1) / 2) * 2 * ST * w.B));
@@ -502,8 +509,13 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
         return efie_residual_finish(ctx, w, wv, b, tol, V, nact);
     };
     EFIE_TRY(efie_refine_init(ctx, w, x, bnorm, !x0_given));
-    // r0 = b - Z x0 (b for x0 = 0): the residual also stores it at V slot 0
-    EFIE_TRY(residual());
+    // r0 = b - Z x0, stored at V slot 0 too; for x0 = 0 without the product
+    if (x0_given || !w.zsym) {
+        EFIE_TRY(residual());
+    } else {
+        EFIE_CUDA(cudaMemsetAsync(wv, 0, sizeof(double2) * (size_t)N * B, s));
+        EFIE_TRY(efie_residual_finish(ctx, w, wv, b, tol, V, nact));
+    }
     std::vector<char> hctl(64 * (size_t)B);
     std::vector<int> hstop(B);
     int matvecs = 0;
@@ -547,9 +559,11 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
                 // a poll costs one synchronisation (tens of us) against a step
                 // of the whole batch (milliseconds at large N)
                 bool all_stop = true;
-                for (int f = 0; f < B; f++) {
-                    EFIE_CUDA(cudaMemcpyAsync(&hstop[f], &st[f].stop, sizeof(int), cudaMemcpyDeviceToHost, s));
-                }
+                tok = log.begin(s);
+                k_gm_stop_flags<<<cdiv(B, 32), 32, 0, s>>>(B, st, w.gflags.as<int>());
+                EFIE_CUDA(cudaGetLastError());
+                log.end(EFIE_K_OTHER, s, tok, 0.0);
+                EFIE_CUDA(cudaMemcpyAsync(hstop.data(), w.gflags.p, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
                 EFIE_CUDA(cudaStreamSynchronize(s));
                 for (int f = 0; f < B; f++)
                     if (active_host[f] && !hstop[f]) all_stop = false;

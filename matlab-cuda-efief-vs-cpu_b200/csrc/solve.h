@@ -47,7 +47,7 @@ struct SolveWork {
     // flexible GMRES (gmres.cu): Krylov basis V [M+1][B][N] and preconditioned
     // vectors Zm [M][B][N] in complex128, the new vector w [B][N], partial
     // sums and per-frequency Arnoldi state
-    DevBuf gV, gZ, gw, gpart, gst;
+    DevBuf gV, gZ, gw, gpart, gst, gflags;
     int gnch = 0;          // row chunks of the orthogonalisation kernels
     // Z is bit-exactly symmetric (symmetric gather): matrix-vector products read
     // only its upper triangle (128 x 128 tiles, partial vectors in spart)
