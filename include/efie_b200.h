@@ -307,8 +307,11 @@ efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32
 void efie_debug_disable_tensor_cores(int disable);
 
 /* 1 makes the mixed LU of a symmetric Z factor it as a general matrix
- * (every trailing update over the full block) instead of L D L^T with U
- * formed from L, process-wide.  No counterpart in the reference. */
+ * (every trailing update over the full block) instead of L D L^T from the
+ * lower part, process-wide.  Diagnostic modes: 2 keeps L D L^T but updates
+ * the full trailing blocks; 3 factors the diagonal blocks as general
+ * matrices (from their lower triangle) with separately inverted factors.
+ * 0 restores the default.  No counterpart in the reference. */
 void efie_debug_disable_symmetric_lu(int disable);
 
 /* Outer panel width of efie_lu_selftest: 64/128/256/512 (anything else:
