@@ -343,8 +343,9 @@ __device__ __forceinline__ void emit_block(const float2 (&acc)[4][4], bool ublk,
 // ---------------------------------------------------------------------------
 // Panels: U12 = Linv * A12 (row panel) and L21 = A21 * Uinv (column panel).
 // One 64x64 tile per CTA, in place.  blockIdx.y: 0 row panel, 1 column panel;
-// blockIdx.z: frequency.  Symmetric Z (sym): column panel CTAs only, each
-// also forming its tile of the row panel, U12 = Linv * A21^T.  Thread (ty, tx) = (t / 16, t mod 16) computes rows
+// blockIdx.z: frequency.  Symmetric Z (sym): one CTA per tile of the column
+// panel forms U12 = Linv * A21^T and from it L21 = U12^T D^-1.  Thread
+// (ty, tx) = (t / 16, t mod 16) computes rows
 // ty + 16a and columns tx + 16b (a, b < 4): the 16 threads of a half-warp
 // read 16 consecutive complex entries of a shared-memory row, which is
 // conflict-free for 64-bit loads.  Tiles are loaded with float4 reads of
@@ -360,8 +361,6 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
                                                 int emit, int sym, int kend) {
     const int f = blockIdx.z;
     if (!active[f]) return;
-    // symmetric Z: the factorization keeps only the lower part; the column
-    // panel's tiles also form the row panel, U[k.., j] = L_kk^-1 A[j, k..]^T
     extern __shared__ float2 dyn[];
     float2(*M)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);               // the inverse
     float2(*T)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));  // the panel tile
