@@ -241,3 +241,36 @@ def test_coarse_to_fine_batches_with_interpolated_guesses():
         omega, k, _, _ = eo.physics(freqs[perm[j]], d.mu, d.eps)
         Z = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
         assert np.linalg.norm(p["b"] - Z @ Iw[:, j]) / np.linalg.norm(p["b"]) < 1e-9
+
+
+def test_asymmetric_near_matrix_sweep_in_batches():
+    """A nearMat that is not symmetric keeps the general gather, the general
+    LU and the full GMRES products; several warm-started batches still match
+    the oracle."""
+    p = eo.build_problem(small_design("grid"))
+    pre = dict(p["prepack"])
+    nm = pre["nearMat"].copy()
+    i, j = np.nonzero(np.triu(nm, 1))
+    nm[i[0], j[0]] = 0
+    pre["nearMat"] = np.asfortranarray(nm)
+    p = dict(p, prepack=pre)
+    d = p["design"]
+    freqs = np.linspace(d.freqs[0], d.freqs[-1], 7)
+    Zin, _, st = _sweep(p, freqs, "mixed", batch=2)
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zin - Zo) / np.abs(Zo)).max() <= 1e-6
+    assert st["n_fp64_fallback"] == 0 and st["max_relres"] <= 1e-10
+
+
+def test_repeated_frequencies_in_warm_started_sweep():
+    """Repeated frequencies (the interpolation then takes the nearest solved
+    one) give the same Zin as their first occurrence."""
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    f = np.linspace(d.freqs[0], d.freqs[-1], 5)
+    freqs = np.array([f[0], f[2], f[2], f[4], f[1], f[1], f[3]])
+    Zin, _, st = _sweep(p, freqs, "mixed", batch=2)
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zin - Zo) / np.abs(Zo)).max() <= 1e-6
+    assert abs(Zin[1] - Zin[2]) <= 1e-7 * abs(Zin[1]) and abs(Zin[4] - Zin[5]) <= 1e-7 * abs(Zin[4])
+    assert st["n_fp64_fallback"] == 0
