@@ -90,3 +90,24 @@ def test_lu_symmetric_matches_general(lu_nb):
     es, eg = errs(sym), errs(gen)
     assert max(eg) <= 5e-5
     assert max(es) <= 4 * max(eg), (es, eg)
+
+
+@pytest.mark.parametrize("n,lu_nb", [(257, 128), (700, 256), (1300, 512), (1300, 128)])
+def test_lu_symmetric_random(n, lu_nb):
+    """Random complex symmetric, diagonally dominant matrices (partial last
+    diagonal block and partial last outer panel): the L D L^T factors
+    reproduce A to FP32 accuracy, with U = D L^T."""
+    nat = importlib.import_module("matlab-cuda-efief-vs-cpu_b200._native")
+    rng = np.random.default_rng(n + lu_nb)
+    A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
+    A = A + A.T + np.diag(4.0 + 2.0j + rng.standard_normal(n))
+    nat.lib().efie_debug_set_selftest_panel(lu_nb)
+    try:
+        LU = _lu(A, True)
+    finally:
+        nat.lib().efie_debug_set_selftest_panel(0)
+    assert _residual(A, LU) <= 2e-6
+    L = np.tril(LU, -1) + np.eye(n)
+    U = np.triu(LU)
+    DLt = np.diag(np.diag(U)) @ L.T
+    assert np.abs(U - DLt).max() <= 1e-5 * np.abs(U).max()
