@@ -1,19 +1,24 @@
 // Centroid assembly (gassemble) that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured, processes that must stay inside a memory budget fixed at
-// start-up, or hosts (a MATLAB gpuArray workflow, a real-time loop) that own
-// every device buffer themselves.  efie_gassemble_zv_noalloc serves them: the
-// caller passes every input and output as a device pointer, and the scratch
-// the kernels need (per-edge side data, per-triangle softening lengths, a
-// status word) lives in one file-scope __device__ array of fixed size that
-// every GPU loading this library keeps until the process exits.
+// Some callers cannot call cudaMalloc: processes that must stay inside a
+// device-memory budget fixed at start-up (an allocation later could fail or
+// evict another tenant's memory), or hosts (a MATLAB gpuArray workflow, a
+// real-time loop) that own every device buffer themselves and do not let a
+// library allocate behind their back.  efie_gassemble_zv_noalloc serves them:
+// the caller passes every input and output as a device pointer, and the
+// scratch the kernels need (per-edge side data, per-triangle softening
+// lengths, a status word) lives in one file-scope __device__ array of fixed
+// size that every GPU loading this library keeps until the process exits.
 //
 // Limits: Ne <= EFIE_NOALLOC_MAX_NE and Nt <= EFIE_NOALLOC_MAX_NT.  All calls
 // on a device share the array, so calls that overlap on the GPU (different
 // streams, or host threads) race; serialise them.  The first call on a
 // device looks up the array's device address (cudaGetSymbolAddress with that
-// device current); make that first call before any stream capture.
+// device current) and keeps it for the life of the process; make that first
+// call before any stream capture, and do not use this entry point across a
+// cudaDeviceReset of that device (the kept address belongs to the destroyed
+// context).  Each call reads its status word back and synchronises `stream`
+// before it returns.
 #include <cmath>
 #include <cstring>
 #include <mutex>
