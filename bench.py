@@ -13,7 +13,16 @@ The reference arm (--impl reference) times the reference's CPU path --
 CPU_FAST assembly + backslash + Zin, restated in the oracle (C, OpenMP, all
 host cores) with LAPACK from numpy -- on the same workload, one frequency
 point per step; it also times the reference's own CUDA sweep (compiled from
-its sources, oracle/_ref) on a bounded sample as ``ref_gpu``.
+its sources, oracle/_ref) on a bounded sample as ``ref_gpu``.  Its inputs
+(mesh, RWG numbering, ports, prepack) come from the oracle's restatement of
+the MATLAB producers, so that process loads no library of this package.
+
+The default line (cfg2) also carries the plain FP64 GPU path of this package
+(complex128 assembly + cuSOLVER Zgetrf/Zgetrs) on the same frequency points
+as ``fp64_gpu``, the Zin error of every point against it and of sampled
+points against the CPU oracle, and a ``secondary`` block: cfg2 with the
+Dunavant 7-point rule + analytic extraction, and cfg5 (Ne 19936) on a few
+points, each with its Zin error against the FP64 path.
 """
 from __future__ import annotations
 
@@ -165,13 +174,52 @@ def _traffic():
         return {}
 
 
-def roofline(classes):
-    """Roofline entry for the dominant kernel class (largest device time)."""
+# FP64 operations the assembly's pipes execute per point-pair evaluation
+# (QPE) of the single-frequency regular-pair kernel: DADD + DMUL + 2 DFMA
+# from the sass instruction counters of one captured launch
+# (profiles/k_regular_moments_cfg2.md), divided by its QPE.  The transcendental
+# functions (sqrt, sincos, the reciprocal) are FP64 instruction sequences, so
+# this is the work the FP64 pipe does per QPE, not a textbook flop count.
+FP64_OPS_PER_QPE = None
+
+
+def _fp64_ops_per_qpe():
+    tr = _traffic().get("quad_fp64_ops_per_qpe")
+    return float(tr) if tr else FP64_OPS_PER_QPE
+
+
+def _fp64_peak_tflops():
+    """Measured FP64 throughput of cuBLAS DGEMM (torch float64 matmul) on this GPU."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 5
+    for _ in range(reps):
+        torch.matmul(a, b)
+    e1.record()
+    torch.cuda.synchronize()
+    tf = reps * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    del a, b
+    torch.cuda.empty_cache()
+    return tf
+
+
+def roofline(classes, name=None, fp64_peak=None):
+    """Roofline entry for one kernel class (default: the dominant one, by device time)."""
     peaks, src = _peaks()
     cand = {k: v for k, v in classes.items() if v["launches"] > 0 and v["ms"] > 0 and k != "other"}
     if not cand:
         return None
-    name = max(cand, key=lambda k: cand[k]["ms"])
+    if name is None:
+        name = max(cand, key=lambda k: cand[k]["ms"])
+    if name not in cand:
+        return None
     c = cand[name]
     per_launch_ms = c["ms"] / c["launches"]
     per_launch_work = c["work"] / c["launches"]
@@ -181,98 +229,97 @@ def roofline(classes):
         peak = peaks["bf16_tflops_sustained"]
         out = dict(bound="tensor", unit="TFLOP/s", peak_source=src + " bf16 sustained")
     elif name in ("quad", "nearself"):
-        # FP64 point-pair evaluations; reported against HBM only for the schema -- see DESIGN.md
-        achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e9
-        peak = None
-        out = dict(bound="fp64", unit="Gpair/s", peak_source="none")
+        # QPE/s times the FP64 operations per QPE, against measured DGEMM
+        ops = _fp64_ops_per_qpe()
+        qpe_rate = per_launch_work / (per_launch_ms * 1e-3)
+        achieved = qpe_rate * ops / 1e12 if ops else None
+        peak = fp64_peak
+        out = dict(bound="fp64", unit="TFLOP/s", peak_source="measured cuBLAS DGEMM (torch float64 matmul)",
+                   gqpe_per_s=qpe_rate / 1e9, fp64_ops_per_qpe=ops)
     else:
         achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e9
         peak = peaks["hbm_gbs"]
         out = dict(bound="hbm", unit="GB/s", peak_source=src)
-    out.update(kernel=name, achieved=achieved, peak=peak, frac=(achieved / peak) if peak else None,
+    out.update(kernel=name, achieved=achieved, peak=peak,
+               frac=(achieved / peak) if (peak and achieved is not None) else None,
                traffic=tr, launches=c["launches"], ms_per_launch=per_launch_ms)
     return out
 
 
-def cpu_baseline_sample(inp, n_points=1):
-    """Oracle port of the reference CPU path on all host cores, one frequency point."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_c  # noqa: E402  (CPU-baseline leg only)
-    oracle_c.build()
-    rwg = dict(inp["rwg"])
-    pre = inp["pre"]
+def _oracle_mod():
+    """The oracle package (test infrastructure): checker and CPU baseline only."""
+    d = os.path.join(ROOT, "oracle")
+    if d not in sys.path:
+        sys.path.insert(0, d)
+    import efie_oracle  # noqa: E402
+    import oracle_c  # noqa: E402
+    return efie_oracle, oracle_c
+
+
+def oracle_inputs(wl):
+    """Mesh, RWG, ports, prepack and RHS of a workload through the oracle's
+    restatement of the MATLAB producers (no library of this package)."""
+    eo, _ = _oracle_mod()
+    w = WORKLOADS[wl]
+    a, b, n = w["freqs"]
+    d = eo.Design(Lp=w["Lp"], Wp=w["Wp"], Lg=w["Lg"], Wg=w["Wg"], h=w["h"], Np_x=w["Np"][0], Np_y=w["Np"][1],
+                  Ng_x=w["Ng"][0], Ng_y=w["Ng"][1], feed=(0.0, -7e-3), mu=MU0, eps=EPS0, V0=1.0, Z0=50.0,
+                  freqs=np.linspace(a, b, n), vertex_order="grid", opts=dict(OPTS_REF_GPU))
+    return eo.build_problem(d)
+
+
+def cpu_oracle_points(prob, freqs):
+    """The reference CPU path per frequency point, restated in the oracle:
+    CPU_FAST assembly (C, OpenMP, all host cores) + LAPACK solve + Zin.
+    Returns (Zin [n], seconds, cores)."""
+    eo, oc = _oracle_mod()
+    oc.build()
+    d = prob["design"]
     cores = os.cpu_count() or 1
-    b = None
     t0 = time.perf_counter()
-    for f in inp["freqs"][:n_points]:
-        omega = 2 * math.pi * f
-        k = omega * np.sqrt(MU0 * EPS0 + 0j)
-        Z = oracle_c.assemble_z(rwg, pre, k, omega, MU0, EPS0, nthreads=cores)
-        if b is None:
-            m = _pkg()
-            # RHS is O(Ne): reuse the product's host RHS through a tiny ggassemble-free path
-            b = _rhs(inp)
-        x = np.linalg.solve(Z, b)
-        _ = np.sum(x)
-    dt = time.perf_counter() - t0
-    return n_points / dt, cores, dt
-
-
-def _rhs(inp):
-    V = inp["V"]
-    E = inp["rwg"]["edge"].astype(np.int64) - 1
-    c = 0.5 * (V[E[:, 0]] + V[E[:, 1]])
-    zmid = 0.5 * (c[:, 2].min() + c[:, 2].max())
-    lay = np.where(c[:, 2] > zmid, 1, -1)
-
-    def w(e0):
-        d = np.sqrt(((c - c[e0]) ** 2).sum(1))
-        v = np.exp(-(d / inp["spread"]) ** 2) * (lay == lay[e0])
-        return v / v.sum()
-    return (0.5 * w(inp["pe"] - 1) - 0.5 * w(inp["ge"] - 1)).astype(np.complex128)
+    Zin = np.zeros(len(freqs), np.complex128)
+    for i, f in enumerate(freqs):
+        omega, k, _, _ = eo.physics(f, d.mu, d.eps)
+        Z = oc.assemble_z(prob["rwg"], prob["prepack"], k, omega, d.mu, d.eps, nthreads=cores)
+        x = np.linalg.solve(Z, prob["b"].astype(np.complex128))
+        Zin[i], _ = eo.zin_s11(eo.port_current(x, prob["wP"], prob["wG"], prob["rwg"]["len"]), d.V0, d.Z0)
+    return Zin, time.perf_counter() - t0, cores
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    m = _pkg()
-    inp = build_inputs(m, args.workload)
-    cores = os.cpu_count() or 1
+    prob = oracle_inputs(args.workload)
+    freqs = prob["design"].freqs
     for _ in range(min(args.warmup, 1)):
-        cpu_baseline_sample(inp, 1)
+        cpu_oracle_points(prob, freqs[:1])
     times = []
-    for _ in range(args.steps):
-        v, cores, dt = cpu_baseline_sample(inp, 1)
+    cores = os.cpu_count() or 1
+    for s in range(args.steps):
+        _, dt, cores = cpu_oracle_points(prob, freqs[s % len(freqs):s % len(freqs) + 1])
         times.append(dt)
     value = args.steps / sum(times)
     line = dict(metric=METRIC, value=value, unit="freq points/s", impl="reference", n_gpus=args.gpus,
                 steps=args.steps, warmup=min(args.warmup, 1), ms_per_step=1e3 * sum(times) / args.steps,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="c128", data="synthetic",
-                config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=1,
-                            scheme="reference cached subdivision + softening (GPU option set)"),
+                config=dict(workload=args.workload, Ne=prob["rwg"]["Ne"], Nt=int(prob["F"].shape[0]), batch=1,
+                            scheme="reference cached subdivision + softening (GPU option set)",
+                            inputs="oracle restatement of the MATLAB producers"),
                 cpu_baseline=dict(value=value, unit="freq points/s", cores=cores, kind="port",
                                   sample="1 frequency point of %s per step: C restatement of CPU_FAST "
                                          "(OpenMP, %d threads) + numpy LAPACK solve" % (args.workload, cores)),
                 e2e=dict(value=value, unit="freq points/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     # the reference's own CUDA sweep (compiled from its sources) on a bounded sample
     try:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import ref_mex  # noqa: E402
+        import ref_mex  # noqa: E402  (oracle/, on sys.path through _oracle_mod)
         import torch
         if torch.cuda.is_available():
-            n = max(2, min(args.batch, 4))
-            fr = inp["freqs"][:n]
-            r = inp["rwg"]
-            mex = ref_mex.RefMex("patch_sweep_fastquad_ref")
-            call = lambda ff: mex.call(2, inp["V"], inp["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"],
-                                       r["minusSign"], r["rp"], r["rm"], r["Ap"], r["Am"], r["len"], inp["pre"],
-                                       np.asarray(ff, np.float64), MU0, complex(EPS0), float(inp["pe"]),
-                                       float(inp["ge"]), 1.0, inp["spread"], 50.0)
-            call(fr[:1])
+            n = max(8, min(args.batch or 8, 16))
+            fr = freqs[:n]
+            ref_mex.patch_sweep_fastquad(prob, fr[:1])
             t0 = time.perf_counter()
-            call(fr)
+            ref_mex.patch_sweep_fastquad(prob, fr)
             dt = time.perf_counter() - t0
             line["ref_gpu"] = dict(value=n / dt, unit="freq points/s",
                                    sample="%d frequency points through the reference patch_sweep_fastquad_cuda "
@@ -281,6 +328,79 @@ def run_reference(args):
         line["ref_gpu"] = dict(unavailable=str(e)[:200])
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _stream_time(stream, fn):
+    """Device time (ms, CUDA events on `stream`) of fn() and its result."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b) / np.abs(b))) if len(b) else None
+
+
+def fp64_arm(m, pargs, tail, freqs, stream, scheme="ref"):
+    """The plain FP64 GPU path (complex128 assembly + cuSOLVER Zgetrf/Zgetrs
+    per frequency) on `freqs`: (points/s, Zin)."""
+    plan = m.SweepPlan(*pargs, *tail, opts=m.sweep_opts(solver="fp64", scheme=scheme), rule_order=RULE[scheme])
+    plan.run(freqs[:2])
+    ms, (Zin, _) = _stream_time(stream, lambda: plan.run(freqs))
+    plan.close()
+    return len(freqs) / (ms * 1e-3), Zin
+
+
+def secondary_block(m, stream):
+    """cfg2 with the BASELINE quadrature (Dunavant 7-point rule + analytic
+    extraction) on all 101 points, and cfg5 (Ne 19936) on 8 points: points/s
+    of the mixed solver and Zin error against the FP64 GPU path."""
+    out = {}
+    inp = build_inputs(m, "cfg2")
+    pargs = list(inp["args"])
+    pargs[-1] = None
+    fr = inp["freqs"]
+    plan = m.SweepPlan(*pargs, *inp["tail"], opts=m.sweep_opts(scheme="extract"), rule_order=RULE["extract"])
+    plan.run(fr[:4])
+    plan.run(fr)
+    ms, (Zin, _) = _stream_time(stream, lambda: plan.run(fr))
+    st = plan.stats
+    plan.close()
+    v64, Z64 = fp64_arm(m, pargs, inp["tail"], fr, stream, scheme="extract")
+    out["cfg2_extract"] = dict(value=len(fr) / (ms * 1e-3), unit="freq points/s", points=len(fr), Ne=inp["Ne"],
+                               scheme=SCHEME_NAME["extract"], fp64_gpu=v64,
+                               max_rel_zin_err_vs_fp64=_rel(Zin, Z64), max_relres=st["max_relres"],
+                               refine_iters_max=st["refine_iters_max"], fp64_fallbacks=st["n_fp64_fallback"])
+    inp = build_inputs(m, "cfg5")
+    fr = inp["freqs"][::7][:8]
+    # plan creation from the host prepack (host producers + upload + near-pair
+    # scan), then with the prepack computed on the device from V/F
+    t0 = time.perf_counter()
+    pre = m.efie_precompute_pack({"V": inp["V"], "F": inp["F"]}, OPTS_REF_GPU)
+    plan = m.SweepPlan(*inp["args"][:-1], pre, *inp["tail"], opts=m.sweep_opts(), rule_order=0)
+    t_host = time.perf_counter() - t0
+    plan.close()
+    del pre
+    t0 = time.perf_counter()
+    plan = m.SweepPlan(*inp["args"][:-1], None, *inp["tail"], opts=m.sweep_opts(), precompute=OPTS_REF_GPU)
+    t_plan = time.perf_counter() - t0
+    plan.run(fr[:2])
+    ms, (Zin, _) = _stream_time(stream, lambda: plan.run(fr))
+    st = plan.stats
+    plan.close()
+    f3 = fr[[0, 3, 7]]
+    v64, Z64 = fp64_arm(m, inp["args"], inp["tail"], f3, stream)
+    out["cfg5"] = dict(value=len(fr) / (ms * 1e-3), unit="freq points/s", points=len(fr), Ne=inp["Ne"],
+                       scheme=SCHEME_NAME["ref"], plan_create_s=dict(host_prepack=t_host, device_prepack=t_plan),
+                       fp64_gpu=v64, fp64_points=len(f3),
+                       max_rel_zin_err_vs_fp64=_rel(Zin[[0, 3, 7]], Z64), max_relres=st["max_relres"],
+                       refine_iters_max=st["refine_iters_max"], fp64_fallbacks=st["n_fp64_fallback"])
+    return out
 
 
 def run_ours(args):
@@ -308,8 +428,11 @@ def run_ours(args):
     freqs = inp["freqs"]
     B = args.batch or len(freqs)
     # frequency slots of the plan: automatic, but no more than the points of a step
+    # tensor-core tile widths: the command line's, else the autotuner's table
+    tuned = importlib.import_module(PKG + ".autotune").tuned_opts(inp["Ne"])
+    tiles = (args.tile_chain or (tuned[2] if tuned else 0), args.tile_bulk or (tuned[3] if tuned else 0))
     opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
-                        batch=B if B < 8 else 0, lu_nb=args.lu_nb)
+                        batch=B if B < 8 else 0, lu_nb=args.lu_nb, tile_chain=tiles[0], tile_bulk=tiles[1])
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -335,7 +458,8 @@ def run_ours(args):
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for s in range(args.steps):
-            plan.run(batch(args.warmup + s))
+            fr_last = batch(args.warmup + s)
+            Zin_last, _ = plan.run(fr_last)
             st = plan.stats
             launches += st["n_launches"]
             fallback += st["n_fp64_fallback"]
@@ -364,10 +488,14 @@ def run_ours(args):
         fr = batch(args.warmup + s)
         t0 = time.perf_counter()
         if args.scheme == "ref":
-            m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"], opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb))
+            m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"],
+                                        opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb, tile_chain=tiles[0],
+                                                          tile_bulk=tiles[1]))
         else:
             # plan create (host mesh upload) + run + destroy through the C ABI
-            p2 = m.SweepPlan(*pargs, *inp["tail"], opts=m.sweep_opts(solver=args.solver, scheme="extract", lu_nb=args.lu_nb),
+            p2 = m.SweepPlan(*pargs, *inp["tail"],
+                             opts=m.sweep_opts(solver=args.solver, scheme="extract", lu_nb=args.lu_nb,
+                                               tile_chain=tiles[0], tile_bulk=tiles[1]),
                              rule_order=RULE[args.scheme])
             p2.run(fr)
             p2.close()
@@ -379,6 +507,27 @@ def run_ours(args):
         e2e = float(t.item())
     e2e_value = (max(1, args.steps) * B * world) / (e2e * 1e-3)
 
+    # the metric's FP64 arm: the plain FP64 GPU path on the same points, and
+    # the Zin error of every point of the last timed step against it
+    fp64 = None
+    accuracy = dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback)
+    if args.solver == "mixed" and not args.no_fp64_arm:
+        v64, Z64 = fp64_arm(m, pargs, inp["tail"], fr_last, stream, scheme=args.scheme)
+        fp64 = dict(value=v64, unit="freq points/s", points=len(fr_last),
+                    solver="complex128 assembly + cuSOLVER Zgetrf/Zgetrs per frequency")
+        err = np.abs(Zin_last - Z64) / np.abs(Z64)
+        accuracy.update(max_rel_zin_err_vs_fp64=float(err.max()), median_rel_zin_err_vs_fp64=float(np.median(err)),
+                        points_vs_fp64=len(err))
+    fp64_peak = None
+    if rank == 0:
+        try:
+            fp64_peak = _fp64_peak_tflops()
+        except Exception:  # noqa: BLE001
+            fp64_peak = None
+    secondary = None
+    if rank == 0 and world == 1 and args.workload == "cfg2" and args.scheme == "ref" and not args.no_secondary:
+        secondary = secondary_block(m, stream)
+
     line = None
     if rank == 0:
         line = dict(metric=METRIC, value=value, unit="freq points/s", n_gpus=world, steps=args.steps,
@@ -387,21 +536,36 @@ def run_ours(args):
                     else "c128", data="synthetic",
                     config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=B,
                                 solver=args.solver, parallelism="replicas x%d" % world,
+                                tc_tiles="256x%d (panel chain) / 256x%d (outer panels)"
+                                         % (tiles[0] or 256, tiles[1] or 256),
                                 scheme=SCHEME_NAME[args.scheme],
                                 l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
                     e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
                              d2h_bytes_per_step=2 * 16 * B),
                     gpu_launches=launches, clocks=clk.summary(),
-                    accuracy=dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback),
+                    accuracy=accuracy, fp64_gpu=fp64,
                     roofline=roofline(classes),
+                    roofline_assembly=roofline(classes, "quad", fp64_peak),
                     phases_ms_per_point={k: v["ms"] / B for k, v in classes.items()},
                     phases_note="one extra step with per-launch CUDA events (eager launches), outside the "
                                 "timed region; the timed steps replay the factorization as a CUDA graph")
         if world == 1 and not args.no_cpu_baseline:
-            v, cores, dt = cpu_baseline_sample(inp, 1)
-            line["cpu_baseline"] = dict(value=v, unit="freq points/s", cores=cores, kind="port",
-                                        sample="1 frequency point of %s: C restatement of CPU_FAST (OpenMP, %d "
-                                               "threads) + numpy LAPACK solve, %.1f s" % (args.workload, cores, dt))
+            # the oracle's CPU path on the box's host cores: the first point of
+            # the last step and the point furthest from the FP64 arm
+            prob = oracle_inputs(args.workload) if args.scheme == "ref" else None
+            if prob is not None:
+                j = [0]
+                if "max_rel_zin_err_vs_fp64" in accuracy:
+                    j.append(int(np.argmax(np.abs(Zin_last - Z64) / np.abs(Z64))))
+                j = sorted(set(j))
+                Zc, dt, cores = cpu_oracle_points(prob, fr_last[j])
+                line["cpu_baseline"] = dict(value=len(j) / dt, unit="freq points/s", cores=cores, kind="port",
+                                            sample="%d frequency point(s) of %s: C restatement of CPU_FAST (OpenMP, "
+                                                   "%d threads) + numpy LAPACK solve, %.1f s"
+                                                   % (len(j), args.workload, cores, dt))
+                accuracy.update(max_rel_zin_err_vs_cpu_oracle=_rel(Zin_last[j], Zc), points_vs_cpu_oracle=len(j))
+        if secondary:
+            line["secondary"] = secondary
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -416,11 +580,14 @@ def _family():
 
 
 def run_family(args):
-    """cfg3: one step = one design of the family (host mesh -> plan -> 41-point
-    sweep -> results); designs of uneven Ne, each swept with batched
-    frequencies.  Device time (CUDA events on the library's stream) covers
-    geometry upload, assembly, solve and port reduction; e2e adds the host
-    producers and the result read-back (wall clock)."""
+    """cfg3: one step = ``--designs`` designs of the family (GPU mesh + RWG ->
+    plan -> 41-point sweep -> results), ``--workers`` of them in flight at
+    once on their own contexts and streams (surrogate.sweep_family).  Device
+    time: CUDA events on a root stream that every worker stream waits on at
+    the start and that waits on every worker stream at the end; it covers
+    mesh building, plan set-up, assembly, solve and port reduction and the
+    host work between them.  e2e adds the Python driver around it (wall
+    clock)."""
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -434,19 +601,19 @@ def run_family(args):
                                 device_id=torch.device("cuda", local))
     nat = importlib.import_module(PKG + "._native")
     nat.context(local)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    nat.check(nat.lib().efie_ctx_set_stream(nat.context(local), stream.cuda_stream))
     sur, designs = _family()
     nf = FAMILY["nfreq"]
+    W, D = max(1, args.workers), max(1, args.designs)
+    root = torch.cuda.Stream()
+    streams = [torch.cuda.Stream() for _ in range(W)]
+
+    def chunk(i):
+        # the D designs of step i for this rank (ranks take disjoint designs)
+        return [designs[((i * world + rank) * D + j) % len(designs)] for j in range(D)]
 
     def step(i):
-        d = designs[(i * world + rank) % len(designs)]
-        x = sur.design_inputs(d)
-        plan = sur.design_plan(d, inputs=x)
-        Zin, _ = plan.run(d.band(nf))
-        plan.close()
-        return x["Ne"], Zin
+        out = sur.sweep_family(chunk(i), nf, workers=W, device=local, streams=[st.cuda_stream for st in streams])
+        return [n for n, _ in out]
 
     for i in range(args.warmup):
         step(i)
@@ -458,11 +625,16 @@ def run_family(args):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
-        ev0.record(stream)
+        ev0.record(root)
+        for st in streams:
+            st.wait_event(ev0)
         for i in range(args.steps):
-            n, _ = step(args.warmup + i)
-            Ns.append(n)
-        ev1.record(stream)
+            Ns += step(args.warmup + i)
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            root.wait_event(e)
+        ev1.record(root)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     ms = ev0.elapsed_time(ev1)
@@ -470,17 +642,19 @@ def run_family(args):
         t = torch.tensor([ms, wall * 1e3], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, wall = float(t[0].item()), float(t[1].item()) * 1e-3
-    pts = args.steps * nf * world
+    pts = args.steps * D * nf * world
     if rank == 0:
         line = dict(metric=METRIC, value=pts / (ms * 1e-3), unit="freq points/s", n_gpus=world, steps=args.steps,
                     warmup=args.warmup, ms_per_step=ms / args.steps, higher_is_better=True, scaling="weak",
                     vs_baseline=None, dtype="c128 (assembly, residual) / c64 (LU)", data="synthetic",
-                    config=dict(workload="cfg3", designs=FAMILY["n"], Ne_of_timed_designs=Ns, freqs_per_design=nf,
+                    config=dict(workload="cfg3", designs=FAMILY["n"], designs_per_step=D, workers=W,
+                                Ne_of_timed_designs=Ns, freqs_per_design=nf,
                                 mesh_pitch_mm=[1e3 * FAMILY["pitch"], 1e3 * FAMILY["ground_pitch"]],
                                 scheme="Dunavant 7-point rule + analytic 1/R extraction", solver="mixed (GMRES)",
-                                parallelism="replicas x%d" % world),
+                                mesh="built on the GPU (mesh, RWG numbering, ports)",
+                                parallelism="replicas x%d, %d designs in flight per GPU" % (world, W)),
                     e2e=dict(value=pts / wall, unit="freq points/s", h2d_bytes_per_step=None,
-                             d2h_bytes_per_step=nf * 32),
+                             d2h_bytes_per_step=D * nf * 32),
                     clocks=clk.summary())
         print(json.dumps(line), flush=True)
     if dist:
@@ -562,6 +736,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS) + ["cfg3", "cfg4"], default="cfg2")
     ap.add_argument("--samples", type=int, default=20000, help="cfg4: solver samples for training")
+    ap.add_argument("--workers", type=int, default=3, help="cfg3: designs in flight at once per GPU")
+    ap.add_argument("--designs", type=int, default=8, help="cfg3: designs per step")
     ap.add_argument("--epochs", type=int, default=300, help="cfg4: training epochs")
     ap.add_argument("--batch", type=int, default=0, help="frequency points per step (0 = the whole sweep)")
     ap.add_argument("--solver", choices=["mixed", "fp64"], default="mixed")
@@ -570,7 +746,14 @@ def main():
     ap.add_argument("--scheme", choices=["ref", "extract"], default="ref",
                     help="ref: the reference's cached subdivision + softening; extract: Dunavant 7-point rule "
                          "+ analytic 1/R extraction")
+    ap.add_argument("--tile-chain", type=int, default=0, choices=[0, 128, 256],
+                    help="tensor-core tile width of the LU's K = 64 updates (0: the autotuner's table)")
+    ap.add_argument("--tile-bulk", type=int, default=0, choices=[0, 128, 256],
+                    help="tensor-core tile width of the outer panels' updates (0: the autotuner's table)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true", help="skip the plain FP64 GPU path on the same points")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the extraction-scheme and cfg5 block of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -169,6 +169,9 @@ typedef struct efie_sweep_opts {
     int32_t graphs;          /* 1 (default): with timing off, the mixed LU of a
                                 batch replays a CUDA graph captured on the
                                 plan's first batch; 0: eager launches        */
+    int32_t tile_chain;      /* complex columns of the tensor-core tile of the LU's
+                                K = 64 panel-chain updates: 128 or 256 (0 = tuned) */
+    int32_t tile_bulk;       /* ... of the outer panels' trailing updates (0 = tuned) */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */
@@ -199,6 +202,9 @@ typedef struct efie_sweep_stats {
     int32_t class_launches[EFIE_NUM_KERNEL_CLASSES];
     double class_ms[EFIE_NUM_KERNEL_CLASSES];   /* summed CUDA-event time (timing = 1) */
     double class_work[EFIE_NUM_KERNEL_CLASSES]; /* summed algorithmic work, units above */
+    int32_t n_wait_timeouts;    /* frequencies whose bounded device wait gave up (then
+                                   re-solved by the complex128 LU)                */
+    int32_t n_zero_pivots;      /* frequencies whose complex64 LU met a zero pivot */
 } efie_sweep_stats;
 
 /* Replaces patch_sweep_fastquad_cuda.cu:461-844 (mexFunction):
@@ -292,6 +298,46 @@ typedef struct efie_precompute_opts {
 efie_status efie_precompute_pack(int32_t Nv, const double *V, int32_t Nt, const int32_t *F,
                                  const efie_precompute_opts *opts, efie_prepack *out);
 
+/* A two-plate design meshed and numbered on the GPU of `ctx`:
+ * make_patch_with_ground_mesh.m:1-46 (same arguments and vertex_order as
+ * efie_make_patch_with_ground_mesh), build_rwg_interior.m:1-113 and
+ * pick_port_edge_by_point_and_layer.m:1-11 for the port edges nearest to
+ * (feed[0], feed[1], +h/2) on the patch layer and (feed[0], feed[1], -h/2) on
+ * the ground layer.  Every output is bit-identical to the host producers
+ * (same RWG numbering, signs and port edges).  The arrays stay on the device
+ * until efie_design_read copies them to caller arrays in the MEX layout
+ * (sizes from efie_design_sizes; any output pointer may be NULL). */
+typedef struct efie_design efie_design;
+efie_status efie_design_build(efie_ctx *ctx, double Lp, double Wp, double Lg, double Wg, double h,
+                              int32_t Npx, int32_t Npy, int32_t Ngx, int32_t Ngy, int32_t vertex_order,
+                              const double feed[2], efie_design **out);
+efie_status efie_design_sizes(const efie_design *d, int32_t *Nv, int32_t *Nt, int32_t *Ne,
+                              int32_t *patchEdge, int32_t *groundEdge);
+efie_status efie_design_read(const efie_design *d, double *V, int32_t *F, int32_t *edge, int32_t *plusTri,
+                             int32_t *minusTri, int32_t *plusSign, int32_t *minusSign, double *rp,
+                             double *rm, double *Ap, double *Am, double *len, double *center, int32_t *zSign);
+void efie_design_destroy(efie_design *d);
+
+/* The same outputs as efie_precompute_pack, computed on the GPU of `ctx`
+ * from V and F (host arrays in, host arrays out; nearMat included, so
+ * Nt <= 65535).  Floating-point outputs are bit-identical to the host
+ * producer (every operation rounded as in efie_precompute.m, no FMA
+ * contraction), and so is the uint8 nearMat. */
+efie_status efie_precompute_pack_gpu(efie_ctx *ctx, int32_t Nv, const double *V, int32_t Nt, const int32_t *F,
+                                     const efie_precompute_opts *opts, efie_prepack *out);
+
+/* efie_plan_create for the reference scheme whose efie_precompute +
+ * efie_precompute_pack step (efie_precompute.m:1-97,
+ * efie_precompute_pack.m:1-59, MATLAB-side in the reference) runs on the
+ * GPU from mesh->V and mesh->F: the quadrature caches go straight into the
+ * plan's layout and the near pairs straight into its ordered pair list, so
+ * the Nt x Nt nearMat is never formed on the host or sent to the device.
+ * The plan is identical to one created from the host prepack of the same
+ * options. */
+efie_status efie_plan_create_mesh(efie_ctx *ctx, const efie_mesh *mesh, const efie_precompute_opts *popts,
+                                  double mu, efie_c128 eps, int32_t patchEdge, int32_t groundEdge, double V0,
+                                  double spreadRadius, double Z0, const efie_sweep_opts *opts, efie_plan **out);
+
 /* ---------------------------------------------------------------------- */
 /* Self-tests                                                              */
 /* ---------------------------------------------------------------------- */
@@ -319,6 +365,21 @@ void efie_debug_disable_symmetric_lu(int disable);
  * symmetric factorization unless efie_debug_disable_symmetric_lu(1). */
 void efie_debug_set_selftest_panel(int lu_nb);
 
+/* Test hook for the bounded device waits of the triangular solves (the
+ * mixed solver's refinement), process-wide on the current device: enable = 1
+ * makes every later wait target a count that no block ever publishes, so
+ * each wait gives up after `spins` polls, records a timeout for its frequency
+ * and returns; those frequencies are re-solved by the complex128 LU and
+ * counted in efie_sweep_stats.n_wait_timeouts.  enable = 0 restores the
+ * production limit (2^23 polls, about a second).  No counterpart in the
+ * reference. */
+efie_status efie_debug_set_wait_test(int32_t enable, int64_t spins);
+
+/* Tensor-core tile widths (128 or 256 complex columns per CTA pair; anything
+ * else: 256) of efie_lu_selftest's K = 64 chain updates and outer-panel
+ * updates, process-wide.  No counterpart in the reference. */
+void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk);
+
 /* 1 makes efie_plan_run take its batches in frequency order with every
  * refinement starting from zero, instead of coarse to fine with initial
  * guesses interpolated from the solved neighbours (mixed solver, GMRES, more
@@ -333,9 +394,9 @@ void efie_debug_disable_warm_start(int disable);
 
 /* No counterpart in the reference.  The same result as efie_gassemble_zv
  * (Z and Vrhs of the one-point centroid assembly) for callers that cannot
- * call cudaMalloc -- code running while a CUDA graph is captured, processes
- * held to a memory budget fixed at start-up, hosts that own every device
- * buffer.  Every array argument (V ... len, Z, Vrhs) is a DEVICE pointer in
+ * call cudaMalloc -- processes held to a device-memory budget fixed at
+ * start-up, hosts that own every device buffer and do not let a library
+ * allocate.  Every array argument (V ... len, Z, Vrhs) is a DEVICE pointer in
  * the MEX layout; exc (host) = [patchEdge, groundEdge, V0, spreadRadius,
  * selfAlpha].  The function allocates nothing: its scratch is one fixed
  * __device__ array (about 3.2 MB) that every GPU loading this library keeps
@@ -343,8 +404,12 @@ void efie_debug_disable_warm_start(int disable);
  * EFIE_NOALLOC_MAX_NT (larger sizes are rejected with EFIE_ERR_ARGS).  All
  * calls share that array: calls that overlap on the GPU race, so serialise
  * them.  The first call on a device looks up the array's address with that
- * device current; make it before any stream capture.  Runs on `stream` (a
- * cudaStream_t) and returns after synchronising it. */
+ * device current and keeps it for the life of the process: make it before
+ * any stream capture, and do not call this function across a cudaDeviceReset
+ * of that device.  Runs on `stream` (a cudaStream_t) and returns after
+ * synchronising it.  Index errors that only the device sees (F, E,
+ * plusTri/minusTri out of range, no Gaussian port weights) return mex:F,
+ * mex:E, mex:rwg and mex:rhs without touching out-of-range memory. */
 efie_status efie_gassemble_zv_noalloc(int device, void *stream, int32_t Nv, int32_t Nt, int32_t Ne,
                                       const double *V, const int32_t *F, const int32_t *E,
                                       const int32_t *plusTri, const int32_t *minusTri,

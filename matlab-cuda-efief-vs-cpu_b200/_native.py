@@ -44,7 +44,8 @@ class EfieSweepOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("port_model", C.c_int32), ("scheme", C.c_int32),
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
                 ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
-                ("refine_method", C.c_int32), ("graphs", C.c_int32)]
+                ("refine_method", C.c_int32), ("graphs", C.c_int32), ("tile_chain", C.c_int32),
+                ("tile_bulk", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
@@ -55,7 +56,8 @@ class EfieSweepStats(C.Structure):
                 ("n_fp64_fallback", C.c_int32), ("max_relres", C.c_double),
                 ("ms_assemble", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
                 ("n_launches", C.c_int32),
-                ("class_launches", C.c_int32 * 8), ("class_ms", C.c_double * 8), ("class_work", C.c_double * 8)]
+                ("class_launches", C.c_int32 * 8), ("class_ms", C.c_double * 8), ("class_work", C.c_double * 8),
+                ("n_wait_timeouts", C.c_int32), ("n_zero_pivots", C.c_int32)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("class_")}
@@ -112,11 +114,24 @@ SIGNATURES = {
     "efie_quad_rule_size": (C.c_int32, [C.c_int32]),
     "efie_precompute_pack": (C.c_int, [C.c_int32, c_double_p, C.c_int32, c_int32_p,
                                        C.POINTER(EfiePrecomputeOpts), C.POINTER(EfiePrepack)]),
+    "efie_design_build": (C.c_int, [_P] + [C.c_double] * 5 + [C.c_int32] * 5 + [c_double_p, C.POINTER(_P)]),
+    "efie_design_sizes": (C.c_int, [_P] + [c_int32_p] * 5),
+    "efie_design_read": (C.c_int, [_P, c_double_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p,
+                                   c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p,
+                                   c_int32_p]),
+    "efie_design_destroy": (None, [_P]),
+    "efie_precompute_pack_gpu": (C.c_int, [_P, C.c_int32, c_double_p, C.c_int32, c_int32_p,
+                                           C.POINTER(EfiePrecomputeOpts), C.POINTER(EfiePrepack)]),
+    "efie_plan_create_mesh": (C.c_int, [_P, C.POINTER(EfieMesh), C.POINTER(EfiePrecomputeOpts), C.c_double, c128,
+                                        C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                        C.POINTER(EfieSweepOpts), C.POINTER(_P)]),
     "efie_lu_selftest": (C.c_int, [_P, C.c_int32, _P, C.c_int32, _P]),
     "efie_debug_disable_tensor_cores": (None, [C.c_int]),
     "efie_debug_disable_symmetric_lu": (None, [C.c_int]),
     "efie_debug_set_selftest_panel": (None, [C.c_int]),
+    "efie_debug_set_selftest_tiles": (None, [C.c_int, C.c_int]),
     "efie_debug_disable_warm_start": (None, [C.c_int]),
+    "efie_debug_set_wait_test": (C.c_int, [C.c_int32, C.c_int64]),
     "efie_gassemble_zv_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_int32] + [_P] * 12 +
                                   [c128, C.c_double, C.c_double, c128, c_double_p, _P, _P]),
     "efie_mlp_config_default": (None, [_P]),
@@ -191,6 +206,20 @@ def context(device=0):
         _ctx = h
         atexit.register(_destroy_ctx)
     return _ctx
+
+
+def new_context(device=0):
+    """A further context on `device` (its own CUDA stream and solver handle),
+    for a host thread of its own; release it with destroy_context after the
+    plans created on it."""
+    h = C.c_void_p()
+    check(lib().efie_ctx_create(device, C.byref(h)))
+    return h
+
+
+def destroy_context(h):
+    if h is not None and h.value:
+        lib().efie_ctx_destroy(h)
 
 
 def register_plan(plan):

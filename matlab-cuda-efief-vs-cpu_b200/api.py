@@ -29,7 +29,8 @@ __all__ = [
     "MexError", "ggassemble_ZV_EFIE_RWG_DIFF_GPU_FAST", "gassemble_ZV_EFIE_RWG_DIFF_GPU_FAST",
     "patch_sweep_fastquad_cuda", "patch_sweep_cuda", "assemble_ZV_EFIE_RWG_DIFF_GPU_FAST",
     "make_patch_with_ground_mesh", "build_rwg_interior", "pick_port_edge_by_point_and_layer",
-    "efie_precompute_pack", "quad_rule_size", "SweepPlan", "sweep_opts",
+    "efie_precompute_pack", "efie_precompute_pack_gpu", "build_patch_design_gpu", "quad_rule_size", "SweepPlan",
+    "sweep_opts",
 ]
 
 
@@ -289,9 +290,10 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # Sweeps
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
-               timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True):
+               timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True, tile_chain=0, tile_bulk=0):
     """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
-    scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only)."""
+    scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only),
+    tile_chain / tile_bulk: tensor-core tile widths 128 | 256 (0 = tuned)."""
     o = nat.EfieSweepOpts()
     nat.lib().efie_sweep_opts_default(C.byref(o))
     o.solver = {"fp64": nat.SOLVER_FP64, "mixed": nat.SOLVER_MIXED}[solver]
@@ -304,6 +306,8 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.lu_nb = int(lu_nb)
     o.refine_method = {"gmres": nat.REFINE_GMRES, "classical": nat.REFINE_CLASSICAL}[refine]
     o.graphs = 1 if graphs else 0
+    o.tile_chain = int(tile_chain)
+    o.tile_bulk = int(tile_bulk)
     return o
 
 
@@ -380,14 +384,25 @@ def patch_sweep_cuda(*args, nargout=2, opts=None, stats=None):
     return Zin, S11
 
 
+def _precompute_opts(opts):
+    """efie_precompute_opts with efie_precompute.m's defaults (:5, :45-48)."""
+    return nat.EfiePrecomputeOpts(int(opts["quad_order"]), int(opts.get("near_order", 4)),
+                                  int(opts.get("self_subdiv", 2)), int(opts.get("near_subdiv", 2)),
+                                  float(opts["near_sing_eps"]), float(opts.get("self_alpha", 0.20)),
+                                  float(opts.get("near_alpha", 0.15)))
+
+
 class SweepPlan:
     """Geometry uploaded once; ``run(freqs)`` sweeps with device-resident data.
 
-    Arguments are those of patch_sweep_fastquad_cuda minus ``freqs``.
+    Arguments are those of patch_sweep_fastquad_cuda minus ``freqs``.  With
+    ``pre=None`` and ``precompute`` (the options of efie_precompute, e.g.
+    ``quad_order``, ``near_sing_eps``, ...) the prepack of the reference
+    scheme is computed on the GPU from V/F (no host nearMat).
     """
 
     def __init__(self, V, F, E, pt, mt, ps, ms, rp, rm, Ap, Am, ln, pre, mu, eps, pe, ge, V0, spread, Z0,
-                 opts=None, rule_order=0):
+                 opts=None, rule_order=0, precompute=None, ctx=None):
         Nv, Nt, Ne = _check_VFE(V, F, E)
         self.Ne = Ne
         self._m = _Marshal()
@@ -396,15 +411,24 @@ class SweepPlan:
         if opts is None:
             from .autotune import tuned_opts
             t = tuned_opts(Ne)
-            opts = sweep_opts(batch=t[0], lu_nb=t[1]) if t else sweep_opts()
+            opts = sweep_opts(batch=t[0], lu_nb=t[1], tile_chain=t[2], tile_bulk=t[3]) if t else sweep_opts()
         self.opts = opts
         h = C.c_void_p()
-        nat.check(nat.lib().efie_plan_create(
-            nat.context(), C.byref(self._mesh), C.byref(self._pp) if self._pp is not None else None,
-            float(_scalar(mu)), _cscalar(eps), int(_scalar(pe)), int(_scalar(ge)), float(_scalar(V0)),
-            float(_scalar(spread)), float(_scalar(Z0)), C.byref(self.opts), int(rule_order), C.byref(h)))
+        cx = ctx if ctx is not None else nat.context()
+        if pre is None and precompute is not None:
+            po = _precompute_opts(precompute)
+            nat.check(nat.lib().efie_plan_create_mesh(
+                cx, C.byref(self._mesh), C.byref(po), float(_scalar(mu)), _cscalar(eps),
+                int(_scalar(pe)), int(_scalar(ge)), float(_scalar(V0)), float(_scalar(spread)), float(_scalar(Z0)),
+                C.byref(self.opts), C.byref(h)))
+        else:
+            nat.check(nat.lib().efie_plan_create(
+                cx, C.byref(self._mesh), C.byref(self._pp) if self._pp is not None else None,
+                float(_scalar(mu)), _cscalar(eps), int(_scalar(pe)), int(_scalar(ge)), float(_scalar(V0)),
+                float(_scalar(spread)), float(_scalar(Z0)), C.byref(self.opts), int(rule_order), C.byref(h)))
         self._h = h
-        nat.register_plan(self)
+        if ctx is None:
+            nat.register_plan(self)   # plans on their own contexts are closed by their owner
 
     def run(self, freqs, return_currents=False):
         fr = _f64(freqs)
@@ -485,6 +509,42 @@ def build_rwg_interior(mesh):
     return out
 
 
+def build_patch_design_gpu(Lp, Wp, Lg, Wg, h, Np_x, Np_y, Ng_x, Ng_y, feed=(0.0, -7e-3), vertex_order="reference",
+                           ctx=None):
+    """Mesh, RWG topology and port edges of a two-plate design built on the GPU
+    (make_patch_with_ground_mesh.m, build_rwg_interior.m,
+    pick_port_edge_by_point_and_layer.m at (feed, +-h/2)).  Returns
+    (V, F, rwg, patchEdge, groundEdge) exactly as the host producers do."""
+    vo = {"reference": 0, "grid": 1}[vertex_order]
+    L = nat.lib()
+    h_ = C.c_void_p()
+    fd = np.ascontiguousarray(np.asarray(feed, dtype=np.float64).reshape(2))
+    nat.check(L.efie_design_build(ctx if ctx is not None else nat.context(), float(Lp), float(Wp), float(Lg), float(Wg), float(h), int(Np_x),
+                                  int(Np_y), int(Ng_x), int(Ng_y), vo, fd.ctypes.data_as(nat.c_double_p),
+                                  C.byref(h_)))
+    try:
+        n = [C.c_int32() for _ in range(5)]
+        nat.check(L.efie_design_sizes(h_, *[C.byref(x) for x in n]))
+        Nv, Nt, Ne, pe, ge = (x.value for x in n)
+        V = np.zeros((Nv, 3), np.float64, order="F")
+        F = np.zeros((Nt, 3), np.int32, order="F")
+        r = dict(edge=np.zeros((Ne, 2), np.int32, order="F"), plusTri=np.zeros(Ne, np.int32),
+                 minusTri=np.zeros(Ne, np.int32), plusSign=np.zeros(Ne, np.int32), minusSign=np.zeros(Ne, np.int32),
+                 rp=np.zeros((Ne, 3), order="F"), rm=np.zeros((Ne, 3), order="F"), Ap=np.zeros(Ne),
+                 Am=np.zeros(Ne), len=np.zeros(Ne), center=np.zeros((Ne, 3), order="F"),
+                 zSign=np.zeros(Ne, np.int32))
+        i32 = lambda a: a.ctypes.data_as(nat.c_int32_p)
+        f64 = lambda a: a.ctypes.data_as(nat.c_double_p)
+        nat.check(L.efie_design_read(h_, f64(V), i32(F), i32(r["edge"]), i32(r["plusTri"]), i32(r["minusTri"]),
+                                     i32(r["plusSign"]), i32(r["minusSign"]), f64(r["rp"]), f64(r["rm"]),
+                                     f64(r["Ap"]), f64(r["Am"]), f64(r["len"]), f64(r["center"]),
+                                     i32(r["zSign"])))
+        r["Ne"] = Ne
+    finally:
+        L.efie_design_destroy(h_)
+    return V, F, r, pe, ge
+
+
 def pick_port_edge_by_point_and_layer(rwg, p, layerSign):
     """eidx = pick_port_edge_by_point_and_layer(rwg,p,layerSign) (1-based; first minimum)."""
     c = np.asfortranarray(np.asarray(rwg["center"], dtype=np.float64))
@@ -501,7 +561,12 @@ def quad_rule_size(order):
     return int(nat.lib().efie_quad_rule_size(int(order)))
 
 
-def efie_precompute_pack(mesh, opts):
+def efie_precompute_pack_gpu(mesh, opts):
+    """efie_precompute_pack computed on the GPU (same outputs, bit for bit)."""
+    return efie_precompute_pack(mesh, opts, gpu=True)
+
+
+def efie_precompute_pack(mesh, opts, gpu=False):
     """prepack = efie_precompute_pack(efie_precompute(mesh,opts),opts) in one call
     (efie_precompute.m:1-97, efie_precompute_pack.m:1-59), with the same option
     defaults (near_order 4, self_subdiv 2, self_alpha 0.20, near_subdiv 2,
@@ -509,10 +574,7 @@ def efie_precompute_pack(mesh, opts):
     V = np.asfortranarray(np.asarray(mesh["V"], dtype=np.float64))
     F = np.asfortranarray(np.asarray(mesh["F"], dtype=np.int32))
     Nv, Nt = V.shape[0], F.shape[0]
-    o = nat.EfiePrecomputeOpts(int(opts["quad_order"]), int(opts.get("near_order", 4)),
-                               int(opts.get("self_subdiv", 2)), int(opts.get("near_subdiv", 2)),
-                               float(opts["near_sing_eps"]), float(opts.get("self_alpha", 0.20)),
-                               float(opts.get("near_alpha", 0.15)))
+    o = _precompute_opts(opts)
     Nq, Nq2 = quad_rule_size(o.quad_order), quad_rule_size(o.near_order)
     NsS, NsN = 4 ** o.self_subdiv, 4 ** o.near_subdiv
     pre = dict(r_reg=np.zeros((Nq, 3, Nt), order="F"), w_reg=np.zeros((Nq, Nt), order="F"),
@@ -524,8 +586,12 @@ def efie_precompute_pack(mesh, opts):
     pp = nat.EfiePrepack(Nt, Nq, Nq2, NsS, NsN, f64(pre["r_reg"]), f64(pre["w_reg"]),
                          pre["nearMat"].ctypes.data_as(nat.c_uint8_p), f64(pre["self_r"]), f64(pre["self_w"]),
                          f64(pre["self_a"]), f64(pre["near_r"]), f64(pre["near_w"]), f64(pre["aeqTri"]), 0.0, 0.0)
-    nat.check(nat.lib().efie_precompute_pack(Nv, V.ctypes.data_as(nat.c_double_p), Nt,
-                                             F.ctypes.data_as(nat.c_int32_p), C.byref(o), C.byref(pp)))
+    if gpu:
+        nat.check(nat.lib().efie_precompute_pack_gpu(nat.context(), Nv, V.ctypes.data_as(nat.c_double_p), Nt,
+                                                     F.ctypes.data_as(nat.c_int32_p), C.byref(o), C.byref(pp)))
+    else:
+        nat.check(nat.lib().efie_precompute_pack(Nv, V.ctypes.data_as(nat.c_double_p), Nt,
+                                                 F.ctypes.data_as(nat.c_int32_p), C.byref(o), C.byref(pp)))
     pre["near_alpha"] = pp.near_alpha
     pre["self_alpha"] = pp.self_alpha
     return pre

@@ -1,10 +1,14 @@
-"""Autotuner for the sweep solver: frequencies per batch and LU outer panel width.
+"""Autotuner for the sweep solver: frequencies per batch, LU outer panel width
+and the tensor-core tile widths of the LU's trailing updates.
 
 For a given geometry it times short sweeps over the candidate settings and
-keeps the fastest whose refinement still converges (no FP64 fallback).  The
-winners are cached in ``tuned.json`` next to this file, keyed by the Ne bucket
-(powers of two) and the GPU's SM count; ``tuned_opts()`` looks them up so
-that a SweepPlan created without explicit options uses them.
+keeps the fastest whose refinement still converges (no FP64 fallback): first
+(batch, panel width) with 256-column tiles, then the four tile-width pairs
+(128 or 256 complex columns per CTA pair, for the panel chain's K = 64
+updates and for the outer panels' updates) at the winning batch and panel
+width.  The winners are cached in ``tuned.json`` next to this file, keyed by
+the Ne bucket (powers of two) and the GPU's SM count; ``tuned_opts()`` looks
+them up so that a SweepPlan created without explicit options uses them.
 
     python -m autotune  (from the package directory) or tune(plan_args, freqs)
 """
@@ -19,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned.json")
 BATCHES = (8, 16, 32)
 PANELS = (128, 256, 512)
+TILES = ((256, 256), (128, 256), (256, 128), (128, 128))
 
 
 def _key(Ne, sms):
@@ -39,43 +44,91 @@ def load_table():
 
 
 def tuned_opts(Ne, sms=None):
-    """(batch, lu_nb) for this size on this GPU, or None when untuned."""
+    """(batch, lu_nb, tile_chain, tile_bulk) for this size on this GPU, or
+    None when untuned (tile widths 0 = the library's default)."""
     try:
         sms = sms or _sms()
     except Exception:  # noqa: BLE001 - no torch/GPU: no table lookup
         return None
     e = load_table().get(_key(Ne, sms))
-    return (e["batch"], e["lu_nb"]) if e else None
+    return (e["batch"], e["lu_nb"], e.get("tile_chain", 0), e.get("tile_bulk", 0)) if e else None
 
 
-def tune(plan_args, freqs, candidates=None, repeats=1, save=True):
-    """Time every (batch, lu_nb) candidate on the sweep of ``freqs``.
+def _time(plan_args, freqs, repeats, **kw):
+    from .api import SweepPlan, sweep_opts
+    plan = SweepPlan(*plan_args, opts=sweep_opts(**kw))
+    plan.run(freqs[:kw["batch"]])                    # warm-up: workspaces, kernels, graph
+    t0 = time.perf_counter()
+    ok = True
+    for _ in range(repeats):
+        plan.run(freqs)
+        ok = ok and plan.stats["n_fp64_fallback"] == 0
+    dt = time.perf_counter() - t0
+    Ne = plan.Ne
+    plan.close()
+    return Ne, ((repeats * len(freqs) / dt) if ok else None)
+
+
+def tune(plan_args, freqs, candidates=None, repeats=1, save=True, tiles=True):
+    """Time every (batch, lu_nb) candidate on the sweep of ``freqs``, then
+    (with ``tiles``) the tile-width pairs at the winner.
 
     plan_args: the positional arguments of SweepPlan (geometry .. Z0).
-    Returns (best, results) with results[(batch, lu_nb)] = points/s or None.
+    Returns (best, results): best = (batch, lu_nb, tile_chain, tile_bulk),
+    results[(batch, lu_nb, tile_chain, tile_bulk)] = points/s or None.
     """
-    from .api import SweepPlan, sweep_opts
     cands = candidates or [(b, p) for b in BATCHES for p in PANELS]
     results = {}
     Ne = None
     for batch, panel in cands:
-        plan = SweepPlan(*plan_args, opts=sweep_opts(batch=batch, lu_nb=panel))
-        Ne = plan.Ne
-        plan.run(freqs[:batch])                      # warm-up: workspaces, kernels
-        t0 = time.perf_counter()
-        ok = True
-        for _ in range(repeats):
-            plan.run(freqs)
-            ok = ok and plan.stats["n_fp64_fallback"] == 0
-        dt = time.perf_counter() - t0
-        plan.close()
-        results[(batch, panel)] = (repeats * len(freqs) / dt) if ok else None
+        Ne, results[(batch, panel, 256, 256)] = _time(plan_args, freqs, repeats, batch=batch, lu_nb=panel,
+                                                      tile_chain=256, tile_bulk=256)
     good = {k: v for k, v in results.items() if v}
     best = max(good, key=good.get) if good else None
+    if best and tiles:
+        for tc, tb in TILES:
+            key = (best[0], best[1], tc, tb)
+            if key not in results:
+                _, results[key] = _time(plan_args, freqs, repeats, batch=best[0], lu_nb=best[1], tile_chain=tc,
+                                        tile_bulk=tb)
+        good = {k: v for k, v in results.items() if v}
+        best = max(good, key=good.get)
     if save and best:
         table = load_table()
-        table[_key(Ne, _sms())] = dict(batch=best[0], lu_nb=best[1], points_per_s=good[best],
-                                       candidates={"%d/%d" % k: v for k, v in results.items()})
+        table[_key(Ne, _sms())] = dict(batch=best[0], lu_nb=best[1], tile_chain=best[2], tile_bulk=best[3],
+                                       points_per_s=good[best],
+                                       candidates={"%d/%d/%d/%d" % k: v for k, v in results.items()})
         with open(TABLE, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
     return best, results
+
+
+def _patch_problem(Npx, Npy, Ngx, Ngy, Lp=30e-3, Wp=38e-3, Lg=60e-3, Wg=60e-3, h=1.6e-3):
+    """SweepPlan arguments of a two-plate patch (reference GPU option set,
+    main_patch_gpu_mex_sweep_l.m:50-56) through the package's producers."""
+    from .api import build_rwg_interior, efie_precompute_pack, make_patch_with_ground_mesh, \
+        pick_port_edge_by_point_and_layer
+    import numpy as np
+    V, F, _, _ = make_patch_with_ground_mesh(Lp, Wp, Lg, Wg, h, Npx, Npy, Ngx, Ngy, vertex_order="grid")
+    r = build_rwg_interior({"V": V, "F": F})
+    pe = pick_port_edge_by_point_and_layer(r, (0.0, -7e-3, +h / 2), +1)
+    ge = pick_port_edge_by_point_and_layer(r, (0.0, -7e-3, -h / 2), -1)
+    pre = efie_precompute_pack({"V": V, "F": F}, dict(quad_order=2, near_sing_eps=1.2, self_subdiv=2,
+                                                      self_alpha=0.20, near_subdiv=1, near_alpha=0.15,
+                                                      near_order=2))
+    mu0 = 4e-7 * math.pi
+    eps0 = 1.0 / (mu0 * 299792458.0 ** 2)
+    return [V, F, r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"], r["rm"],
+            r["Ap"], r["Am"], r["len"], pre, mu0, eps0, pe, ge, 1.0, 1.5 * float(np.mean(r["len"])), 50.0]
+
+
+if __name__ == "__main__":
+    # python -m <package>.autotune [grid ...]: tune the 101-point 2-3 GHz sweep
+    # of the patch 38x30 mm over a 60x60 mm ground for each grid (default:
+    # the 32x24 / 40x40 mesh, Ne 6968)
+    import sys
+    import numpy as np
+    grids = [tuple(int(x) for x in a.split("x")) for a in sys.argv[1:]] or [(32, 24, 40, 40)]
+    for g in grids:
+        best, res = tune(_patch_problem(*g), np.linspace(2e9, 3e9, 101))
+        print(json.dumps({"grid": g, "best": best, "results": {"%d/%d/%d/%d" % k: v for k, v in res.items()}}))

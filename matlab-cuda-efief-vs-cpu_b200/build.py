@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libefie_b200.so")
-SOURCES = ["capi.cu", "assemble.cu", "solve.cu", "trsv.cu", "gemm_tc.cu", "noalloc.cu", "surrogate.cu", "gmres.cu", "geom.cpp"]
+SOURCES = ["capi.cu", "assemble.cu", "solve.cu", "trsv.cu", "gemm_tc.cu", "noalloc.cu", "surrogate.cu", "gmres.cu", "precompute.cu", "mesh.cu", "geom.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -738,12 +738,14 @@ Physics efie_physics(double freq, double mu, efie_c128 eps) {
 
 // Host-side repacking of the boundary arrays into the device layout.
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
-                             int rule_order, GeomDev &g) {
+                             int rule_order, GeomDev &g, const efie_precompute_opts *popts) {
     const int Ne = mesh->Ne, Nt = mesh->Nt, Nv = mesh->Nv;
     g.Ne = Ne;
     g.Nt = Nt;
     g.scheme = scheme;
     g.near_alpha = pre ? pre->near_alpha : 0.0;
+    if (scheme == EFIE_SCHEME_REF && !pre && !popts)
+        return efie_fail(EFIE_ERR_PREPACK, "the reference scheme needs a prepack or precompute options");
     // origins: triangle centroids from V/F
     std::vector<double4> origin(Nt);
     for (int t = 0; t < Nt; t++) {
@@ -826,7 +828,10 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     // the pair list whose entries (and diagonal) the device mask marks
     std::vector<int2> list;
     bool mask_both = true;
-    if (scheme == EFIE_SCHEME_REF) {
+    if (scheme == EFIE_SCHEME_REF && !pre) {
+        // caches and near-pair list computed on the device from V/F (precompute.cu)
+        EFIE_TRY(efie_geom_precompute_device(ctx, mesh, popts, g));
+    } else if (scheme == EFIE_SCHEME_REF) {
         const int Nq = pre->Nq, Nq2 = pre->Nq2, NsS = pre->NsS, NsN = pre->NsN;
         g.Nq = Nq;
         g.Nq2 = Nq2;
@@ -945,7 +950,7 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
         EFIE_TRY(g.near_mask.reserve(nn));
         EFIE_CUDA(cudaMemsetAsync(g.near_mask.p, 0, nn, ctx->stream));
         DevBuf &lst = scheme == EFIE_SCHEME_REF ? g.near_list : g.adj_list;
-        const int n = (int)list.size();
+        const int n = scheme == EFIE_SCHEME_REF ? g.n_near : g.n_adj;
         if (n > 0)
             k_mask_pairs<<<(n + 255) / 256, 256, 0, ctx->stream>>>(Nt, n, lst.as<int2>(), mask_both,
                                                                    g.near_mask.as<uint8_t>());

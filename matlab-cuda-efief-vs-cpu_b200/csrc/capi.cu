@@ -68,6 +68,8 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->lu_nb = 0;
     o->timing = 0;
     o->batch = 0;
+    o->tile_chain = 0;
+    o->tile_bulk = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -515,6 +517,10 @@ int choose_panel(int N, int requested) {
     return N >= 4096 ? 512 : 128;
 }
 
+// Tile width (complex columns per CTA pair) of the tensor-core updates: the
+// caller's (tuned) choice, else 256.
+int choose_tile(int requested) { return requested == 128 ? 128 : 256; }
+
 efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c128 eps, int pe, int ge, double V0,
                         double spread, double Z0, const efie_sweep_opts *opts) {
     efie_ctx *ctx = p->ctx;
@@ -552,7 +558,11 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
     EFIE_TRY(p->ipiv.reserve(sizeof(int) * N));
     EFIE_CUDA(cudaMemcpyAsync(p->b.p, bc.data(), sizeof(efie_c128) * N, cudaMemcpyHostToDevice, ctx->stream));
     EFIE_CUDA(cudaMemcpyAsync(p->wport.p, wport.data(), sizeof(double) * N, cudaMemcpyHostToDevice, ctx->stream));
-    if (p->opts.solver == EFIE_SOLVER_MIXED) EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B, choose_panel(N, p->opts.lu_nb)));
+    if (p->opts.solver == EFIE_SOLVER_MIXED) {
+        EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B, choose_panel(N, p->opts.lu_nb)));
+        p->sw.tn_chain = choose_tile(p->opts.tile_chain);
+        p->sw.tn_bulk = choose_tile(p->opts.tile_bulk);
+    }
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
 }
@@ -578,6 +588,33 @@ extern "C" efie_status efie_plan_create(efie_ctx *ctx, const efie_mesh *mesh, co
     // products then read only the upper triangle
     if (s == EFIE_OK) p->sw.zsym = p->g.symmetric;
     // the symmetric gather also writes the mixed solver's complex64 planes
+    if (s == EFIE_OK) p->sw.planes_from_assembly = p->opts.solver == EFIE_SOLVER_MIXED && p->g.symmetric;
+    if (s == EFIE_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        s = efie_fail(EFIE_ERR_CUDA, "geometry upload failed");
+    if (s != EFIE_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return EFIE_OK;
+}
+
+extern "C" efie_status efie_plan_create_mesh(efie_ctx *ctx, const efie_mesh *mesh, const efie_precompute_opts *popts,
+                                             double mu, efie_c128 eps, int32_t patchEdge, int32_t groundEdge,
+                                             double V0, double spreadRadius, double Z0, const efie_sweep_opts *opts,
+                                             efie_plan **out) {
+    if (!ctx || !out || !popts) return efie_fail(EFIE_ERR_ARGS, "null context, options or output");
+    *out = nullptr;
+    EFIE_TRY(check_mesh(mesh, true));
+    if (opts && opts->scheme != EFIE_SCHEME_REF)
+        return efie_fail(EFIE_ERR_ARGS, "efie_plan_create_mesh builds the reference scheme's caches");
+    DeviceGuard dg(ctx->device);
+    efie_plan *p = new (std::nothrow) efie_plan();
+    if (!p) return efie_fail(EFIE_ERR_NOMEM, "out of host memory");
+    p->ctx = ctx;
+    efie_status s = plan_common(p, mesh, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, opts);
+    if (s == EFIE_OK) s = efie_geom_upload(ctx, mesh, nullptr, EFIE_SCHEME_REF, 0, p->g, popts);
+    if (s == EFIE_OK) p->sw.zsym = p->g.symmetric;
     if (s == EFIE_OK) p->sw.planes_from_assembly = p->opts.solver == EFIE_SOLVER_MIXED && p->g.symmetric;
     if (s == EFIE_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         s = efie_fail(EFIE_ERR_CUDA, "geometry upload failed");
@@ -737,6 +774,8 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                                       p->opts.refine_max_iter, active, &rr, guess);
             if (rc != EFIE_OK) break;
             S->refine_iters_max = std::max(S->refine_iters_max, rr.iters);
+            int err1[EFIE_MAX_BATCH];   // device error codes of the first attempt
+            for (int f = 0; f < nb; f++) err1[f] = rr.err[f];
             if (p->sw.zsym && p->sw.sym_lu && p->opts.refine_method == EFIE_REFINE_GMRES) {
                 // a frequency that missed the target with the L D L^T factors
                 // is factored again as a general matrix (eager launches, from
@@ -763,6 +802,9 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 }
             }
             for (int f = 0; f < nb; f++) {
+                // 1: zero pivot (k_diag_factor); 2, 3: a bounded wait gave up (k_trsv, k_update_tc)
+                if (err1[f] == 1 || rr.err[f] == 1) S->n_zero_pivots++;
+                if (err1[f] >= 2 || rr.err[f] >= 2) S->n_wait_timeouts++;
                 if (!rr.converged[f] || rr.err[f]) {
                     // zero pivot, timeout or stalled refinement: complex128 LU for this frequency
                     fallback[f] = true;
@@ -897,8 +939,13 @@ extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh 
 // Self-test of the complex64 LU (no pivoting) used by the mixed solver.
 // ---------------------------------------------------------------------------
 static int g_selftest_nb = 256;
+static int g_selftest_tile[2] = {256, 256};
 extern "C" void efie_debug_set_selftest_panel(int lu_nb) {
     g_selftest_nb = (lu_nb == 64 || lu_nb == 128 || lu_nb == 256 || lu_nb == 512) ? lu_nb : 256;
+}
+extern "C" void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk) {
+    g_selftest_tile[0] = choose_tile(tile_chain);
+    g_selftest_tile[1] = choose_tile(tile_bulk);
 }
 
 extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores,
@@ -908,6 +955,8 @@ extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c12
     ctx->log.reset(false);
     SolveWork w;
     EFIE_TRY(efie_mixed_workspace(w, N, 1, g_selftest_nb));
+    w.tn_chain = g_selftest_tile[0];
+    w.tn_bulk = g_selftest_tile[1];
     // a bit-exactly symmetric A takes the symmetric factorization, as a
     // sweep's Z from the symmetric gather does
     bool sym = true;

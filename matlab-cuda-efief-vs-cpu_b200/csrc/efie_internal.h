@@ -187,8 +187,14 @@ Physics efie_physics(double freq, double mu, efie_c128 eps);
 Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
 
 // assemble.cu
+// pre == nullptr with the reference scheme: the caches and the near-pair
+// list are computed on the device from V/F with the options `popts`
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
-                             int rule_order, GeomDev &g);
+                             int rule_order, GeomDev &g, const efie_precompute_opts *popts = nullptr);
+// precompute.cu: efie_precompute + efie_precompute_pack on the device, straight
+// into the plan's layout (origins, cache points, near-pair list)
+efie_status efie_geom_precompute_device(efie_ctx *ctx, const efie_mesh *mesh, const efie_precompute_opts *o,
+                                        GeomDev &g);
 // pr (optional, symmetric gather only): also write the complex64 working
 // matrix of the mixed solver as FP32 planes, re at pr[m * ld + n], im at
 // pr[(Ne + m) * ld + n]

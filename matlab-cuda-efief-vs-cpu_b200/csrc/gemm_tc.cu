@@ -51,17 +51,28 @@ namespace {
 
 constexpr int KMAX = 512;        // largest complex K of one update (the outer LU block)
 constexpr int TR = 128;          // complex rows of L21 per CTA (one TMEM lane each)
-constexpr int TN = 256;          // complex columns of the pair's tile (MMA N)
+constexpr int TM = 2 * TR;       // complex rows of the pair's tile (MMA M)
 constexpr int KC = 32;           // fp16 elements per 64-byte swizzle row (one K chunk)
 constexpr int NCHUNK_MAX = KMAX / KC;
 constexpr int SUB = TR * KC;     // halves per 128 x 32 sub-tile (8 KB)
 // a packed K chunk of one 128-row (128-column) tile: re hi, re lo, im hi, im lo
 constexpr int CHUNK_HALVES = 4 * SUB;                      // 32 KB
-constexpr int STAGE_HALVES = 2 * CHUNK_HALVES;             // L chunk + U half chunk: 64 KB
-constexpr int NSTAGE = 3;
-constexpr int NBAR = 3 * NSTAGE + 1;  // full[], empty[], pair_full[], done
-constexpr size_t GEMM_SMEM =
-    sizeof(__half) * NSTAGE * STAGE_HALVES + 1024 + 8 * NBAR + 16 + sizeof(float) * TN;
+
+// Tile shapes of the pair: TM x BN complex entries, BN = 256 or 128 columns.
+// Each CTA holds TR rows of L and BN/2 columns of U per K chunk; the real and
+// imaginary accumulators take 2 BN TMEM columns.  BN = 128 halves the U bytes
+// and the drain per tile, so a 4-stage ring fits and narrow updates (the
+// panel chain's last blocks) waste fewer columns.
+template <int BN>
+struct Tile {
+    static constexpr int UH = BN / 2;                           // U columns per CTA
+    static constexpr int USUB = UH * KC;                        // halves per U component sub-tile
+    static constexpr int STAGE = CHUNK_HALVES + 4 * USUB;       // L chunk + U half chunk
+    static constexpr int NST = BN == 256 ? 3 : 4;               // stages of the ring (192 KB either way)
+    static constexpr int NBAR = 3 * NST + 1;                    // full[], empty[], pair_full[], done
+    static constexpr int BAR_WORDS = (NBAR + 1 + 1) & ~1;       // + TMEM slot and flag, 16-byte aligned
+    static constexpr size_t SMEM = sizeof(__half) * NST * STAGE + 1024 + 8 * BAR_WORDS + sizeof(float) * BN;
+};
 
 __host__ __device__ __forceinline__ uint32_t swz(uint32_t r, uint32_t k) { return efie_swz64(r, k); }
 __device__ __forceinline__ float pow2_scale(float mx) { return efie_pow2_scale(mx); }
@@ -267,9 +278,12 @@ __device__ __forceinline__ uint64_t desc_sw64(const void *smem_tile) {
 
 // kind::f16, D = F32, A = B = F16, both K-major, M = 256 (CTA pair), N = 256;
 // bit 13 negates A
-constexpr uint32_t IDESC = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(2 * TR >> 4) << 24);
-constexpr uint32_t IDESC_NEG_A = IDESC | (1u << 13);
+template <int BN>
+struct Idesc {
+    static constexpr uint32_t POS = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                    ((uint32_t)(TM >> 4) << 24);
+    static constexpr uint32_t NEG_A = POS | (1u << 13);
+};
 
 __device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -300,19 +314,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Column tiles of row pair p in the lower-triangle mode: those whose first
-// column block of width kb does not lie right of the pair's last row block.
-__host__ __device__ __forceinline__ int tri_cols(int p, int nct, int kb) {
-    const int qr = (p * TN + TN - 1) / kb;
-    const int n = ((qr + 1) * kb + TN - 1) / TN;
+// Column tiles (width bn) of row pair p in the lower-triangle mode: those
+// whose first column block of width kb does not lie right of the pair's last
+// row block.
+__host__ __device__ __forceinline__ int tri_cols(int p, int nct, int kb, int bn) {
+    const int qr = (p * TM + TM - 1) / kb;
+    const int n = ((qr + 1) * kb + bn - 1) / bn;
     return n < nct ? n : nct;
 }
 
 // ---------------------------------------------------------------------------
 // The update kernel.  C[r0:r1, c0:c1] -= (packed L) * (packed U) for the
-// pair's 256 x 256 tile; grid (2 x column tiles, row-pair tiles, frequency),
+// pair's 256 x BN tile; grid (2 x column tiles, row-pair tiles, frequency),
 // clusters of two CTAs along x, 256 threads.
 // ---------------------------------------------------------------------------
+template <int BN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     k_update_tc(const __grid_constant__ CUtensorMap cmap, int N, int r0, int r1, int c0, int c1, int nchunk,
                 const __half *__restrict__ Lpackb, size_t lstride, int lpitch, int loff,
@@ -322,20 +338,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 const int *__restrict__ active, int tri_kb) {
     const int f = blockIdx.z;
     if (!active[f]) return;   // both CTAs of a cluster share f
-    int ct = blockIdx.x >> 1;   // 256-column tile of the pair
+    using T = Tile<BN>;
+    constexpr int NSTAGE = T::NST;
+    int ct = blockIdx.x >> 1;   // BN-column tile of the pair
     int rp = blockIdx.y;        // 256-row tile of the pair
     if (tri_kb > 0) {
         // lower tiles of a square block in row order (both CTAs of the pair
         // map the same x to the same tile)
-        const int npr = (r1 - r0 + TN - 1) / TN, nct = (c1 - c0 + TN - 1) / TN;
+        const int npr = (r1 - r0 + TM - 1) / TM, nct = (c1 - c0 + BN - 1) / BN;
         rp = 0;
         while (rp < npr - 1) {
-            const int nc = tri_cols(rp, nct, tri_kb);
+            const int nc = tri_cols(rp, nct, tri_kb, BN);
             if (ct < nc) break;
             ct -= nc;
             rp++;
         }
-        if (ct >= tri_cols(rp, nct, tri_kb)) return;
+        if (ct >= tri_cols(rp, nct, tri_kb, BN)) return;
     }
     const uint32_t rank = cluster_rank();
     const bool leader = rank == 0;
@@ -346,23 +364,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     extern __shared__ uint8_t dyn_raw[];
     // 1024-byte alignment for the swizzled tiles (the same offset in both CTAs)
     __half *stage = reinterpret_cast<__half *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * STAGE_HALVES);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stage + NSTAGE * T::STAGE);
     uint64_t *full = bars, *empty = bars + NSTAGE, *pfull = bars + 2 * NSTAGE, *done = bars + 3 * NSTAGE;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + NBAR);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + T::NBAR);
     int *ok_sh = reinterpret_cast<int *>(tmem_slot + 1);
-    float *col_is = reinterpret_cast<float *>(bars + 12);   // 16-byte aligned: inverse column scales
+    float *col_is = reinterpret_cast<float *>(bars + T::BAR_WORDS);   // 16-byte aligned: inverse column scales
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int rtile = rp * 2 + (int)rank;            // this CTA's 128-row tile
-    const int utile = ct * 2 + (int)rank;            // this CTA's 128-column half of U
+    const int ucol = ct * BN + (int)rank * T::UH;    // first column of this CTA's half of U
 
     if (tid == 0) {
-        for (int i = 0; i < NBAR; i++) mbar_init(&bars[i], 1);
+        for (int i = 0; i < T::NBAR; i++) mbar_init(&bars[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *ok_sh = 1;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(2 * TN));
+                     "r"(2 * BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -374,14 +392,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         bool ok = true;
         // this CTA's 128 rows of each component plane of L (columns of U)
         const __half *gl = Lpack + (size_t)(loff + rtile * TR) * KC;
-        const __half *gu = Upack + (size_t)(uoff + utile * TR) * KC;
-        constexpr uint32_t sbytes = sizeof(__half) * SUB;
+        const __half *gu = Upack + (size_t)(uoff + ucol) * KC;
+        constexpr uint32_t sbytes = sizeof(__half) * SUB, ubytes = sizeof(__half) * T::USUB;
         auto load = [&](int c) {
-            __half *st = stage + (c % NSTAGE) * STAGE_HALVES;
-            mbar_expect_tx(&full[c % NSTAGE], 8 * sbytes);
+            __half *st = stage + (c % NSTAGE) * T::STAGE;
+            mbar_expect_tx(&full[c % NSTAGE], 4 * (sbytes + ubytes));
             for (int comp = 0; comp < 4; comp++) {
                 bulk_g2s(st + comp * SUB, gl + (size_t)(c * 4 + comp) * lpitch * KC, sbytes, &full[c % NSTAGE]);
-                bulk_g2s(st + CHUNK_HALVES + comp * SUB, gu + (size_t)(c * 4 + comp) * upitch * KC, sbytes,
+                bulk_g2s(st + CHUNK_HALVES + comp * T::USUB, gu + (size_t)(c * 4 + comp) * upitch * KC, ubytes,
                          &full[c % NSTAGE]);
             }
         };
@@ -396,13 +414,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const __half *st = stage + sidx * STAGE_HALVES;
+                const __half *st = stage + sidx * T::STAGE;
                 const uint64_t lrh = desc_sw64(st), lrl = desc_sw64(st + SUB), lih = desc_sw64(st + 2 * SUB),
                                lil = desc_sw64(st + 3 * SUB);
                 const __half *su = st + CHUNK_HALVES;
-                const uint64_t urh = desc_sw64(su), url = desc_sw64(su + SUB), uih = desc_sw64(su + 2 * SUB),
-                               uil = desc_sw64(su + 3 * SUB);
-                const uint32_t dre = tmem, dim = tmem + TN;
+                const uint64_t urh = desc_sw64(su), url = desc_sw64(su + T::USUB), uih = desc_sw64(su + 2 * T::USUB),
+                               uil = desc_sw64(su + 3 * T::USUB);
+                const uint32_t dre = tmem, dim = tmem + BN;
+                constexpr uint32_t IDESC = Idesc<BN>::POS, IDESC_NEG_A = Idesc<BN>::NEG_A;
 #pragma unroll
                 for (int kk = 0; kk < KC / 16; kk++) {
                     const uint64_t a = (uint64_t)((kk * 32) >> 4);   // 16 fp16 = 32 bytes along K
@@ -454,18 +473,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         if (!ok) *ok_sh = 0;
     } else if (warp > 0) {
         // inverse column scales of the tile into shared memory
-        for (int j = tid - 32; j < TN; j += 224) {
-            const int col = c0 + ct * TN + j;
+        for (int j = tid - 32; j < BN; j += 224) {
+            const int col = c0 + ct * BN + j;
             col_is[j] = (col < c1) ? 1.f / pow2_scale(col_max(um, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
         }
         // C rows of this CTA into L2 while the MMAs run: (plane, row) segments
-        const int ncol = min(TN, c1 - (c0 + ct * TN));
+        const int ncol = min(BN, c1 - (c0 + ct * BN));
         const uint32_t bytes = (uint32_t)((ncol * 4 + 15) & ~15);
         for (int e = tid - 32; e < 2 * TR; e += 224) {
             const int pl = e / TR, rr = e % TR;
             const int row = r0 + rtile * TR + rr;
             if (row < r1 && ncol > 0) {
-                const float *src = (pl ? Ai : Ar) + (size_t)row * ld + c0 + ct * TN;
+                const float *src = (pl ? Ai : Ar) + (size_t)row * ld + c0 + ct * BN;
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
             }
         }
@@ -480,14 +499,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         const int quarter = warp & 3;               // TMEM lanes 32 quarter ... (tcgen05.ld reach of this warp)
         const int pl = warp >> 2;                   // 0: real part, 1: imaginary part
         const int rowq = r0 + rtile * TR + quarter * 32;   // first row of this warp's 32
-        const int ncol = c1 - (c0 + ct * TN);       // valid columns of this tile (may exceed TN)
+        const int ncol = c1 - (c0 + ct * BN);       // valid columns of this tile (may exceed BN)
         if (rowq < r1) {                            // warp-uniform
             const int row = rowq + lane;
             const float rs = row < r1 ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
-            const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(pl * TN);
+            const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(pl * BN);
             // the stages are free once the MMAs are done: four 4 KB tiles per warp
             float *ring = reinterpret_cast<float *>(stage) + warp * 4 * 1024;
-            constexpr int NJ = TN / 32;
+            constexpr int NJ = BN / 32;
 #pragma unroll 1
             for (int j = 0; j < NJ && j * 32 < ncol; j++) {
                 uint32_t v[32];
@@ -511,7 +530,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // visible to the bulk copy
                 __syncwarp();
-                if (lane == 0) reduce_add_tile(&cmap, tile, c0 + ct * TN + j * 32, rowq, pl, f);
+                if (lane == 0) reduce_add_tile(&cmap, tile, c0 + ct * BN + j * 32, rowq, pl, f);
             }
             if (lane == 0) bulk_wait_read<0>();   // shared memory is read before the CTA exits
             __syncwarp();
@@ -521,7 +540,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     // both CTAs are past every access to each other's shared memory and TMEM
     cluster_sync();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN));
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
     }
 }
 
@@ -532,7 +551,10 @@ static bool g_tc_disabled = false;
 efie_status efie_tc_attrs() {
     static bool done = false;
     if (done) return EFIE_OK;
-    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)Tile<256>::SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)Tile<128>::SMEM));
     done = true;
     return EFIE_OK;
 }
@@ -646,13 +668,17 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
             EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
         return EFIE_OK;
     }
+    // tile width of the pair: the panel chain's K = 64 updates and the outer
+    // panels' updates each have their own (tuned) choice
+    const int BN = K <= 64 ? w.tn_chain : w.tn_bulk;
+    if (BN != 256 && BN != 128) return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: tile width must be 128 or 256");
     if (!Lv.base || !Uv.base || (Lv.off & 7) || (Uv.off & 7) ||
-        Lv.off + (rows + TN - 1) / TN * TN > Lv.pitch || Uv.off + (cols + TN - 1) / TN * TN > Uv.pitch)
+        Lv.off + (rows + TM - 1) / TM * TM > Lv.pitch || Uv.off + (cols + BN - 1) / BN * BN > Uv.pitch)
         return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: packed operands do not cover the block");
     EFIE_TRY(efie_tc_attrs());
     const int N = w.N, B = w.B;
     cudaStream_t st = ctx->stream;
-    const int npr = (rows + TN - 1) / TN, nct = (cols + TN - 1) / TN;   // 256-row pairs, 256-column tiles
+    const int npr = (rows + TM - 1) / TM, nct = (cols + BN - 1) / BN;   // 256-row pairs, BN-column tiles
     const int nchunk = (K + KC - 1) / KC;
     // work: the entries the update must produce (in the lower-triangle mode
     // those of column blocks <= row block, not the tiles' overhang)
@@ -660,18 +686,25 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     double entries = (double)rows * cols;
     if (tri_kb > 0) {
         int ntiles = 0;
-        for (int p = 0; p < npr; p++) ntiles += tri_cols(p, nct, tri_kb);
+        for (int p = 0; p < npr; p++) ntiles += tri_cols(p, nct, tri_kb, BN);
         grid = dim3(2 * ntiles, 1, B);
         entries = 0;
         for (int q0 = 0; q0 < rows; q0 += tri_kb)
             entries += (double)std::min(tri_kb, rows - q0) * std::min(cols, q0 + tri_kb);
     }
     size_t tok = ctx->log.begin(st);
-    k_update_tc<<<grid, 256, GEMM_SMEM, st>>>(
-        *reinterpret_cast<const CUtensorMap *>(w.planes_map), N, r0, r1, c0, c1, nchunk,
-        static_cast<const __half *>(Lv.base), Lv.stride, Lv.pitch, Lv.off, static_cast<const __half *>(Uv.base),
-        Uv.stride, Uv.pitch, Uv.off, w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K,
-        w.planes.as<float>(), w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>(), tri_kb);
+    const CUtensorMap &cm = *reinterpret_cast<const CUtensorMap *>(w.planes_map);
+    const __half *lb = static_cast<const __half *>(Lv.base), *ub = static_cast<const __half *>(Uv.base);
+    if (BN == 256)
+        k_update_tc<256><<<grid, 256, Tile<256>::SMEM, st>>>(
+            cm, N, r0, r1, c0, c1, nchunk, lb, Lv.stride, Lv.pitch, Lv.off, ub, Uv.stride, Uv.pitch, Uv.off,
+            w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K, w.planes.as<float>(),
+            w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>(), tri_kb);
+    else
+        k_update_tc<128><<<grid, 256, Tile<128>::SMEM, st>>>(
+            cm, N, r0, r1, c0, c1, nchunk, lb, Lv.stride, Lv.pitch, Lv.off, ub, Uv.stride, Uv.pitch, Uv.off,
+            w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K, w.planes.as<float>(),
+            w.pstride, w.ld, w.ctl.as<char>(), w.active.as<int>(), tri_kb);
     EFIE_CUDA(cudaGetLastError());
     ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * entries * K * nact);
     return EFIE_OK;

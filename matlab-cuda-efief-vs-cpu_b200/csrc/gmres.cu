@@ -345,9 +345,14 @@ __global__ void k_gm_reset_skip(int B, char *__restrict__ ctl, const int *__rest
 // (t = J (J + 1) / 2 + I): rows I, columns J.  It contributes Z_IJ x_J to y_I
 // and, off the diagonal, Z_IJ^T x_I to y_J; both partial vectors go to
 // P[f][t][2][ST] and k_symv_reduce adds them in a fixed order, so the
-// product is bit-reproducible.  Warp w takes the tile's columns w, w + 8, ...;
-// lane l its rows l + 32 q.  A frequency whose flag (flags[f * fstride]) is
-// set is skipped.
+// product is bit-reproducible.  Warp w takes the tile's columns 16 w .. 16 w
+// + 15 in four groups of four (lane l its rows l + 32 q): the sixteen 16-byte
+// loads of a group are issued before any of them is used, and the four
+// column sums of a group are reduced across the warp together (each halving
+// step exchanges half of the values still held, 6 complex shuffles per group
+// instead of 20).  Z is streamed past the caches (each entry is read once per
+// product); the vectors stay cached.  A frequency whose flag
+// (flags[f * fstride]) is set is skipped.
 // ---------------------------------------------------------------------------
 constexpr int ST = 128;
 
@@ -357,6 +362,15 @@ __device__ __forceinline__ void tile_of(int t, int &I, int &J) {
     while (j * (j + 1) / 2 > t) j--;
     J = j;
     I = t - j * (j + 1) / 2;
+}
+
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int o) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
+
+__device__ __forceinline__ void cadd(double2 &a, const double2 &b) {
+    a.x += b.x;
+    a.y += b.y;
 }
 
 __global__ void __launch_bounds__(256) k_symv_tiles(int N, const double2 *__restrict__ Zb, size_t zstride,
@@ -370,40 +384,59 @@ __global__ void __launch_bounds__(256) k_symv_tiles(int N, const double2 *__rest
     const double2 *x = xb + (size_t)N * f;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int r0 = I * ST, c0 = J * ST;
+    const bool offdiag = I != J;
     __shared__ double2 rsum[8][ST];
     __shared__ double2 csum[ST];
     double2 xr[4], rs[4];
+    bool rv[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int m = r0 + lane + 32 * q;
-        xr[q] = m < N ? x[m] : make_double2(0.0, 0.0);
+        rv[q] = m < N;
+        xr[q] = rv[q] ? x[m] : make_double2(0.0, 0.0);
         rs[q] = make_double2(0.0, 0.0);
     }
-    for (int cc = warp; cc < ST; cc += 8) {
-        const int n = c0 + cc;
-        double2 cs = make_double2(0.0, 0.0);
-        if (n < N) {
-            const double2 xn = x[n];
-            const double2 *col = Z + (size_t)N * n;
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+        const int cb = warp * 16 + g * 4;   // first column of the group within the tile
+        double2 a[4][4], xn[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int n = c0 + cb + j;
+            const bool cvalid = n < N;
+            xn[j] = cvalid ? x[n] : make_double2(0.0, 0.0);
+            const double2 *col = Z + (size_t)N * (cvalid ? n : 0);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                a[j][q] = (cvalid && rv[q]) ? __ldcs(col + r0 + lane + 32 * q) : make_double2(0.0, 0.0);
+        }
+        double2 cs[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            cs[j] = make_double2(0.0, 0.0);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int m = r0 + lane + 32 * q;
-                if (m < N) {
-                    const double2 a = col[m];
-                    rs[q].x += a.x * xn.x - a.y * xn.y;
-                    rs[q].y += a.x * xn.y + a.y * xn.x;
-                    cs.x += a.x * xr[q].x - a.y * xr[q].y;
-                    cs.y += a.x * xr[q].y + a.y * xr[q].x;
-                }
+                const double2 v = a[j][q];
+                rs[q].x += v.x * xn[j].x - v.y * xn[j].y;
+                rs[q].y += v.x * xn[j].y + v.y * xn[j].x;
+                cs[j].x += v.x * xr[q].x - v.y * xr[q].y;
+                cs[j].y += v.x * xr[q].y + v.y * xr[q].x;
             }
         }
-        if (I != J) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                cs.x += __shfl_xor_sync(0xffffffffu, cs.x, o);
-                cs.y += __shfl_xor_sync(0xffffffffu, cs.y, o);
-            }
-            if (lane == 0) csum[cc] = cs;
+        if (offdiag) {   // block-uniform
+            // lanes with bit 4 set keep columns 2, 3 (send 0, 1), the others keep 0, 1
+            const bool b4 = lane & 16, b3 = lane & 8;
+            double2 k0 = b4 ? cs[2] : cs[0], k1 = b4 ? cs[3] : cs[1];
+            cadd(k0, shfl_xor2(b4 ? cs[0] : cs[2], 16));
+            cadd(k1, shfl_xor2(b4 ? cs[1] : cs[3], 16));
+            // bit 3 picks one of the two
+            double2 k = b3 ? k1 : k0;
+            cadd(k, shfl_xor2(b3 ? k0 : k1, 8));
+            cadd(k, shfl_xor2(k, 4));
+            cadd(k, shfl_xor2(k, 2));
+            cadd(k, shfl_xor2(k, 1));
+            // lane 8 c holds column cb + c (c = 2 b4 + b3)
+            if ((lane & 7) == 0) csum[cb + (lane >> 3)] = k;
         }
     }
 #pragma unroll
@@ -417,7 +450,7 @@ __global__ void __launch_bounds__(256) k_symv_tiles(int N, const double2 *__rest
             t.y += rsum[w][threadIdx.x].y;
         }
         out[threadIdx.x] = t;
-    } else if (I != J) {
+    } else if (offdiag) {
         out[threadIdx.x] = csum[threadIdx.x - ST];
     }
 }

@@ -32,6 +32,8 @@ struct SolveWork {
     int vstride = 0;          // float2 per frequency in each vector of `vec`
     int grid = 0;             // CTAs of the triangular-solve grid
     int kb_outer = 256;       // outer panel width of the two-level LU (K of the big updates)
+    int tn_chain = 256;       // tile width (complex columns per CTA pair) of the K = 64 updates
+    int tn_bulk = 256;        // ... and of the outer panels' updates
     DevBuf planes;   // per f: float re[N][ld], im[N][ld]  (row-major)
     DevBuf dinv;     // per f: float2 [nblk][2][NB*NB] (L^-1, U^-1 of each diagonal block)
     DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]

@@ -25,14 +25,24 @@ constexpr int NB = 64;
 constexpr int DS = NB + 1;    // padded row stride of the diagonal inverse in shared memory
 constexpr int LINE = 8;       // u64 per 64-byte progress line
 
+// Limits of the bounded waits, per device.  d_wait_spins: polls before a
+// wait gives up (2^23, about a second).  d_wait_offset: added to every wait
+// target; nonzero only under efie_debug_set_wait_test, where it makes every
+// target unreachable (a count no block ever publishes) so that tests can make
+// the waits run out on purpose.
+__device__ long long d_wait_spins = 1ll << 23;
+__device__ unsigned long long d_wait_offset = 0;
+
 // Wait until the counter reaches `target`; returns the observed value (0 on
 // timeout or error, after which every waiter returns).
 __device__ __forceinline__ unsigned long long wait_progress(const volatile unsigned long long *ctr,
                                                             unsigned long long target, const volatile int *err) {
     long long spins = 0;
+    const long long limit = d_wait_spins;
+    target += d_wait_offset;
     unsigned long long v;
     while ((v = *ctr) < target) {
-        if (++spins > (1ll << 23)) {  // give up after ~1 s: record, let every waiter return
+        if (++spins > limit) {  // give up: record, let every waiter return
             atomicExch((int *)err, 2);
             return 0;
         }
@@ -200,6 +210,18 @@ __global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const floa
 }
 
 }  // namespace
+
+// Test hook (process-wide, on the current device): every later triangular
+// solve waits for a count that is never published and gives up after `spins`
+// polls (enable = 1), or the production limits come back (enable = 0).
+extern "C" efie_status efie_debug_set_wait_test(int32_t enable, int64_t spins) {
+    const long long lim = enable ? (long long)std::max<int64_t>(spins, 1) : (1ll << 23);
+    const unsigned long long off = enable ? (1ull << 31) : 0ull;   // block counts stay below 2^31
+    EFIE_CUDA(cudaMemcpyToSymbol(d_wait_spins, &lim, sizeof(lim)));
+    EFIE_CUDA(cudaMemcpyToSymbol(d_wait_offset, &off, sizeof(off)));
+    EFIE_CUDA(cudaDeviceSynchronize());
+    return EFIE_OK;
+}
 
 efie_status efie_trsv_workspace(SolveWork &w) {
     int dev = 0, sms = 0, occ = 0;

@@ -26,8 +26,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as nat
-from .api import (SweepPlan, build_rwg_interior, make_patch_with_ground_mesh, pick_port_edge_by_point_and_layer,
-                  sweep_opts)
+from .api import (SweepPlan, build_patch_design_gpu, build_rwg_interior, make_patch_with_ground_mesh,
+                  pick_port_edge_by_point_and_layer, sweep_opts)
 
 MU0 = 4.0 * math.pi * 1e-7
 C0 = 299792458.0
@@ -80,25 +80,31 @@ def sample_designs(n, seed=0, W=(25e-3, 45e-3), L=(20e-3, 40e-3), h=(0.8e-3, 3.2
     return out
 
 
-def design_inputs(d: PatchDesign):
-    """Mesh, RWG and port edges of a design (library producers, grid vertex order)."""
+def design_inputs(d: PatchDesign, device=True, ctx=None):
+    """Mesh, RWG and port edges of a design (grid vertex order): built on the
+    GPU (build_patch_design_gpu) or by the host producers; the two are
+    bit-identical."""
     npx, npy, ngx, ngy = d.cells()
     G = d.ground_factor * max(d.W, d.L)
-    V, F, _, _ = make_patch_with_ground_mesh(d.L, d.W, G, G, d.h, npx, npy, ngx, ngy, vertex_order="grid")
-    rwg = build_rwg_interior({"V": V, "F": F})
-    pe = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, +d.h / 2), +1)
-    ge = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, -d.h / 2), -1)
+    if device:
+        V, F, rwg, pe, ge = build_patch_design_gpu(d.L, d.W, G, G, d.h, npx, npy, ngx, ngy, feed=(0.0, d.feed),
+                                                   vertex_order="grid", ctx=ctx)
+    else:
+        V, F, _, _ = make_patch_with_ground_mesh(d.L, d.W, G, G, d.h, npx, npy, ngx, ngy, vertex_order="grid")
+        rwg = build_rwg_interior({"V": V, "F": F})
+        pe = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, +d.h / 2), +1)
+        ge = pick_port_edge_by_point_and_layer(rwg, (0.0, d.feed, -d.h / 2), -1)
     spread = 1.5 * float(np.mean(rwg["len"]))
     return dict(V=V, F=F, rwg=rwg, pe=pe, ge=ge, spread=spread, Ne=rwg["Ne"])
 
 
-def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None):
+def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None, ctx=None):
     """A SweepPlan of the design: Dunavant 7-point rule + analytic 1/R extraction."""
-    x = inputs or design_inputs(d)
+    x = inputs or design_inputs(d, ctx=ctx)
     r = x["rwg"]
     return SweepPlan(x["V"], x["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"],
                      r["rm"], r["Ap"], r["Am"], r["len"], None, MU0, EPS0, x["pe"], x["ge"], 1.0, x["spread"], 50.0,
-                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch), rule_order=-7)
+                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch), rule_order=-7, ctx=ctx)
 
 
 def features(d: PatchDesign, freqs):
@@ -196,6 +202,63 @@ class Surrogate:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Design families: several designs in flight at once
+# ---------------------------------------------------------------------------
+def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=None):
+    """Zin over each design's band (``d.band(nfreq)``) for a family of
+    designs of uneven Ne, ``workers`` designs in flight at once.
+
+    Each worker is a host thread with a library context of its own (its own
+    CUDA stream -- ``streams[w]`` when given, a ``cudaStream_t`` --, solver
+    handle and look-ahead streams): it meshes its next design on the GPU,
+    creates the plan (extraction scheme), sweeps and releases it, while the
+    other workers' designs run on their streams.  The latency-bound phases of
+    one design (the LU's panel chain, GMRES's stop-flag polls, plan set-up on
+    the host) then overlap the bulk kernels of the others.  Every design is
+    solved exactly as design_plan(d).run(d.band(nfreq)) alone (the sweeps
+    share nothing).  Returns [(Ne, Zin)] in the order of ``designs``; a
+    failure in any worker is raised after all workers have stopped."""
+    import queue
+    import threading
+    out = [None] * len(designs)
+    todo = queue.Queue()
+    for i in range(len(designs)):
+        todo.put(i)
+    errors = []
+
+    def work(w):
+        ctx = nat.new_context(device)
+        try:
+            if streams is not None:
+                nat.check(nat.lib().efie_ctx_set_stream(ctx, streams[w]))
+            while not errors:
+                try:
+                    i = todo.get_nowait()
+                except queue.Empty:
+                    return
+                d = designs[i]
+                plan = design_plan(d, solver=solver, ctx=ctx)
+                try:
+                    Zin, _ = plan.run(d.band(nfreq))
+                    out[i] = (plan.Ne, Zin)
+                finally:
+                    plan.close()
+        except Exception as e:  # noqa: BLE001 -- re-raised below
+            errors.append(e)
+        finally:
+            nat.destroy_context(ctx)
+
+    threads = [threading.Thread(target=work, args=(w,)) for w in range(max(1, workers))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return out
 
 
 # ---------------------------------------------------------------------------

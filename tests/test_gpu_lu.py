@@ -111,3 +111,28 @@ def test_lu_symmetric_random(n, lu_nb):
     U = np.triu(LU)
     DLt = np.diag(np.diag(U)) @ L.T
     assert np.abs(U - DLt).max() <= 1e-5 * np.abs(U).max()
+
+
+@pytest.mark.parametrize("tiles", [(128, 128), (128, 256), (256, 128)])
+@pytest.mark.parametrize("n,lu_nb,sym", [(700, 256, False), (1300, 512, True), (1300, 128, True)])
+def test_lu_tile_widths(tiles, n, lu_nb, sym):
+    """The 256 x 128 tensor-core tile (a CTA pair per 128 complex columns)
+    gives the same factors as the 256 x 256 tile to FP32 accuracy, for the
+    panel chain's K = 64 updates and for the outer panels' updates, in the
+    general and in the symmetric factorization."""
+    nat = importlib.import_module("matlab-cuda-efief-vs-cpu_b200._native")
+    rng = np.random.default_rng(n + lu_nb + tiles[0])
+    A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
+    if sym:
+        A = A + A.T
+    A += np.diag(4.0 + 2.0j + rng.standard_normal(n))
+    nat.lib().efie_debug_set_selftest_panel(lu_nb)
+    try:
+        ref = _lu(A, True)
+        nat.lib().efie_debug_set_selftest_tiles(*tiles)
+        got = _lu(A, True)
+    finally:
+        nat.lib().efie_debug_set_selftest_tiles(0, 0)
+        nat.lib().efie_debug_set_selftest_panel(0)
+    assert _residual(A, got) <= 2e-6
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-6
