@@ -380,6 +380,11 @@ efie_status efie_debug_set_wait_test(int32_t enable, int64_t spins);
  * updates, process-wide.  No counterpart in the reference. */
 void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk);
 
+/* Lanes per triangle pair of the multi-frequency regular-pair kernel: 2 (the
+ * default: the pair's frequencies split over two lanes) or 1, process-wide;
+ * the two give the same values.  No counterpart in the reference. */
+void efie_debug_set_regular_lanes(int lanes);
+
 /* 1 makes efie_plan_run take its batches in frequency order with every
  * refinement starting from zero, instead of coarse to fine with initial
  * guesses interpolated from the solved neighbours (mixed solver, GMRES, more

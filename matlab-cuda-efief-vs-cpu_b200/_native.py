@@ -130,6 +130,7 @@ SIGNATURES = {
     "efie_debug_disable_symmetric_lu": (None, [C.c_int]),
     "efie_debug_set_selftest_panel": (None, [C.c_int]),
     "efie_debug_set_selftest_tiles": (None, [C.c_int, C.c_int]),
+    "efie_debug_set_regular_lanes": (None, [C.c_int]),
     "efie_debug_disable_warm_start": (None, [C.c_int]),
     "efie_debug_set_wait_test": (C.c_int, [C.c_int32, C.c_int64]),
     "efie_gassemble_zv_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_int32] + [_P] * 12 +

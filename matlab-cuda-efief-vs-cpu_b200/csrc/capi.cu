@@ -391,6 +391,7 @@ extern "C" efie_status efie_gassemble_zv(efie_ctx *ctx, const efie_mesh *mesh, e
 // ---------------------------------------------------------------------------
 struct efie_plan {
     efie_ctx *ctx = nullptr;
+    DevBuf rs_info;              // cuSOLVER getrs status (argument errors only)
     efie_sweep_opts opts;
     bool centroid = false;       // patch_sweep_cuda model
     double self_alpha = 0.20;
@@ -484,11 +485,15 @@ efie_status plan_solve_fp64(efie_plan *p, int slot, int fi) {
         p->lwork_elems = lw;
     }
     EFIE_CUDA(cudaMemcpyAsync(x, p->b.p, sizeof(cuDoubleComplex) * N, cudaMemcpyDeviceToDevice, ctx->stream));
+    // getrf's info (a zero pivot: efie:singular) in slot fi; getrs reports
+    // only argument errors, into a slot of its own so that it cannot
+    // overwrite getrf's
+    EFIE_TRY(p->rs_info.reserve(sizeof(int)));
     int *dinfo = p->info.as<int>() + fi;
     if (cusolverDnZgetrf(ctx->solver, N, N, A, N, p->lwork.as<cuDoubleComplex>(), p->ipiv.as<int>(), dinfo) !=
         CUSOLVER_STATUS_SUCCESS)
         return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
-    if (cusolverDnZgetrs(ctx->solver, CUBLAS_OP_N, N, 1, A, N, p->ipiv.as<int>(), x, N, dinfo) !=
+    if (cusolverDnZgetrs(ctx->solver, CUBLAS_OP_N, N, 1, A, N, p->ipiv.as<int>(), x, N, p->rs_info.as<int>()) !=
         CUSOLVER_STATUS_SUCCESS)
         return efie_fail(EFIE_ERR_CUSOLVER, "cuSOLVER error");
     return EFIE_OK;
@@ -505,7 +510,7 @@ int choose_batch(int N, int requested, int solver) {
     cudaGetDevice(&dev);
     freeb += efie_pool_cached(dev);   // cached blocks are available to this plan
     const double per = 26.0 * (double)N * N + 1e6;
-    int B = (int)std::floor(0.35 * (double)freeb / per);
+    int B = (int)std::floor(0.45 * (double)freeb / per);
     return std::max(1, std::min(B, EFIE_MAX_BATCH));
 }
 

@@ -5,7 +5,7 @@
 
 #include "efie_internal.h"
 
-constexpr int EFIE_MAX_BATCH = 32;
+constexpr int EFIE_MAX_BATCH = 64;
 
 // Byte offset of element (row r, k) inside a K-major 64B-swizzled FP16 tile
 // (the tensor-core operand layout): 16-byte chunk (k / 8) XOR (r / 2) mod 4,

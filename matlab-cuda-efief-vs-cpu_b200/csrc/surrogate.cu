@@ -31,7 +31,8 @@ namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16;
 
-enum Epilogue { EPI_FWD_HIDDEN = 0, EPI_FWD_OUT = 1, EPI_BWD_DZ = 2, EPI_ATOMIC = 3 };
+enum Epilogue { EPI_FWD_HIDDEN = 0, EPI_FWD_OUT = 1, EPI_BWD_DZ = 2, EPI_PARTIAL = 3 };
+constexpr int KSPLIT = 512;   // K chunk of the weight-gradient products
 
 __device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
 
@@ -45,7 +46,8 @@ __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return _
 // C[i][j] (M x N, row stride ldc) = sum_k A(i,k) B(k,j) with A(i,k) =
 // A[i*sai + k*sak] (FP32) and B(k,j) = B[k*sbk + j*sbj]; 64x64 tiles, 4x4
 // outputs per thread, FP32 accumulation.  blockIdx.z splits K in chunks of
-// kchunk (EPI_ATOMIC adds the partial sums into C).
+// kchunk; EPI_PARTIAL stores chunk z's partial product at C + z M ldc, and
+// k_sum_parts adds the chunks in order (bit-reproducible gradients).
 template <typename TB, int EPI>
 __global__ void __launch_bounds__(256) k_mlp_gemm(int M, int N, int K, const float *__restrict__ A, long sai,
                                                   long sak, const TB *__restrict__ B, long sbk, long sbj,
@@ -112,26 +114,36 @@ __global__ void __launch_bounds__(256) k_mlp_gemm(int M, int N, int K, const flo
                 const float z = Zprev[o], s = sigm(z);
                 C[o] = acc[a][b] * (s * (1.f + z * (1.f - s)));   // d silu / dz
             } else {
-                atomicAdd(C + o, acc[a][b]);
+                C[(long)blockIdx.z * M * ldc + o] = acc[a][b];
             }
         }
 }
 
-// db[j] += sum_i dZ[i][j]
+// out[e] += sum_z part[z * count + e], z in order
+__global__ void k_sum_parts(int nz, long count, const float *__restrict__ part, float *__restrict__ out) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    float t = out[e];
+    for (int z = 0; z < nz; z++) t += part[(long)z * count + e];
+    out[e] = t;
+}
+
+// db[j] += sum_i dZ[i][j]: one CTA per 32 columns, eight row lanes summed in
+// a fixed order (bit-reproducible)
 __global__ void __launch_bounds__(256) k_colsum(int M, int N, const float *__restrict__ dZ, float *__restrict__ db) {
     const int j = blockIdx.x * 32 + (threadIdx.x & 31);
     const int r = threadIdx.x >> 5;
     __shared__ float part[8][33];
     float s = 0.f;
     if (j < N)
-        for (int i = blockIdx.y * 8 + r; i < M; i += 8 * gridDim.y) s += dZ[(long)i * N + j];
+        for (int i = r; i < M; i += 8) s += dZ[(long)i * N + j];
     part[r][threadIdx.x & 31] = s;
     __syncthreads();
     if (r == 0 && j < N) {
         float t = 0.f;
 #pragma unroll
         for (int q = 0; q < 8; q++) t += part[q][threadIdx.x & 31];
-        atomicAdd(db + j, t);
+        db[j] += t;
     }
 }
 
@@ -219,6 +231,7 @@ struct efie_mlp {
     DevBuf w, wb, g, m, v;                       // params FP32, BF16 copy, grads, Adam moments
     DevBuf act;                                  // Z and A of every layer for `cap` rows
     DevBuf dz0, dz1;                             // backward ping-pong
+    DevBuf gpart;                                // K-split partials of the weight gradients
     DevBuf Xd, Td, perm, Xb, Tb, dY, step, hist, loss;
     DevBuf Xin;                                  // inference input
     int cap = 0;                                 // rows the activation buffers hold
@@ -232,7 +245,8 @@ struct efie_mlp {
     float *A(int l) { return act.as<float>() + (size_t)cap * width * (2 * l + 1); }
     float *Y() { return Z(nl - 1); }
     std::vector<void *> step_ptrs() const {
-        return {w.p, wb.p, g.p, m.p, v.p, act.p, dz0.p, dz1.p, Xd.p, Td.p, perm.p, Xb.p, Tb.p, dY.p, step.p, hist.p};
+        return {w.p,  wb.p, g.p,  m.p,  v.p,  act.p, dz0.p, dz1.p, gpart.p,
+                Xd.p, Td.p, perm.p, Xb.p, Tb.p, dY.p, step.p, hist.p};
     }
 
     ~efie_mlp() {
@@ -248,6 +262,9 @@ efie_status mlp_reserve(efie_mlp *p, int rows) {
     EFIE_TRY(p->act.reserve(sizeof(float) * (size_t)rows * width * 2 * p->nl));
     EFIE_TRY(p->dz0.reserve(sizeof(float) * (size_t)rows * width));
     EFIE_TRY(p->dz1.reserve(sizeof(float) * (size_t)rows * width));
+    size_t wmax = 0;
+    for (int l = 0; l < p->nl; l++) wmax = std::max(wmax, (size_t)p->fin[l] * p->fout[l]);
+    EFIE_TRY(p->gpart.reserve(sizeof(float) * wmax * (size_t)cdiv(rows, KSPLIT)));
     p->cap = rows;
     if (p->graph) {  // the captured step addresses the old layout
         cudaGraphExecDestroy(p->graph);
@@ -282,7 +299,7 @@ efie_status mlp_forward(efie_mlp *p, const float *X, int n) {
 // are added to p->g (the caller zeroes it).
 efie_status mlp_backward(efie_mlp *p, const float *X, const float *dY, int n) {
     cudaStream_t s = p->ctx->stream;
-    const int kchunk = 512;
+    const int kchunk = KSPLIT;
     const float *dz = dY;
     float *bufs[2] = {p->dz0.as<float>(), p->dz1.as<float>()};
     int pb = 0;
@@ -292,9 +309,11 @@ efie_status mlp_backward(efie_mlp *p, const float *X, const float *dY, int n) {
         float *gW = p->g.as<float>() + p->woff[l], *gb = p->g.as<float>() + p->boff[l];
         // dW[o][i] += sum_m dz[m][o] ain[m][i]:  A(i=o, k=m) = dz[m*fo + o], B(k=m, j=i) = ain[m*fi + i]
         dim3 gw(cdiv(fi, BN), cdiv(fo, BM), cdiv(n, kchunk));
-        k_mlp_gemm<float, EPI_ATOMIC><<<gw, 256, 0, s>>>(fo, fi, n, dz, 1, fo, ain, fi, 1, gW, fi, nullptr, nullptr,
-                                                        nullptr, kchunk);
-        k_colsum<<<dim3(cdiv(fo, 32), std::min(64, cdiv(n, 8))), 256, 0, s>>>(n, fo, dz, gb);
+        k_mlp_gemm<float, EPI_PARTIAL><<<gw, 256, 0, s>>>(fo, fi, n, dz, 1, fo, ain, fi, 1, p->gpart.as<float>(), fi,
+                                                         nullptr, nullptr, nullptr, kchunk);
+        const long cnt = (long)fo * fi;
+        k_sum_parts<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>((int)gw.z, cnt, p->gpart.as<float>(), gW);
+        k_colsum<<<dim3(cdiv(fo, 32), 1), 256, 0, s>>>(n, fo, dz, gb);
         EFIE_CUDA(cudaGetLastError());
         if (l > 0) {
             // dZ_{l-1}[m][i] = (sum_o dz[m][o] W[o][i]) * silu'(Z_{l-1}[m][i])

@@ -98,13 +98,14 @@ def design_inputs(d: PatchDesign, device=True, ctx=None):
     return dict(V=V, F=F, rwg=rwg, pe=pe, ge=ge, spread=spread, Ne=rwg["Ne"])
 
 
-def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None, ctx=None):
+def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None, ctx=None, graphs=True):
     """A SweepPlan of the design: Dunavant 7-point rule + analytic 1/R extraction."""
     x = inputs or design_inputs(d, ctx=ctx)
     r = x["rwg"]
     return SweepPlan(x["V"], x["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"],
                      r["rm"], r["Ap"], r["Am"], r["len"], None, MU0, EPS0, x["pe"], x["ge"], 1.0, x["spread"], 50.0,
-                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch), rule_order=-7, ctx=ctx)
+                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch, graphs=graphs), rule_order=-7,
+                     ctx=ctx)
 
 
 def features(d: PatchDesign, freqs):
@@ -219,8 +220,11 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
     one design (the LU's panel chain, GMRES's stop-flag polls, plan set-up on
     the host) then overlap the bulk kernels of the others.  Every design is
     solved exactly as design_plan(d).run(d.band(nfreq)) alone (the sweeps
-    share nothing).  Returns [(Ne, Zin)] in the order of ``designs``; a
-    failure in any worker is raised after all workers have stopped."""
+    share nothing).  The factorizations launch eagerly instead of replaying
+    a captured graph: a stream capture in one thread would be invalidated by
+    the device-wide synchronisation that another thread's plan release
+    performs.  Returns [(Ne, Zin)] in the order of ``designs``; a failure in
+    any worker is raised after all workers have stopped."""
     import queue
     import threading
     out = [None] * len(designs)
@@ -240,7 +244,7 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
                 except queue.Empty:
                     return
                 d = designs[i]
-                plan = design_plan(d, solver=solver, ctx=ctx)
+                plan = design_plan(d, solver=solver, ctx=ctx, graphs=False)
                 try:
                     Zin, _ = plan.run(d.band(nfreq))
                     out[i] = (plan.Ne, Zin)

@@ -224,3 +224,19 @@ def test_adaptive_sweep_beats_uniform_budget():
     # at least as well as the same number of uniform solves on nearly every design
     assert np.median(err_ad) <= 0.5
     assert np.sum(err_ad <= err_un + 0.5) >= 6
+
+
+@pytest.mark.gpu
+def test_gradients_are_bit_reproducible():
+    """The weight gradients' K-split partial products are added in a fixed
+    order (no atomics), as are the bias gradients' column sums: the same
+    minibatch gives the same gradient bit for bit."""
+    s = _sur()
+    net = s.Surrogate(seed=4)
+    rng = np.random.default_rng(9)
+    X = rng.uniform(-1, 1, (1500, 5)).astype(np.float32)    # three K chunks of 512 rows
+    T = rng.standard_normal((1500, 3)).astype(np.float32)
+    l1, g1 = net.loss_grad(X, T)
+    l2, g2 = net.loss_grad(X, T)
+    assert l1 == l2 and np.array_equal(g1, g2)
+    net.close()
