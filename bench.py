@@ -432,7 +432,8 @@ def run_ours(args):
     tuned = importlib.import_module(PKG + ".autotune").tuned_opts(inp["Ne"])
     tiles = (args.tile_chain or (tuned[2] if tuned else 0), args.tile_bulk or (tuned[3] if tuned else 0))
     opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
-                        batch=B if B < 8 else 0, lu_nb=args.lu_nb, tile_chain=tiles[0], tile_bulk=tiles[1])
+                        batch=B if B < 8 else 0, lu_nb=args.lu_nb, tile_chain=tiles[0], tile_bulk=tiles[1],
+                        resident_chain=args.resident_chain, nfreq_hint=B)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -750,6 +751,8 @@ def main():
                     help="tensor-core tile width of the LU's K = 64 updates (0: the autotuner's table)")
     ap.add_argument("--tile-bulk", type=int, default=0, choices=[0, 128, 256],
                     help="tensor-core tile width of the outer panels' updates (0: the autotuner's table)")
+    ap.add_argument("--resident-chain", type=int, default=0, choices=[0, 1],
+                    help="1: the LU's K = 64 updates on resident, pipelined CTA pairs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the plain FP64 GPU path on the same points")
     ap.add_argument("--no-secondary", action="store_true",

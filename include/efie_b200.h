@@ -164,7 +164,9 @@ typedef struct efie_sweep_opts {
     int32_t refine_max_iter; /* default 30                                      */
     int32_t lu_nb;           /* outer LU panel width 64/128/256/512 (0 = tuned) */
     int32_t timing;          /* 1 = record per-phase CUDA-event timings         */
-    int32_t batch;           /* frequencies solved together (0 = automatic)     */
+    int32_t batch;           /* frequencies solved together (0 = automatic: up to
+                                64 from Ne 4096 on, 32 below, within 45 % of free
+                                device memory)                                  */
     int32_t refine_method;   /* efie_refine_method; default EFIE_REFINE_GMRES    */
     int32_t graphs;          /* 1 (default): with timing off, the mixed LU of a
                                 batch replays a CUDA graph captured on the
@@ -172,6 +174,14 @@ typedef struct efie_sweep_opts {
     int32_t tile_chain;      /* complex columns of the tensor-core tile of the LU's
                                 K = 64 panel-chain updates: 128 or 256 (0 = tuned) */
     int32_t tile_bulk;       /* ... of the outer panels' trailing updates (0 = tuned) */
+    int32_t resident_chain;  /* 1: the K = 64 chain updates run on resident CTA pairs
+                                that overlap each 256 x 128 tile's TMEM drain with the
+                                next tile's MMAs (tile_chain is then unused); 0: one
+                                tile per CTA pair (default)                    */
+    int32_t nfreq_hint;      /* frequencies the plan's sweeps will solve (0 = unknown):
+                                with batch = 0, the automatic batch is cut to the
+                                balanced size for that many; efie_patch_sweep_fastquad
+                                sets it to Nf                                   */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */
@@ -377,13 +387,9 @@ efie_status efie_debug_set_wait_test(int32_t enable, int64_t spins);
 
 /* Tensor-core tile widths (128 or 256 complex columns per CTA pair; anything
  * else: 256) of efie_lu_selftest's K = 64 chain updates and outer-panel
- * updates, process-wide.  No counterpart in the reference. */
-void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk);
-
-/* Lanes per triangle pair of the multi-frequency regular-pair kernel: 2 (the
- * default: the pair's frequencies split over two lanes) or 1, process-wide;
- * the two give the same values.  No counterpart in the reference. */
-void efie_debug_set_regular_lanes(int lanes);
+ * updates, and resident_chain (efie_sweep_opts), process-wide.  No
+ * counterpart in the reference. */
+void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk, int resident_chain);
 
 /* 1 makes efie_plan_run take its batches in frequency order with every
  * refinement starting from zero, instead of coarse to fine with initial

@@ -45,7 +45,7 @@ class EfieSweepOpts(C.Structure):
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
                 ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
                 ("refine_method", C.c_int32), ("graphs", C.c_int32), ("tile_chain", C.c_int32),
-                ("tile_bulk", C.c_int32)]
+                ("tile_bulk", C.c_int32), ("resident_chain", C.c_int32), ("nfreq_hint", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
@@ -129,8 +129,7 @@ SIGNATURES = {
     "efie_debug_disable_tensor_cores": (None, [C.c_int]),
     "efie_debug_disable_symmetric_lu": (None, [C.c_int]),
     "efie_debug_set_selftest_panel": (None, [C.c_int]),
-    "efie_debug_set_selftest_tiles": (None, [C.c_int, C.c_int]),
-    "efie_debug_set_regular_lanes": (None, [C.c_int]),
+    "efie_debug_set_selftest_tiles": (None, [C.c_int, C.c_int, C.c_int]),
     "efie_debug_disable_warm_start": (None, [C.c_int]),
     "efie_debug_set_wait_test": (C.c_int, [C.c_int32, C.c_int64]),
     "efie_gassemble_zv_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_int32] + [_P] * 12 +

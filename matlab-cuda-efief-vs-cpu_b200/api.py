@@ -290,7 +290,8 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # Sweeps
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
-               timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True, tile_chain=0, tile_bulk=0):
+               timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True, tile_chain=0, tile_bulk=0,
+               resident_chain=0, nfreq_hint=0):
     """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
     scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only),
     tile_chain / tile_bulk: tensor-core tile widths 128 | 256 (0 = tuned)."""
@@ -308,6 +309,8 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.graphs = 1 if graphs else 0
     o.tile_chain = int(tile_chain)
     o.tile_bulk = int(tile_bulk)
+    o.resident_chain = int(resident_chain)
+    o.nfreq_hint = int(nfreq_hint)
     return o
 
 

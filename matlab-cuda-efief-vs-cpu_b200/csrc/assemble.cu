@@ -248,121 +248,6 @@ __global__ void __launch_bounds__(256) k_regular_moments_mf(
     for (int f = 0; f < F; f++) store_mom(ms.s[f], slot, t1, t2, m[f]);
 }
 
-// The same evaluation with every triangle pair on two lanes (lanes 2i, 2i + 1
-// of a warp): both form R, 1/(4 pi R) and the weights; the even lane takes the
-// sincos (and exp) of k0 R, the odd lane that of dk R, and one shuffle each
-// way hands the even lane e^{-j dk R} and the odd lane e^{-j k0 R}.  The even
-// lane accumulates frequencies 0 .. H-1, the odd lane H .. F-1 (H = ceil(F/2)),
-// reaching e^{-j k_f R} by the same chain of complex multiplications as the
-// one-lane kernel.  A lane then holds the moments of at most H frequencies:
-// half the registers, twice the resident warps, half the transcendental work
-// per lane.  CTA of 128 threads, tile 8 (t1) x 8 (t2) pairs: the 3-point
-// rule's state (about 144 registers) then fits three CTAs on an SM, 12
-// resident warps against the one-lane kernel's 8.
-template <int NQ, int F>
-__global__ void __launch_bounds__(128) k_regular_moments_mf2(
-    int Nt, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
-    const uint8_t *__restrict__ skip, double kr0, double ki0, double dkr, double dki, MomStores ms) {
-    constexpr int H = (F + 1) / 2;
-    __shared__ double4 sp[8][NQ];
-    __shared__ double4 so[8];
-    const int half = threadIdx.x & 1, pr = threadIdx.x >> 1;
-    const int tx = pr & 7, ty = pr >> 3;
-    const int t1 = blockIdx.x * 8 + tx;
-    const int t2b = blockIdx.y * 8;
-    if (sym && blockIdx.x * 8 > t2b + 7) return;  // whole tile below the diagonal
-    for (int i = threadIdx.x; i < 8 * NQ; i += blockDim.x) {
-        int tt = t2b + i / NQ;
-        sp[i / NQ][i % NQ] = tt < Nt ? pts[(size_t)tt * NQ + i % NQ] : make_double4(0, 0, 0, 0);
-    }
-    if (threadIdx.x < 8) {
-        int tt = t2b + threadIdx.x;
-        so[threadIdx.x] = tt < Nt ? origin[tt] : make_double4(0, 0, 0, 0);
-    }
-    __syncthreads();
-    const int t2 = t2b + ty;
-    // both lanes of a pair take the same branch, so the pair-wise shuffles
-    // below always find their partner
-    if (t1 >= Nt || t2 >= Nt) return;
-    if (sym && t1 > t2) return;
-    if (skip[(size_t)t1 + (size_t)Nt * t2]) return;
-    const unsigned pmask = 3u << (threadIdx.x & 30);
-    double4 p1[NQ];
-#pragma unroll
-    for (int p = 0; p < NQ; p++) p1[p] = pts[(size_t)t1 * NQ + p];
-    const double4 o1 = origin[t1], o2 = so[ty];
-    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
-    const double kmine = half ? dkr : kr0, kimine = half ? dki : ki0;
-    double m[H][16];
-#pragma unroll
-    for (int f = 0; f < H; f++)
-#pragma unroll
-        for (int i = 0; i < 16; i++) m[f][i] = 0.0;
-#pragma unroll 1
-    for (int q = 0; q < NQ; q++) {
-        const double4 pq = sp[ty][q];
-        const double ax = dox - pq.x, ay = doy - pq.y, az = doz - pq.z;
-#pragma unroll
-        for (int p = 0; p < NQ; p++) {
-            const double dx = ax + p1[p].x, dy = ay + p1[p].y, dz = az + p1[p].z;
-            double R = sqrt(dx * dx + dy * dy + dz * dz);
-            R = fmax(R, 1e-15);
-            double inv = p1[p].w * pq.w / (4.0 * kPi * R);
-            double sn, cn;
-            sincos(kmine * R, &sn, &cn);
-            // even lane: e^{-j k0 R} / (4 pi R) with the weights; odd lane: e^{-j dk R}
-            double vr, vi;
-            if (!half) {
-                if (ki0 != 0.0) inv *= exp(ki0 * R);
-                vr = cn * inv;
-                vi = -sn * inv;
-            } else {
-                vr = cn;
-                vi = -sn;
-                if (kimine != 0.0) {
-                    const double e = exp(kimine * R);
-                    vr *= e;
-                    vi *= e;
-                }
-            }
-            const double ur = __shfl_xor_sync(pmask, vr, 1), ui = __shfl_xor_sync(pmask, vi, 1);
-            const double esr = half ? vr : ur, esi = half ? vi : ui;   // e^{-j dk R}
-            double gr = half ? ur : vr, gi = half ? ui : vi;            // frequency 0
-            if (half) {   // the odd lane starts at frequency H
-#pragma unroll
-                for (int t = 0; t < H; t++) {
-                    const double nr = gr * esr - gi * esi;
-                    gi = gr * esi + gi * esr;
-                    gr = nr;
-                }
-            }
-            const double dd = p1[p].x * pq.x + p1[p].y * pq.y + p1[p].z * pq.z;
-            // the same H slots on both lanes (a slot past F on the odd lane
-            // accumulates a value that is never stored)
-#pragma unroll
-            for (int f = 0; f < H; f++) {
-                m[f][0] += gr; m[f][1] += gi;
-                m[f][2] += gr * p1[p].x; m[f][3] += gi * p1[p].x;
-                m[f][4] += gr * p1[p].y; m[f][5] += gi * p1[p].y;
-                m[f][6] += gr * p1[p].z; m[f][7] += gi * p1[p].z;
-                m[f][8] += gr * pq.x; m[f][9] += gi * pq.x;
-                m[f][10] += gr * pq.y; m[f][11] += gi * pq.y;
-                m[f][12] += gr * pq.z; m[f][13] += gi * pq.z;
-                m[f][14] += gr * dd; m[f][15] += gi * dd;
-                if (f + 1 < H) {
-                    const double nr = gr * esr - gi * esi;
-                    gi = gr * esi + gi * esr;
-                    gr = nr;
-                }
-            }
-        }
-    }
-    const size_t slot = pair_slot(t1, t2, Nt, sym);
-#pragma unroll
-    for (int f = 0; f < H; f++)
-        if (half * H + f < F) store_mom(ms.s[half * H + f], slot, t1, t2, m[f]);
-}
-
 // Generic point count (any Nq a prepack may carry).
 __global__ void __launch_bounds__(256) k_regular_moments_any(
     int Nt, int Nq, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
@@ -1103,37 +988,23 @@ double regular_pairs(const GeomDev &g) {
     return g.scheme == EFIE_SCHEME_EXTRACT ? all - (double)g.n_adj : all - (double)g.n_near - (double)g.Nt;
 }
 
-static bool g_mf_one_lane = false;   // the one-lane multi-frequency kernel (efie_debug_set_regular_lanes)
-
 template <int F>
 void launch_regular_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, const MomStores &ms) {
+    dim3 grid((g.Nt + 31) / 32, (g.Nt + 7) / 8);
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
     const double dkr = (ph[F - 1].kr - ph[0].kr) / (F - 1), dki = (ph[F - 1].ki - ph[0].ki) / (F - 1);
-    if (g_mf_one_lane) {
-        dim3 grid((g.Nt + 31) / 32, (g.Nt + 7) / 8);
-        if (g.Nq == 3)
-            k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki,
-                                                            dkr, dki, ms);
-        else if (g.Nq == 7)
-            k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki,
-                                                            dkr, dki, ms);
-        return;
+    switch (g.Nq) {
+    case 3:
+        k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
+                                                        dki, ms);
+        break;
+    case 7:
+        k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
+                                                        dki, ms);
+        break;
     }
-    dim3 grid((g.Nt + 7) / 8, (g.Nt + 7) / 8);
-    if (g.Nq == 3)
-        k_regular_moments_mf2<3, F><<<grid, 128, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
-                                                         dki, ms);
-    else if (g.Nq == 7)
-        k_regular_moments_mf2<7, F><<<grid, 128, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
-                                                         dki, ms);
 }
-
-}  // namespace
-
-extern "C" void efie_debug_set_regular_lanes(int lanes) { g_mf_one_lane = lanes == 1; }
-
-namespace {
 
 // k_f = k0 + f dk within 1e-12 |k_f| for f < n
 bool equally_spaced(const Physics *ph, int n) {

@@ -70,6 +70,8 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->batch = 0;
     o->tile_chain = 0;
     o->tile_bulk = 0;
+    o->resident_chain = 0;
+    o->nfreq_hint = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -500,8 +502,13 @@ efie_status plan_solve_fp64(efie_plan *p, int slot, int fi) {
 }
 
 // Frequencies per batch: everything a frequency needs on the device (Z in
-// complex128, its complex64 planes, staging) within a fraction of free HBM.
-int choose_batch(int N, int requested, int solver) {
+// complex128, its complex64 planes, staging) within a fraction of free HBM,
+// at most 64 frequencies from Ne 4096 on (where the LU's panel chain is long
+// enough that paying it for fewer batches wins) and 32 below (where more,
+// smaller batches give more warm-started GMRES runs).  With the number of
+// frequencies a sweep will solve (nf > 0), the slots are cut to the balanced
+// batch size of that many batches: no slot stays idle.
+int choose_batch(int N, int requested, int solver, int nf) {
     if (solver == EFIE_SOLVER_FP64) return 1;
     if (requested > 0) return std::min(requested, EFIE_MAX_BATCH);
     size_t freeb = 0, total = 0;
@@ -511,7 +518,12 @@ int choose_batch(int N, int requested, int solver) {
     freeb += efie_pool_cached(dev);   // cached blocks are available to this plan
     const double per = 26.0 * (double)N * N + 1e6;
     int B = (int)std::floor(0.45 * (double)freeb / per);
-    return std::max(1, std::min(B, EFIE_MAX_BATCH));
+    B = std::max(1, std::min(B, N >= 4096 ? EFIE_MAX_BATCH : 32));
+    if (nf > 0) {
+        const int nbat = (nf + B - 1) / B;
+        B = (nf + nbat - 1) / nbat;
+    }
+    return B;
 }
 
 // Outer LU panel width: the caller's choice, else the tuned table (wider
@@ -555,7 +567,7 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         bn += rhs[e] * rhs[e];
     }
     p->bnorm = std::sqrt(bn);
-    p->B = choose_batch(N, p->opts.batch, p->opts.solver);
+    p->B = choose_batch(N, p->opts.batch, p->opts.solver, p->opts.nfreq_hint);
     EFIE_TRY(p->Z.reserve(sizeof(efie_c128) * (size_t)N * N * p->B));
     EFIE_TRY(p->b.reserve(sizeof(efie_c128) * N));
     EFIE_TRY(p->x.reserve(sizeof(efie_c128) * (size_t)N * p->B));
@@ -567,6 +579,7 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         EFIE_TRY(efie_mixed_workspace(p->sw, N, p->B, choose_panel(N, p->opts.lu_nb)));
         p->sw.tn_chain = choose_tile(p->opts.tile_chain);
         p->sw.tn_bulk = choose_tile(p->opts.tile_bulk);
+        p->sw.resident_chain = p->opts.resident_chain == 1;
     }
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
@@ -892,6 +905,7 @@ extern "C" efie_status efie_patch_sweep_fastquad(efie_ctx *ctx, const efie_mesh 
     if (opts) o = *opts;
     else efie_sweep_opts_default(&o);
     o.scheme = EFIE_SCHEME_REF;
+    if (o.nfreq_hint <= 0) o.nfreq_hint = Nf;   // one call, one sweep: size the batches for it
     EFIE_TRY(efie_plan_create(ctx, mesh, pre, mu, eps, patchEdge, groundEdge, V0, spreadRadius, Z0, &o, 0, &p));
     efie_status s = efie_plan_run(p, freqs, Nf, Zin, S11, I, stats);
     efie_plan_destroy(p);
@@ -944,13 +958,14 @@ extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh 
 // Self-test of the complex64 LU (no pivoting) used by the mixed solver.
 // ---------------------------------------------------------------------------
 static int g_selftest_nb = 256;
-static int g_selftest_tile[2] = {256, 256};
+static int g_selftest_tile[3] = {256, 256, 0};
 extern "C" void efie_debug_set_selftest_panel(int lu_nb) {
     g_selftest_nb = (lu_nb == 64 || lu_nb == 128 || lu_nb == 256 || lu_nb == 512) ? lu_nb : 256;
 }
-extern "C" void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk) {
+extern "C" void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk, int resident_chain) {
     g_selftest_tile[0] = choose_tile(tile_chain);
     g_selftest_tile[1] = choose_tile(tile_bulk);
+    g_selftest_tile[2] = resident_chain == 1;
 }
 
 extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores,
@@ -962,6 +977,7 @@ extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c12
     EFIE_TRY(efie_mixed_workspace(w, N, 1, g_selftest_nb));
     w.tn_chain = g_selftest_tile[0];
     w.tn_bulk = g_selftest_tile[1];
+    w.resident_chain = g_selftest_tile[2] != 0;
     // a bit-exactly symmetric A takes the symmetric factorization, as a
     // sweep's Z from the symmetric gather does
     bool sym = true;

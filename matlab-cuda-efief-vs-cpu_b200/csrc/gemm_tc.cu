@@ -544,6 +544,263 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Resident CTA pairs for the panel chain's K = 64 updates.  With K = 64 a
+// tile's MMAs take a few microseconds while the fixed phases around them
+// (cluster launch, TMEM allocation, first operand loads, the TMEM drain and
+// the reductions) take longer.  Here each CTA pair stays resident and walks
+// its tiles t = pair, pair + pairs, ... (256 x 128 tiles over every
+// frequency of the update), with the phases of consecutive tiles overlapped:
+//   * warp 0, lane 0 (both CTAs): producer -- the operand chunks of the next
+//     tiles into a 3-stage ring as soon as the MMAs free a stage;
+//   * warp 1, lane 0: the even CTA issues the MMAs of tile i into TMEM buffer
+//     i mod 2 (two buffers of 256 columns: real and imaginary 128 x 128 per
+//     CTA); the odd CTA forwards its chunk arrivals to the even CTA;
+//   * warps 4-7 (both CTAs): epilogue -- drain buffer i mod 2 (lane quarter
+//     warp - 4, real then imaginary part), scale, stage in shared memory and
+//     reduce into C with bulk tensor reductions, then hand the buffer back to
+//     the MMA thread (tempty, 4 arrivals from each CTA on the even CTA's
+//     barrier), so the drain of tile i overlaps the MMAs of tile i + 1.
+// The arithmetic per element is the kernel above's (same MMA order, same
+// scaling), so the results are identical.  Every wait is bounded; a timeout
+// marks every active frequency of the update failed and all roles stop.
+// ---------------------------------------------------------------------------
+constexpr int PBN = 128;
+constexpr int PNST = 3;
+using PT = Tile<PBN>;
+constexpr int PNBAR = 3 * PNST + 4;                                  // full, empty, pfull, tfull[2], tempty[2]
+constexpr int PEPI_FLOATS = 4 * 4 * 1024;                            // 4 warps x 4 staged 32 x 32 tiles
+constexpr size_t PIPE_SMEM = sizeof(__half) * PNST * PT::STAGE + sizeof(float) * PEPI_FLOATS + 1024 +
+                             8 * (PNBAR + 3) + sizeof(float) * 4 * 2 * PBN;
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+    k_update_tc_pipe(const __grid_constant__ CUtensorMap cmap, int N, int B, int r0, int r1, int c0, int c1,
+                     int nchunk, const __half *__restrict__ Lpackb, size_t lstride, int lpitch, int loff,
+                     const __half *__restrict__ Upackb, size_t ustride, int upitch, int uoff,
+                     const float *__restrict__ lmaxb, const float *__restrict__ umaxb, size_t mstride, int nblk,
+                     int kcol, int krow, int K, int ld, char *__restrict__ ctl, const int *__restrict__ active) {
+    const int npr = (r1 - r0 + TM - 1) / TM, nct = (c1 - c0 + PBN - 1) / PBN;
+    const int per_f = npr * nct, ntiles = per_f * B;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    extern __shared__ uint8_t dyn_raw[];
+    __half *stage = reinterpret_cast<__half *>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~(uintptr_t)1023);
+    float *epi = reinterpret_cast<float *>(stage + PNST * PT::STAGE);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(epi + PEPI_FLOATS);
+    uint64_t *full = bars, *empty = bars + PNST, *pfull = bars + 2 * PNST, *tfull = bars + 3 * PNST,
+             *tempty = tfull + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + PNBAR);
+    volatile int *abort_sh = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    // [epilogue warp][2][PBN] inverse column scales (16-byte aligned)
+    float *colsc = reinterpret_cast<float *>(bars + PNBAR + 3);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    auto errp = [&](int f) { return reinterpret_cast<int *>(ctl + 64 * f + 36); };
+    auto fail_all = [&]() {
+        *abort_sh = 1;
+        for (int f = 0; f < B; f++)
+            if (active[f]) atomicExch(errp(f), 3);
+    };
+
+    if (tid == 0) {
+        for (int i = 0; i < PNBAR; i++) mbar_init(&bars[i], i >= 3 * PNST + 2 ? 8 : 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *abort_sh = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(4 * PBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    cluster_sync();   // barriers initialised and TMEM allocated in both CTAs
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        constexpr uint32_t sbytes = sizeof(__half) * SUB, ubytes = sizeof(__half) * PT::USUB;
+        long long g = 0;
+        for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
+            const int f = t / per_f, rr = t - f * per_f, rp = rr / nct, ct = rr - rp * nct;
+            if (!active[f]) continue;
+            const __half *gl = Lpackb + lstride * f + (size_t)(loff + (rp * 2 + (int)rank) * TR) * KC;
+            const __half *gu = Upackb + ustride * f + (size_t)(uoff + ct * PBN + (int)rank * PT::UH) * KC;
+            for (int c = 0; c < nchunk; c++, g++) {
+                const int sidx = (int)(g % PNST);
+                if (g >= PNST && !mbar_wait(&empty[sidx], (uint32_t)((g / PNST - 1) & 1), errp(f))) {
+                    fail_all();
+                    break;
+                }
+                __half *st = stage + sidx * PT::STAGE;
+                mbar_expect_tx(&full[sidx], 4 * (sbytes + ubytes));
+                for (int comp = 0; comp < 4; comp++) {
+                    bulk_g2s(st + comp * SUB, gl + (size_t)(c * 4 + comp) * lpitch * KC, sbytes, &full[sidx]);
+                    bulk_g2s(st + CHUNK_HALVES + comp * PT::USUB, gu + (size_t)(c * 4 + comp) * upitch * KC, ubytes,
+                             &full[sidx]);
+                }
+            }
+        }
+    } else if (warp == 1 && lane == 0 && leader) {
+        // MMA issuer
+        const uint32_t tf_peer = peer_addr(tfull, 1);
+        long long g = 0;
+        int i = 0;
+        for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
+            const int f = t / per_f;
+            if (!active[f]) continue;
+            const int b = i & 1;
+            if (!mbar_wait(&tempty[b], (uint32_t)(((i >> 1) & 1) ^ 1), errp(f))) {
+                fail_all();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dre = tmem + (uint32_t)(b * 2 * PBN), dim = dre + PBN;
+            bool ok = true;
+            for (int c = 0; c < nchunk; c++, g++) {
+                const int sidx = (int)(g % PNST);
+                const uint32_t par = (uint32_t)((g / PNST) & 1);
+                if (!mbar_wait(&full[sidx], par, errp(f)) || !mbar_wait(&pfull[sidx], par, errp(f))) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const __half *st = stage + sidx * PT::STAGE;
+                const uint64_t lrh = desc_sw64(st), lrl = desc_sw64(st + SUB), lih = desc_sw64(st + 2 * SUB),
+                               lil = desc_sw64(st + 3 * SUB);
+                const __half *su = st + CHUNK_HALVES;
+                const uint64_t urh = desc_sw64(su), url = desc_sw64(su + PT::USUB),
+                               uih = desc_sw64(su + 2 * PT::USUB), uil = desc_sw64(su + 3 * PT::USUB);
+                constexpr uint32_t IDESC = Idesc<PBN>::POS, IDESC_NEG_A = Idesc<PBN>::NEG_A;
+#pragma unroll
+                for (int kk = 0; kk < KC / 16; kk++) {
+                    const uint64_t a = (uint64_t)((kk * 32) >> 4);
+                    const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
+                    mma_pair(dre, lrl + a, urh + a, IDESC, acc0);
+                    mma_pair(dre, lrh + a, url + a, IDESC, 1u);
+                    mma_pair(dre, lil + a, uih + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lih + a, uil + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lih + a, uih + a, IDESC_NEG_A, 1u);
+                    mma_pair(dre, lrh + a, urh + a, IDESC, 1u);
+                    mma_pair(dim, lrl + a, uih + a, IDESC, acc0);
+                    mma_pair(dim, lrh + a, uil + a, IDESC, 1u);
+                    mma_pair(dim, lil + a, urh + a, IDESC, 1u);
+                    mma_pair(dim, lih + a, url + a, IDESC, 1u);
+                    mma_pair(dim, lih + a, urh + a, IDESC, 1u);
+                    mma_pair(dim, lrh + a, uih + a, IDESC, 1u);
+                }
+                mma_commit(smem_u32(&empty[sidx]));
+                mma_commit(peer_addr(&empty[sidx], 1));
+            }
+            if (!ok) {
+                fail_all();
+                break;
+            }
+            // buffer b complete in both CTAs
+            mma_commit(smem_u32(&tfull[b]));
+            mma_commit(tf_peer + 8u * (uint32_t)b);
+            i++;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // the odd CTA: forward the arrival of each chunk to the even CTA
+        const uint32_t pf0 = peer_addr(pfull, 0);
+        long long g = 0;
+        for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
+            const int f = t / per_f;
+            if (!active[f]) continue;
+            bool ok = true;
+            for (int c = 0; c < nchunk; c++, g++) {
+                const int sidx = (int)(g % PNST);
+                if (!mbar_wait(&full[sidx], (uint32_t)((g / PNST) & 1), errp(f))) {
+                    ok = false;
+                    break;
+                }
+                mbar_arrive_remote(pf0 + 8u * (uint32_t)sidx);
+            }
+            if (!ok) {
+                fail_all();
+                break;
+            }
+        }
+    } else if (warp >= 4) {
+        // epilogue: lane quarter q of the TMEM accumulators
+        const int q = warp - 4;
+        const uint32_t te0 = peer_addr(tempty, 0);
+        float *ring = epi + q * 4 * 1024;
+        float *wcs = colsc + q * 2 * PBN;   // this warp's copy: no barrier across the epilogue warps
+        int staged = 0, i = 0;
+        for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
+            const int f = t / per_f, rr = t - f * per_f, rp = rr / nct, ct = rr - rp * nct;
+            if (!active[f]) continue;
+            const int b = i & 1;
+            const float *lm = lmaxb + mstride * f, *um = umaxb + mstride * f;
+            // inverse column scales of this tile (the warp's slot b, read last by tile i - 2)
+            for (int e = lane; e < PBN; e += 32) {
+                const int col = c0 + ct * PBN + e;
+                wcs[b * PBN + e] =
+                    col < c1 ? 1.f / pow2_scale(col_max(um, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
+            }
+            __syncwarp();
+            bool have = mbar_wait(&tfull[b], (uint32_t)((i >> 1) & 1), errp(f));
+            have = __all_sync(0xffffffffu, have);
+            if (!have) {
+                if (lane == 0) fail_all();
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int rowq = r0 + (rp * 2 + (int)rank) * TR + q * 32;
+            const int ncol = c1 - (c0 + ct * PBN);
+            if (rowq < r1) {   // warp-uniform
+                const int row = rowq + lane;
+                const float rs =
+                    row < r1 ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
+#pragma unroll 1
+                for (int pl = 0; pl < 2; pl++) {
+                    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 2 * PBN + pl * PBN);
+#pragma unroll 1
+                    for (int j = 0; j < PBN / 32 && j * 32 < ncol; j++) {
+                        uint32_t v[32];
+                        tmem_ld32(tbase + j * 32, v);
+                        float *tile = ring + (staged & 3) * 1024;
+                        if (staged >= 4) {   // the reduction that read this tile four tiles ago is done with it
+                            if (lane == 0) bulk_wait_read<3>();
+                            __syncwarp();
+                        }
+#pragma unroll
+                        for (int qq = 0; qq < 8; qq++) {
+                            const float4 cs = *reinterpret_cast<const float4 *>(wcs + b * PBN + j * 32 + 4 * qq);
+                            const float s0 = rs * cs.x, s1 = rs * cs.y, s2 = rs * cs.z, s3 = rs * cs.w;
+                            float4 x;
+                            x.x = s0 != 0.f ? -__uint_as_float(v[4 * qq]) * s0 : 0.f;
+                            x.y = s1 != 0.f ? -__uint_as_float(v[4 * qq + 1]) * s1 : 0.f;
+                            x.z = s2 != 0.f ? -__uint_as_float(v[4 * qq + 2]) * s2 : 0.f;
+                            x.w = s3 != 0.f ? -__uint_as_float(v[4 * qq + 3]) * s3 : 0.f;
+                            *reinterpret_cast<float4 *>(tile + lane * 32 + ((qq ^ (lane & 7)) << 2)) = x;
+                        }
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) reduce_add_tile(&cmap, tile, c0 + ct * PBN + j * 32, rowq, pl, f);
+                        staged++;
+                    }
+                }
+            }
+            // buffer b drained in this CTA: hand it back to the MMA thread
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(te0 + 8u * (uint32_t)b);
+            i++;
+        }
+        if (lane == 0) bulk_wait_read<0>();   // shared memory is read before the CTA exits
+        __syncwarp();
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    cluster_sync();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * PBN));
+    }
+}
+
 }  // namespace
 
 static bool g_tc_disabled = false;
@@ -555,6 +812,7 @@ efie_status efie_tc_attrs() {
                                    (int)Tile<256>::SMEM));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)Tile<128>::SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     done = true;
     return EFIE_OK;
 }
@@ -666,6 +924,25 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
     if (!efie_gemm_uses_tc(rows, cols, K)) {
         for (int k0 = 0; k0 < K; k0 += 64)
             EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
+        return EFIE_OK;
+    }
+    if (K <= 64 && tri_kb == 0 && w.resident_chain) {
+        // the panel chain's updates on resident CTA pairs, 256 x 128 tiles
+        if (!Lv.base || !Uv.base || (Lv.off & 7) || (Uv.off & 7) ||
+            Lv.off + (rows + TM - 1) / TM * TM > Lv.pitch || Uv.off + (cols + PBN - 1) / PBN * PBN > Uv.pitch)
+            return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: packed operands do not cover the block");
+        EFIE_TRY(efie_tc_attrs());
+        cudaStream_t st = ctx->stream;
+        const long long ntiles = (long long)((rows + TM - 1) / TM) * ((cols + PBN - 1) / PBN) * w.B;
+        const int pairs = (int)std::min<long long>(std::max(1, ctx->num_sms / 2), ntiles);
+        size_t tok = ctx->log.begin(st);
+        k_update_tc_pipe<<<2 * pairs, 256, PIPE_SMEM, st>>>(
+            *reinterpret_cast<const CUtensorMap *>(w.planes_map), w.N, w.B, r0, r1, c0, c1, (K + KC - 1) / KC,
+            static_cast<const __half *>(Lv.base), Lv.stride, Lv.pitch, Lv.off, static_cast<const __half *>(Uv.base),
+            Uv.stride, Uv.pitch, Uv.off, w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K,
+            w.ld, w.ctl.as<char>(), w.active.as<int>());
+        EFIE_CUDA(cudaGetLastError());
+        ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
         return EFIE_OK;
     }
     // tile width of the pair: the panel chain's K = 64 updates and the outer

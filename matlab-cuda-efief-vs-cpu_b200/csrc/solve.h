@@ -34,6 +34,7 @@ struct SolveWork {
     int kb_outer = 256;       // outer panel width of the two-level LU (K of the big updates)
     int tn_chain = 256;       // tile width (complex columns per CTA pair) of the K = 64 updates
     int tn_bulk = 256;        // ... and of the outer panels' updates
+    bool resident_chain = false;   // K = 64 updates on resident, pipelined CTA pairs (k_update_tc_pipe)
     DevBuf planes;   // per f: float re[N][ld], im[N][ld]  (row-major)
     DevBuf dinv;     // per f: float2 [nblk][2][NB*NB] (L^-1, U^-1 of each diagonal block)
     DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]

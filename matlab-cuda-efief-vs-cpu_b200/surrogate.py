@@ -98,13 +98,15 @@ def design_inputs(d: PatchDesign, device=True, ctx=None):
     return dict(V=V, F=F, rwg=rwg, pe=pe, ge=ge, spread=spread, Ne=rwg["Ne"])
 
 
-def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None, ctx=None, graphs=True):
-    """A SweepPlan of the design: Dunavant 7-point rule + analytic 1/R extraction."""
+def design_plan(d: PatchDesign, solver="mixed", batch=0, inputs=None, ctx=None, graphs=True, nfreq=0):
+    """A SweepPlan of the design: Dunavant 7-point rule + analytic 1/R extraction
+    (``nfreq``: the points its sweeps will solve, to size the batches)."""
     x = inputs or design_inputs(d, ctx=ctx)
     r = x["rwg"]
     return SweepPlan(x["V"], x["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"],
                      r["rm"], r["Ap"], r["Am"], r["len"], None, MU0, EPS0, x["pe"], x["ge"], 1.0, x["spread"], 50.0,
-                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch, graphs=graphs), rule_order=-7,
+                     opts=sweep_opts(solver=solver, scheme="extract", batch=batch, graphs=graphs, nfreq_hint=nfreq),
+                     rule_order=-7,
                      ctx=ctx)
 
 
@@ -208,13 +210,33 @@ class Surrogate:
 # ---------------------------------------------------------------------------
 # Design families: several designs in flight at once
 # ---------------------------------------------------------------------------
+_worker_ctx = {}   # (device, worker) -> context of a sweep_family worker, kept for later calls
+
+
+def _worker_context(device, w):
+    key = (device, w)
+    if key not in _worker_ctx:
+        if not _worker_ctx:
+            import atexit
+            atexit.register(_release_worker_contexts)
+        _worker_ctx[key] = nat.new_context(device)
+    return _worker_ctx[key]
+
+
+def _release_worker_contexts():
+    for h in _worker_ctx.values():
+        nat.destroy_context(h)
+    _worker_ctx.clear()
+
+
 def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=None):
     """Zin over each design's band (``d.band(nfreq)``) for a family of
     designs of uneven Ne, ``workers`` designs in flight at once.
 
     Each worker is a host thread with a library context of its own (its own
     CUDA stream -- ``streams[w]`` when given, a ``cudaStream_t`` --, solver
-    handle and look-ahead streams): it meshes its next design on the GPU,
+    handle and look-ahead streams; the contexts are kept for later calls and
+    released at exit): it meshes its next design on the GPU,
     creates the plan (extraction scheme), sweeps and releases it, while the
     other workers' designs run on their streams.  The latency-bound phases of
     one design (the LU's panel chain, GMRES's stop-flag polls, plan set-up on
@@ -233,18 +255,19 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
         todo.put(i)
     errors = []
 
+    ctxs = [_worker_context(device, w) for w in range(max(1, workers))]   # created in this thread
+
     def work(w):
-        ctx = nat.new_context(device)
+        ctx = ctxs[w]
         try:
-            if streams is not None:
-                nat.check(nat.lib().efie_ctx_set_stream(ctx, streams[w]))
+            nat.check(nat.lib().efie_ctx_set_stream(ctx, streams[w] if streams is not None else None))
             while not errors:
                 try:
                     i = todo.get_nowait()
                 except queue.Empty:
                     return
                 d = designs[i]
-                plan = design_plan(d, solver=solver, ctx=ctx, graphs=False)
+                plan = design_plan(d, solver=solver, ctx=ctx, graphs=False, nfreq=nfreq)
                 try:
                     Zin, _ = plan.run(d.band(nfreq))
                     out[i] = (plan.Ne, Zin)
@@ -252,8 +275,6 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
                     plan.close()
         except Exception as e:  # noqa: BLE001 -- re-raised below
             errors.append(e)
-        finally:
-            nat.destroy_context(ctx)
 
     threads = [threading.Thread(target=work, args=(w,)) for w in range(max(1, workers))]
     for t in threads:
