@@ -431,9 +431,11 @@ def run_ours(args):
     # tensor-core tile widths: the command line's, else the autotuner's table
     tuned = importlib.import_module(PKG + ".autotune").tuned_opts(inp["Ne"])
     tiles = (args.tile_chain or (tuned[2] if tuned else 0), args.tile_bulk or (tuned[3] if tuned else 0))
+    resident = (args.resident_chain if args.resident_chain >= 0 else (tuned[4] if tuned else 0),
+                args.resident_bulk if args.resident_bulk >= 0 else (tuned[5] if tuned else 0))
     opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
                         batch=B if B < 8 else 0, lu_nb=args.lu_nb, tile_chain=tiles[0], tile_bulk=tiles[1],
-                        resident_chain=args.resident_chain, nfreq_hint=B)
+                        resident_chain=resident[0], resident_bulk=resident[1], nfreq_hint=B)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -491,12 +493,14 @@ def run_ours(args):
         if args.scheme == "ref":
             m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"],
                                         opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb, tile_chain=tiles[0],
-                                                          tile_bulk=tiles[1]))
+                                                          tile_bulk=tiles[1], resident_chain=resident[0],
+                                                          resident_bulk=resident[1]))
         else:
             # plan create (host mesh upload) + run + destroy through the C ABI
             p2 = m.SweepPlan(*pargs, *inp["tail"],
                              opts=m.sweep_opts(solver=args.solver, scheme="extract", lu_nb=args.lu_nb,
-                                               tile_chain=tiles[0], tile_bulk=tiles[1]),
+                                               tile_chain=tiles[0], tile_bulk=tiles[1], resident_chain=resident[0],
+                                               resident_bulk=resident[1], nfreq_hint=B),
                              rule_order=RULE[args.scheme])
             p2.run(fr)
             p2.close()
@@ -537,8 +541,9 @@ def run_ours(args):
                     else "c128", data="synthetic",
                     config=dict(workload=args.workload, Ne=inp["Ne"], Nt=inp["Nt"], batch=B,
                                 solver=args.solver, parallelism="replicas x%d" % world,
-                                tc_tiles="256x%d (panel chain) / 256x%d (outer panels)"
-                                         % (tiles[0] or 256, tiles[1] or 256),
+                                tc_tiles="256x%s (panel chain) / 256x%s (outer panels)"
+                                         % ("128 resident" if resident[0] else tiles[0] or 256,
+                                            "128 resident" if resident[1] else tiles[1] or 256),
                                 scheme=SCHEME_NAME[args.scheme],
                                 l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
                     e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
@@ -751,8 +756,11 @@ def main():
                     help="tensor-core tile width of the LU's K = 64 updates (0: the autotuner's table)")
     ap.add_argument("--tile-bulk", type=int, default=0, choices=[0, 128, 256],
                     help="tensor-core tile width of the outer panels' updates (0: the autotuner's table)")
-    ap.add_argument("--resident-chain", type=int, default=0, choices=[0, 1],
-                    help="1: the LU's K = 64 updates on resident, pipelined CTA pairs")
+    ap.add_argument("--resident-chain", type=int, default=-1, choices=[-1, 0, 1],
+                    help="1: the LU's K = 64 updates on resident, pipelined CTA pairs (-1: the autotuner's table)")
+    ap.add_argument("--resident-bulk", type=int, default=-1, choices=[-1, 0, 1],
+                    help="1: the LU's outer-panel updates on resident, pipelined CTA pairs (-1: the autotuner's "
+                         "table)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the plain FP64 GPU path on the same points")
     ap.add_argument("--no-secondary", action="store_true",

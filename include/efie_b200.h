@@ -178,6 +178,9 @@ typedef struct efie_sweep_opts {
                                 that overlap each 256 x 128 tile's TMEM drain with the
                                 next tile's MMAs (tile_chain is then unused); 0: one
                                 tile per CTA pair (default)                    */
+    int32_t resident_bulk;   /* 1: the outer panels' rectangular updates likewise (the
+                                strip of the next panel; the symmetric factorization's
+                                lower-triangle bulk stays on one tile per pair)  */
     int32_t nfreq_hint;      /* frequencies the plan's sweeps will solve (0 = unknown):
                                 with batch = 0, the automatic batch is cut to the
                                 balanced size for that many; efie_patch_sweep_fastquad
@@ -387,9 +390,10 @@ efie_status efie_debug_set_wait_test(int32_t enable, int64_t spins);
 
 /* Tensor-core tile widths (128 or 256 complex columns per CTA pair; anything
  * else: 256) of efie_lu_selftest's K = 64 chain updates and outer-panel
- * updates, and resident_chain (efie_sweep_opts), process-wide.  No
- * counterpart in the reference. */
-void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk, int resident_chain);
+ * updates, and which of them run on resident CTA pairs (bit 0: the chain's,
+ * bit 1: the outer panels'; efie_sweep_opts.resident_chain / resident_bulk),
+ * process-wide.  No counterpart in the reference. */
+void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk, int resident);
 
 /* 1 makes efie_plan_run take its batches in frequency order with every
  * refinement starting from zero, instead of coarse to fine with initial

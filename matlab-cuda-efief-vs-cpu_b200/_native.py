@@ -45,7 +45,8 @@ class EfieSweepOpts(C.Structure):
                 ("refine_tol", C.c_double), ("refine_max_iter", C.c_int32),
                 ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
                 ("refine_method", C.c_int32), ("graphs", C.c_int32), ("tile_chain", C.c_int32),
-                ("tile_bulk", C.c_int32), ("resident_chain", C.c_int32), ("nfreq_hint", C.c_int32)]
+                ("tile_bulk", C.c_int32), ("resident_chain", C.c_int32), ("resident_bulk", C.c_int32),
+                ("nfreq_hint", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")

@@ -291,7 +291,7 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
                timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True, tile_chain=0, tile_bulk=0,
-               resident_chain=0, nfreq_hint=0):
+               resident_chain=0, resident_bulk=0, nfreq_hint=0):
     """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
     scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only),
     tile_chain / tile_bulk: tensor-core tile widths 128 | 256 (0 = tuned)."""
@@ -310,6 +310,7 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.tile_chain = int(tile_chain)
     o.tile_bulk = int(tile_bulk)
     o.resident_chain = int(resident_chain)
+    o.resident_bulk = int(resident_bulk)
     o.nfreq_hint = int(nfreq_hint)
     return o
 
@@ -414,7 +415,8 @@ class SweepPlan:
         if opts is None:
             from .autotune import tuned_opts
             t = tuned_opts(Ne)
-            opts = sweep_opts(batch=t[0], lu_nb=t[1], tile_chain=t[2], tile_bulk=t[3]) if t else sweep_opts()
+            opts = (sweep_opts(batch=t[0], lu_nb=t[1], tile_chain=t[2], tile_bulk=t[3], resident_chain=t[4],
+                               resident_bulk=t[5]) if t else sweep_opts())
         self.opts = opts
         h = C.c_void_p()
         cx = ctx if ctx is not None else nat.context()

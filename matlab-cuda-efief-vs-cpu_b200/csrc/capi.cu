@@ -71,6 +71,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->tile_chain = 0;
     o->tile_bulk = 0;
     o->resident_chain = 0;
+    o->resident_bulk = 0;
     o->nfreq_hint = 0;
 }
 
@@ -580,6 +581,7 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         p->sw.tn_chain = choose_tile(p->opts.tile_chain);
         p->sw.tn_bulk = choose_tile(p->opts.tile_bulk);
         p->sw.resident_chain = p->opts.resident_chain == 1;
+        p->sw.resident_bulk = p->opts.resident_bulk == 1;
     }
     EFIE_CUDA(cudaStreamSynchronize(ctx->stream));
     return EFIE_OK;
@@ -958,14 +960,14 @@ extern "C" efie_status efie_patch_sweep_centroid(efie_ctx *ctx, const efie_mesh 
 // Self-test of the complex64 LU (no pivoting) used by the mixed solver.
 // ---------------------------------------------------------------------------
 static int g_selftest_nb = 256;
-static int g_selftest_tile[3] = {256, 256, 0};
+static int g_selftest_tile[3] = {256, 256, 0};   // chain tile, bulk tile, resident (1 chain, 2 bulk)
 extern "C" void efie_debug_set_selftest_panel(int lu_nb) {
     g_selftest_nb = (lu_nb == 64 || lu_nb == 128 || lu_nb == 256 || lu_nb == 512) ? lu_nb : 256;
 }
 extern "C" void efie_debug_set_selftest_tiles(int tile_chain, int tile_bulk, int resident_chain) {
     g_selftest_tile[0] = choose_tile(tile_chain);
     g_selftest_tile[1] = choose_tile(tile_bulk);
-    g_selftest_tile[2] = resident_chain == 1;
+    g_selftest_tile[2] = resident_chain & 3;
 }
 
 extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c128 *A, int32_t tensor_cores,
@@ -977,7 +979,8 @@ extern "C" efie_status efie_lu_selftest(efie_ctx *ctx, int32_t N, const efie_c12
     EFIE_TRY(efie_mixed_workspace(w, N, 1, g_selftest_nb));
     w.tn_chain = g_selftest_tile[0];
     w.tn_bulk = g_selftest_tile[1];
-    w.resident_chain = g_selftest_tile[2] != 0;
+    w.resident_chain = (g_selftest_tile[2] & 1) != 0;
+    w.resident_bulk = (g_selftest_tile[2] & 2) != 0;
     // a bit-exactly symmetric A takes the symmetric factorization, as a
     // sweep's Z from the symmetric gather does
     bool sym = true;

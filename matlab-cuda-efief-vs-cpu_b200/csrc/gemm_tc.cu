@@ -578,9 +578,32 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
                      int nchunk, const __half *__restrict__ Lpackb, size_t lstride, int lpitch, int loff,
                      const __half *__restrict__ Upackb, size_t ustride, int upitch, int uoff,
                      const float *__restrict__ lmaxb, const float *__restrict__ umaxb, size_t mstride, int nblk,
-                     int kcol, int krow, int K, int ld, char *__restrict__ ctl, const int *__restrict__ active) {
+                     int kcol, int krow, int K, int ld, char *__restrict__ ctl, const int *__restrict__ active,
+                     int tri_kb) {
     const int npr = (r1 - r0 + TM - 1) / TM, nct = (c1 - c0 + PBN - 1) / PBN;
-    const int per_f = npr * nct, ntiles = per_f * B;
+    // tiles per frequency: the full npr x nct grid, or (lower-triangle mode,
+    // tri_kb > 0) the tiles of row pair p with column tile < tri_cols(p)
+    int per_f = npr * nct;
+    if (tri_kb > 0) {
+        per_f = 0;
+        for (int p = 0; p < npr; p++) per_f += tri_cols(p, nct, tri_kb, PBN);
+    }
+    const int ntiles = per_f * B;
+    auto tile_of = [&](int rr, int &rp, int &ct) {
+        if (tri_kb <= 0) {
+            rp = rr / nct;
+            ct = rr - rp * nct;
+            return;
+        }
+        rp = 0;
+        while (rp < npr - 1) {
+            const int nc = tri_cols(rp, nct, tri_kb, PBN);
+            if (rr < nc) break;
+            rr -= nc;
+            rp++;
+        }
+        ct = rr;
+    };
     const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
     const uint32_t rank = cluster_rank();
     const bool leader = rank == 0;
@@ -622,7 +645,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         constexpr uint32_t sbytes = sizeof(__half) * SUB, ubytes = sizeof(__half) * PT::USUB;
         long long g = 0;
         for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
-            const int f = t / per_f, rr = t - f * per_f, rp = rr / nct, ct = rr - rp * nct;
+            const int f = t / per_f;
+            int rp, ct;
+            tile_of(t - f * per_f, rp, ct);
             if (!active[f]) continue;
             const __half *gl = Lpackb + lstride * f + (size_t)(loff + (rp * 2 + (int)rank) * TR) * KC;
             const __half *gu = Upackb + ustride * f + (size_t)(uoff + ct * PBN + (int)rank * PT::UH) * KC;
@@ -730,7 +755,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
         float *wcs = colsc + q * 2 * PBN;   // this warp's copy: no barrier across the epilogue warps
         int staged = 0, i = 0;
         for (int t = pair; t < ntiles && !*abort_sh; t += npairs) {
-            const int f = t / per_f, rr = t - f * per_f, rp = rr / nct, ct = rr - rp * nct;
+            const int f = t / per_f;
+            int rp, ct;
+            tile_of(t - f * per_f, rp, ct);
             if (!active[f]) continue;
             const int b = i & 1;
             const float *lm = lmaxb + mstride * f, *um = umaxb + mstride * f;
@@ -926,23 +953,40 @@ efie_status efie_gemm_update(efie_ctx *ctx, SolveWork &w, int r0, int r1, int c0
             EFIE_TRY(efie_update_simt(ctx, w, r0, r1, c0, c1, kcol + k0, krow + k0, std::min(64, K - k0), nact));
         return EFIE_OK;
     }
-    if (K <= 64 && tri_kb == 0 && w.resident_chain) {
-        // the panel chain's updates on resident CTA pairs, 256 x 128 tiles
+    // resident pairs: the chain's K = 64 updates, and of the outer panels'
+    // updates the rectangular ones (the strip of the next panel on the
+    // critical path; the lower-triangle bulk runs beside the chain on the
+    // one-tile kernel, whose short-lived pairs leave the chain its SMs)
+    if (K <= 64 ? w.resident_chain : (w.resident_bulk && tri_kb == 0)) {
+        // resident, pipelined CTA pairs over 256 x 128 tiles
         if (!Lv.base || !Uv.base || (Lv.off & 7) || (Uv.off & 7) ||
             Lv.off + (rows + TM - 1) / TM * TM > Lv.pitch || Uv.off + (cols + PBN - 1) / PBN * PBN > Uv.pitch)
             return efie_fail(EFIE_ERR_ARGS, "efie_gemm_update: packed operands do not cover the block");
         EFIE_TRY(efie_tc_attrs());
         cudaStream_t st = ctx->stream;
-        const long long ntiles = (long long)((rows + TM - 1) / TM) * ((cols + PBN - 1) / PBN) * w.B;
-        const int pairs = (int)std::min<long long>(std::max(1, ctx->num_sms / 2), ntiles);
+        const int npr = (rows + TM - 1) / TM, nct = (cols + PBN - 1) / PBN;
+        long long per_f = (long long)npr * nct;
+        double entries = (double)rows * cols;
+        if (tri_kb > 0) {
+            per_f = 0;
+            for (int p = 0; p < npr; p++) per_f += tri_cols(p, nct, tri_kb, PBN);
+            entries = 0;
+            for (int q0 = 0; q0 < rows; q0 += tri_kb)
+                entries += (double)std::min(tri_kb, rows - q0) * std::min(cols, q0 + tri_kb);
+        }
+        // the outer panels' updates run beside the panel chain (look-ahead
+        // streams): resident pairs would hold every SM for the whole update, so
+        // they leave 16 SMs to the chain's kernels
+        const int avail = K <= 64 ? ctx->num_sms / 2 : ctx->num_sms / 2 - 8;
+        const int pairs = (int)std::min<long long>(std::max(1, avail), per_f * w.B);
         size_t tok = ctx->log.begin(st);
         k_update_tc_pipe<<<2 * pairs, 256, PIPE_SMEM, st>>>(
             *reinterpret_cast<const CUtensorMap *>(w.planes_map), w.N, w.B, r0, r1, c0, c1, (K + KC - 1) / KC,
             static_cast<const __half *>(Lv.base), Lv.stride, Lv.pitch, Lv.off, static_cast<const __half *>(Uv.base),
             Uv.stride, Uv.pitch, Uv.off, w.lmax.as<float>(), w.umax.as<float>(), w.mstride, w.nblk, kcol, krow, K,
-            w.ld, w.ctl.as<char>(), w.active.as<int>());
+            w.ld, w.ctl.as<char>(), w.active.as<int>(), tri_kb);
         EFIE_CUDA(cudaGetLastError());
-        ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * (double)rows * cols * K * nact);
+        ctx->log.end(EFIE_K_GEMM, st, tok, 8.0 * entries * K * nact);
         return EFIE_OK;
     }
     // tile width of the pair: the panel chain's K = 64 updates and the outer

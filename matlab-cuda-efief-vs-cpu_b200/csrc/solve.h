@@ -35,6 +35,7 @@ struct SolveWork {
     int tn_chain = 256;       // tile width (complex columns per CTA pair) of the K = 64 updates
     int tn_bulk = 256;        // ... and of the outer panels' updates
     bool resident_chain = false;   // K = 64 updates on resident, pipelined CTA pairs (k_update_tc_pipe)
+    bool resident_bulk = false;    // the outer panels' updates likewise
     DevBuf planes;   // per f: float re[N][ld], im[N][ld]  (row-major)
     DevBuf dinv;     // per f: float2 [nblk][2][NB*NB] (L^-1, U^-1 of each diagonal block)
     DevBuf vec;      // float2 rf[B][vstride], y[B][vstride], d[B][vstride]

@@ -113,14 +113,15 @@ def test_lu_symmetric_random(n, lu_nb):
     assert np.abs(U - DLt).max() <= 1e-5 * np.abs(U).max()
 
 
-@pytest.mark.parametrize("tiles", [(128, 128, 0), (128, 256, 0), (256, 128, 0), (256, 256, 1)])
+@pytest.mark.parametrize("tiles", [(128, 128, 0), (128, 256, 0), (256, 128, 0), (256, 256, 1), (256, 256, 3)])
 @pytest.mark.parametrize("n,lu_nb,sym", [(700, 256, False), (1300, 512, True), (1300, 128, True)])
 def test_lu_tile_widths(tiles, n, lu_nb, sym):
     """The 256 x 128 tensor-core tile (a CTA pair per 128 complex columns)
     gives the same factors as the 256 x 256 tile to FP32 accuracy, for the
     panel chain's K = 64 updates and for the outer panels' updates, in the
     general and in the symmetric factorization; so do the resident, pipelined
-    CTA pairs of the chain updates (third entry 1)."""
+    CTA pairs (third entry: 1 the chain updates, 3 also the outer panels'
+    rectangular updates)."""
     nat = importlib.import_module("matlab-cuda-efief-vs-cpu_b200._native")
     rng = np.random.default_rng(n + lu_nb + tiles[0])
     A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
