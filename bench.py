@@ -617,8 +617,11 @@ def run_family(args):
         # the D designs of step i for this rank (ranks take disjoint designs)
         return [designs[((i * world + rank) * D + j) % len(designs)] for j in range(D)]
 
+    times = []
+
     def step(i):
-        out = sur.sweep_family(chunk(i), nf, workers=W, device=local, streams=[st.cuda_stream for st in streams])
+        out = sur.sweep_family(chunk(i), nf, workers=W, device=local, streams=[st.cuda_stream for st in streams],
+                               times=times)
         return [n for n, _ in out]
 
     for i in range(args.warmup):
@@ -626,6 +629,7 @@ def run_family(args):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    times.clear()
     Ns = []
     with ClockSampler(local) as clk:
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -661,6 +665,8 @@ def run_family(args):
                                 parallelism="replicas x%d, %d designs in flight per GPU" % (world, W)),
                     e2e=dict(value=pts / wall, unit="freq points/s", h2d_bytes_per_step=None,
                              d2h_bytes_per_step=D * nf * 32),
+                    plan_create_s_per_design=statistics.mean(t for t, _ in times) if times else None,
+                    sweep_s_per_design=statistics.mean(t for _, t in times) if times else None,
                     clocks=clk.summary())
         print(json.dumps(line), flush=True)
     if dist:

@@ -229,7 +229,7 @@ def _release_worker_contexts():
     _worker_ctx.clear()
 
 
-def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=None):
+def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=None, times=None):
     """Zin over each design's band (``d.band(nfreq)``) for a family of
     designs of uneven Ne, ``workers`` designs in flight at once.
 
@@ -246,7 +246,10 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
     a captured graph: a stream capture in one thread would be invalidated by
     the device-wide synchronisation that another thread's plan release
     performs.  Returns [(Ne, Zin)] in the order of ``designs``; a failure in
-    any worker is raised after all workers have stopped."""
+    any worker is raised after all workers have stopped.  ``times`` (a list,
+    optional) receives one (mesh + plan set-up seconds, sweep seconds) pair
+    per design, host wall clock in its worker thread."""
+    import time
     import queue
     import threading
     out = [None] * len(designs)
@@ -267,10 +270,14 @@ def sweep_family(designs, nfreq, workers=2, device=0, solver="mixed", streams=No
                 except queue.Empty:
                     return
                 d = designs[i]
+                t0 = time.perf_counter()
                 plan = design_plan(d, solver=solver, ctx=ctx, graphs=False, nfreq=nfreq)
+                t1 = time.perf_counter()
                 try:
                     Zin, _ = plan.run(d.band(nfreq))
                     out[i] = (plan.Ne, Zin)
+                    if times is not None:
+                        times.append((t1 - t0, time.perf_counter() - t1))
                 finally:
                     plan.close()
         except Exception as e:  # noqa: BLE001 -- re-raised below
