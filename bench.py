@@ -174,12 +174,13 @@ def _traffic():
         return {}
 
 
-# FP64 operations the assembly's pipes execute per point-pair evaluation
-# (QPE) of the single-frequency regular-pair kernel: DADD + DMUL + 2 DFMA
-# from the sass instruction counters of one captured launch
-# (profiles/k_regular_moments_cfg2.md), divided by its QPE.  The transcendental
-# functions (sqrt, sincos, the reciprocal) are FP64 instruction sequences, so
-# this is the work the FP64 pipe does per QPE, not a textbook flop count.
+# FP64 operations the assembly's pipes execute per point-pair evaluation and
+# frequency (QPE) of the regular-pair kernel: DADD + DMUL + 2 DFMA from the
+# sass instruction counters of one captured launch of the four-frequency
+# kernel (cfg2), divided by the launch's QPE.  The transcendental functions
+# (sqrt, sincos, the reciprocal) are FP64 instruction sequences, so this is
+# the work the FP64 pipe does per QPE, not a textbook flop count; it is kept
+# in profiles/traffic.json beside the DRAM bytes of the same capture.
 FP64_OPS_PER_QPE = None
 
 
@@ -228,7 +229,7 @@ def roofline(classes, name=None, fp64_peak=None):
         achieved = per_launch_work / (per_launch_ms * 1e-3) / 1e12
         peak = peaks["bf16_tflops_sustained"]
         out = dict(bound="tensor", unit="TFLOP/s", peak_source=src + " bf16 sustained")
-    elif name in ("quad", "nearself"):
+    elif name == "quad":
         # QPE/s times the FP64 operations per QPE, against measured DGEMM
         ops = _fp64_ops_per_qpe()
         qpe_rate = per_launch_work / (per_launch_ms * 1e-3)
@@ -553,8 +554,10 @@ def run_ours(args):
                     roofline=roofline(classes),
                     roofline_assembly=roofline(classes, "quad", fp64_peak),
                     phases_ms_per_point={k: v["ms"] / B for k, v in classes.items()},
-                    phases_note="one extra step with per-launch CUDA events (eager launches), outside the "
-                                "timed region; the timed steps replay the factorization as a CUDA graph")
+                    phases_note="one extra step with per-launch CUDA events (eager launches, the LU's "
+                                "look-ahead stream folded into the chain's so each pair of events brackets "
+                                "one kernel running alone), outside the timed region; the timed steps replay "
+                                "the factorization as a CUDA graph with the look-ahead")
         if world == 1 and not args.no_cpu_baseline:
             # the oracle's CPU path on the box's host cores: the first point of
             # the last step and the point furthest from the FP64 arm

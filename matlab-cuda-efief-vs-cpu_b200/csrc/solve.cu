@@ -933,6 +933,10 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     const bool sym = w.zsym && w.sym_lu && g_sym_lu_disabled != 1;
     const bool symtri = sym && g_sym_lu_disabled != 2;
     bool rest_pending = false;   // ev_rest holds the record of the previous D^rest
+    // with per-launch timing on, D^rest goes to the chain's stream too: the
+    // launches run one at a time, so each pair of events brackets its kernel
+    // alone instead of a kernel sharing the SMs with the other stream's
+    cudaStream_t lo = log.timing ? w.hi : w.lo;
     const PackView ipl = efie_inpanel_view(w, true), ipu = efie_inpanel_view(w, false);
     {
         OnStream on(ctx, w.hi);
@@ -987,11 +991,11 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
             }
             // D_P^rest on the low-priority stream, after F_P and the packs
             if (K1 < N) {
-                OnStream on_lo(ctx, w.lo);
-                EFIE_CUDA(cudaStreamWaitEvent(w.lo, w.ev_panel, 0));
+                OnStream on_lo(ctx, lo);
+                EFIE_CUDA(cudaStreamWaitEvent(lo, w.ev_panel, 0));
                 EFIE_TRY(efie_gemm_update(ctx, w, K1, N, K1, N, K0, K0, K, nact, Lp.at(K1 - Kend),
                                           Up.at(K1 - Kend), symtri ? KB : 0));
-                EFIE_CUDA(cudaEventRecord(w.ev_rest, w.lo));
+                EFIE_CUDA(cudaEventRecord(w.ev_rest, lo));
                 rest_pending = true;
             }
         }
