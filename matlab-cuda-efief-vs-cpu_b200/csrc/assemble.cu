@@ -163,23 +163,89 @@ __global__ void __launch_bounds__(256) k_regular_moments(
 
 // Several frequencies at once (F = 2..4, equally spaced: k_f = k0 + f dk).
 // Per point pair R, 1/(4 pi R) and the weights are shared, e^{-j k0 R} and
-// e^{-j dk R} take one sincos (and exp for lossy media) each, and every
+// e^{-j dk R} take one sincos each (and exp for lossy media), and every
 // further frequency costs one complex multiplication: e^{-j k_f R} =
 // e^{-j k0 R} (e^{-j dk R})^f.  The pair values go to each frequency's store.
+//
+// Cost per point pair, shared by the F frequencies: R and 1/R come from one
+// reciprocal square root of R^2 (R = R^2 rsqrt(R^2)) instead of a square
+// root and a division; the phase step dk R of a dense sweep is small, and for
+// |dk R| <= 1/2 its cosine and sine are the Maclaurin series through x^14 and
+// x^15 (truncation below 1e-18, Horner in x^2), larger steps take sincos.
+// With symmetric pairs the launch covers the tiles on or above the diagonal
+// only (a host-built list of (t1 block, t2 block)); the free-vertex vectors
+// of the tile's 40 triangles are staged in shared memory with the points, so
+// the nine edge combinations per frequency read them there.
 struct MomStores {
     MomStore s[4];
 };
 
+// cos x and sin x for |x| <= 1/2 from their Maclaurin series:
+// cos x = sum (-1)^n x^{2n} / (2n)!, sin x = x sum (-1)^n x^{2n} / (2n+1)!
+__device__ __forceinline__ void small_sincos(double x, double &sn, double &cs) {
+    const double u = x * x;
+    double c = 1.0 / 87178291200.0;                        // 1/14!
+    c = fma(c, -u, 1.0 / 479001600.0);                      // 1/12!
+    c = fma(c, -u, 1.0 / 3628800.0);                        // 1/10!
+    c = fma(c, -u, 1.0 / 40320.0);                          // 1/8!
+    c = fma(c, -u, 1.0 / 720.0);                            // 1/6!
+    c = fma(c, -u, 1.0 / 24.0);                             // 1/4!
+    c = fma(c, -u, 0.5);                                    // 1/2!
+    cs = fma(c, -u, 1.0);
+    double t = 1.0 / 1307674368000.0;                       // 1/15!
+    t = fma(t, -u, 1.0 / 6227020800.0);                     // 1/13!
+    t = fma(t, -u, 1.0 / 39916800.0);                       // 1/11!
+    t = fma(t, -u, 1.0 / 362880.0);                         // 1/9!
+    t = fma(t, -u, 1.0 / 5040.0);                           // 1/7!
+    t = fma(t, -u, 1.0 / 120.0);                            // 1/5!
+    t = fma(t, -u, 1.0 / 6.0);                              // 1/3!
+    sn = fma(x * u, -t, x);
+}
+
+// the nine edge combinations of one pair and frequency from its moments,
+// with the free-vertex vectors d1[3] (triangle t1) and d2[3] (t2) at hand
+__device__ __forceinline__ void store_combo(const MomStore &M, size_t slot, const double4 *d1s, const double4 *d2s,
+                                            const double *a) {
+    const double s0r = 4.0 * a[0], s0i = 4.0 * a[1];
+    const double bsr = M.ber * s0r - M.bei * s0i, bsi = M.ber * s0i + M.bei * s0r;   // beta 4 S0
+#pragma unroll
+    for (int l1 = 0; l1 < 3; l1++) {
+        const double4 d1 = d1s[l1];
+        const double ar = a[14] - (d1.x * a[8] + d1.y * a[10] + d1.z * a[12]);
+        const double ai = a[15] - (d1.x * a[9] + d1.y * a[11] + d1.z * a[13]);
+        const double bxr = a[2] - d1.x * a[0], bxi = a[3] - d1.x * a[1];
+        const double byr = a[4] - d1.y * a[0], byi = a[5] - d1.y * a[1];
+        const double bzr = a[6] - d1.z * a[0], bzi = a[7] - d1.z * a[1];
+#pragma unroll
+        for (int l2 = 0; l2 < 3; l2++) {
+            const double4 d2 = d2s[l2];
+            const double ivr = ar - (d2.x * bxr + d2.y * byr + d2.z * bzr);
+            const double ivi = ai - (d2.x * bxi + d2.y * byi + d2.z * bzi);
+            __stcs(M.p + (size_t)(3 * l1 + l2) * M.stride + slot,
+                   make_double2((M.alr * ivr - M.ali * ivi) + bsr, (M.alr * ivi + M.ali * ivr) + bsi));
+        }
+    }
+}
+
 template <int NQ, int F>
 __global__ void __launch_bounds__(256) k_regular_moments_mf(
-    int Nt, bool sym, const double4 *__restrict__ origin, const double4 *__restrict__ pts,
-    const uint8_t *__restrict__ skip, double kr0, double ki0, double dkr, double dki, MomStores ms) {
+    int Nt, bool sym, const int2 *__restrict__ tiles, const double4 *__restrict__ origin,
+    const double4 *__restrict__ pts, const uint8_t *__restrict__ skip, double kr0, double ki0, double dkr,
+    double dki, MomStores ms) {
     __shared__ double4 sp[8][NQ];
     __shared__ double4 so[8];
+    __shared__ double4 sd1[32][3], sd2[8][3];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int t1 = blockIdx.x * 32 + tx;
-    const int t2b = blockIdx.y * 8;
-    if (sym && blockIdx.x * 32 > t2b + 7) return;  // whole tile below the diagonal
+    int bx = blockIdx.x, by = blockIdx.y;
+    if (tiles) {
+        const int2 tl = tiles[blockIdx.x];
+        bx = tl.x;
+        by = tl.y;
+    }
+    const int t1 = bx * 32 + tx;
+    const int t2b = by * 8;
+    if (sym && bx * 32 > t2b + 7) return;  // whole tile below the diagonal
+    const double4 *tri_d = ms.s[0].tri_d;
     for (int i = threadIdx.x; i < 8 * NQ; i += blockDim.x) {
         int tt = t2b + i / NQ;
         sp[i / NQ][i % NQ] = tt < Nt ? pts[(size_t)tt * NQ + i % NQ] : make_double4(0, 0, 0, 0);
@@ -187,6 +253,15 @@ __global__ void __launch_bounds__(256) k_regular_moments_mf(
     if (threadIdx.x < 8) {
         int tt = t2b + threadIdx.x;
         so[threadIdx.x] = tt < Nt ? origin[tt] : make_double4(0, 0, 0, 0);
+    }
+    if (tri_d) {
+        for (int i = threadIdx.x; i < 40 * 3; i += blockDim.x) {
+            const int r = i / 3, l = i % 3;
+            const int tt = r < 32 ? bx * 32 + r : t2b + (r - 32);
+            const double4 v = tt < Nt ? tri_d[3 * (size_t)tt + l] : make_double4(0, 0, 0, 0);
+            if (r < 32) sd1[r][l] = v;
+            else sd2[r - 32][l] = v;
+        }
     }
     __syncthreads();
     const int t2 = t2b + ty;
@@ -203,19 +278,24 @@ __global__ void __launch_bounds__(256) k_regular_moments_mf(
     for (int f = 0; f < F; f++)
 #pragma unroll
         for (int i = 0; i < 16; i++) m[f][i] = 0.0;
+    constexpr double k4pi = 1.0 / (4.0 * kPi);
 #pragma unroll 1
     for (int q = 0; q < NQ; q++) {
         const double4 pq = sp[ty][q];
         const double ax = dox - pq.x, ay = doy - pq.y, az = doz - pq.z;
+        const double wq = pq.w * k4pi;
 #pragma unroll
         for (int p = 0; p < NQ; p++) {
             const double dx = ax + p1[p].x, dy = ay + p1[p].y, dz = az + p1[p].z;
-            double R = sqrt(dx * dx + dy * dy + dz * dz);
-            R = fmax(R, 1e-15);
-            double inv = p1[p].w * pq.w / (4.0 * kPi * R);
+            const double R2 = fmax(dx * dx + dy * dy + dz * dz, 1e-30);
+            const double rs = rsqrt(R2);
+            const double R = R2 * rs;
+            double inv = p1[p].w * wq * rs;
             double s0, c0, ss, cs;
             sincos(kr0 * R, &s0, &c0);
-            sincos(dkr * R, &ss, &cs);
+            const double x = dkr * R;
+            if (fabs(x) <= 0.5) small_sincos(x, ss, cs);
+            else sincos(x, &ss, &cs);
             if (ki0 != 0.0) inv *= exp(ki0 * R);
             double esr = cs, esi = -ss;   // e^{-j dk R}
             if (dki != 0.0) {
@@ -245,7 +325,10 @@ __global__ void __launch_bounds__(256) k_regular_moments_mf(
     }
     const size_t slot = pair_slot(t1, t2, Nt, sym);
 #pragma unroll
-    for (int f = 0; f < F; f++) store_mom(ms.s[f], slot, t1, t2, m[f]);
+    for (int f = 0; f < F; f++) {
+        if (tri_d) store_combo(ms.s[f], slot, sd1[tx], sd2[ty], m[f]);
+        else store_mom(ms.s[f], slot, t1, t2, m[f]);
+    }
 }
 
 // Generic point count (any Nq a prepack may carry).
@@ -958,6 +1041,15 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
         EFIE_CUDA(cudaGetLastError());
     }
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
+    if (g.symmetric) {
+        // the 32 x 8 tiles of the regular-pair launches with t1 block <= t2 block
+        std::vector<int2> tl;
+        const int ntx = (Nt + 31) / 32, nty = (Nt + 7) / 8;
+        for (int by = 0; by < nty; by++)
+            for (int bx = 0; bx < ntx && bx * 32 <= by * 8 + 7; bx++) tl.push_back(make_int2(bx, by));
+        g.n_reg_tiles = (int)tl.size();
+        EFIE_TRY(up(g.reg_tiles, tl.data(), sizeof(int2) * tl.size()));
+    }
     // component planes of npairs (9 edge combinations or the 8 moments) for up
     // to four frequencies assembled together, within a quarter of free memory
     const size_t per = sizeof(double2) * (g.combo ? 9 : 8) * g.npairs;
@@ -990,18 +1082,21 @@ double regular_pairs(const GeomDev &g) {
 
 template <int F>
 void launch_regular_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, const MomStores &ms) {
-    dim3 grid((g.Nt + 31) / 32, (g.Nt + 7) / 8);
+    // symmetric pairs: the tiles on or above the diagonal from the list
+    const bool lst = g.symmetric && g.n_reg_tiles > 0;
+    dim3 grid = lst ? dim3((unsigned)g.n_reg_tiles) : dim3((g.Nt + 31) / 32, (g.Nt + 7) / 8);
+    const int2 *tiles = lst ? g.reg_tiles.as<int2>() : nullptr;
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
     const double dkr = (ph[F - 1].kr - ph[0].kr) / (F - 1), dki = (ph[F - 1].ki - ph[0].ki) / (F - 1);
     switch (g.Nq) {
     case 3:
-        k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
-                                                        dki, ms);
+        k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
+                                                        dkr, dki, ms);
         break;
     case 7:
-        k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, org, pts, skip, ph[0].kr, ph[0].ki, dkr,
-                                                        dki, ms);
+        k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
+                                                        dkr, dki, ms);
         break;
     }
 }

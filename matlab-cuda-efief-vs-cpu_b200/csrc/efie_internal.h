@@ -176,6 +176,8 @@ struct GeomDev {
     DevBuf tri_d;             // double4[3*Nt] free-vertex vectors per triangle slot
     DevBuf edge_tl;           // int32[2*Ne] 4 t + slot per RWG side (-1 = none)
     DevBuf edge_c;            // double[2*Ne] RWG coefficient c per side
+    DevBuf reg_tiles;         // int2[n_reg_tiles] (t1 block, t2 block) of the symmetric regular-pair launches
+    int n_reg_tiles = 0;
 };
 
 // Per-frequency physics: k = w sqrt(mu eps) (principal branch), alpha = j w mu,
