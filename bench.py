@@ -553,6 +553,8 @@ def run_ours(args):
                     accuracy=accuracy, fp64_gpu=fp64,
                     roofline=roofline(classes),
                     roofline_assembly=roofline(classes, "quad", fp64_peak),
+                    # the HBM-bound classes: algorithmic bytes over their event time
+                    roofline_hbm={k: roofline(classes, k) for k in ("trsv", "residual", "gather")},
                     phases_ms_per_point={k: v["ms"] / B for k, v in classes.items()},
                     phases_note="one extra step with per-launch CUDA events (eager launches, the LU's "
                                 "look-ahead stream folded into the chain's so each pair of events brackets "

@@ -1220,7 +1220,9 @@ efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, i
         else k_gather_z<false><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
     }
     EFIE_CUDA(cudaGetLastError());
-    log.end(EFIE_K_GATHER, s, tok, (pr ? 24.0 : 16.0) * (double)Ne * Ne);
+    // algorithmic bytes: one read of every pair value, Z (and the planes) written once
+    log.end(EFIE_K_GATHER, s, tok,
+            16.0 * (g.combo ? 9.0 : 8.0) * (double)g.npairs + (pr ? 24.0 : 16.0) * (double)Ne * Ne);
     return EFIE_OK;
 }
 

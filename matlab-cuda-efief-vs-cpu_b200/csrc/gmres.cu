@@ -552,6 +552,9 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
     std::vector<char> hctl(64 * (size_t)B);
     std::vector<int> hstop(B);
     int matvecs = 0;
+    // frequencies still iterating as of the last stop-flag poll: the work the
+    // in-cycle launches count (a stopped frequency's CTAs return at once)
+    int nrun = nact;
     bool all_conv = false, failed = false;
     const dim3 vg(cdiv(N, 256), B), og(nch, B), mg(cdiv(N, 32), B);
     while (!all_conv && !failed && matvecs < max_iter) {
@@ -567,15 +570,15 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
             tok = log.begin(s);
             EFIE_TRY(efie_trsv(ctx, w, true, rf, yv, nullptr, epoch));
             EFIE_TRY(efie_trsv(ctx, w, false, yv, dv, zj, epoch));
-            log.end(EFIE_K_TRSV, s, tok, lubytes * nact, 2);
+            log.end(EFIE_K_TRSV, s, tok, lubytes * nrun, 2);
             tok = log.begin(s);
             if (w.zsym) {
                 EFIE_TRY(symv(ctx, w, Z, zstride, zj, wv, &st[0].stop, (int)(sizeof(GmState) / sizeof(int))));
-                log.end(EFIE_K_RESIDUAL, s, tok, 0.5 * zbytes * nact, 2);
+                log.end(EFIE_K_RESIDUAL, s, tok, 0.5 * zbytes * nrun, 2);
             } else {
                 k_gm_matvec<<<mg, 256, 0, s>>>(N, static_cast<const double2 *>(Z), zstride, zj, wv, st);
                 EFIE_CUDA(cudaGetLastError());
-                log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nact);
+                log.end(EFIE_K_RESIDUAL, s, tok, zbytes * nrun);
             }
             tok = log.begin(s);
             k_gm_zero_col<<<B, GM_M + 1, 0, s>>>(B, j, st);
@@ -586,7 +589,7 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
             k_gm_arnoldi<<<cdiv(B, 32), 32, 0, s>>>(B, j, nch, npart, st, ctl);
             k_gm_normalize<<<vg, 256, 0, s>>>(N, B, j, V, wv, rf, w.vstride, st);
             EFIE_CUDA(cudaGetLastError());
-            log.end(EFIE_K_OTHER, s, tok, 32.0 * (double)N * (j + 1) * 2 * nact, 7);
+            log.end(EFIE_K_OTHER, s, tok, 32.0 * (double)N * (j + 1) * 2 * nrun, 7);
             matvecs++;
             if (j >= 2) {
                 // a poll costs one synchronisation (tens of us) against a step
@@ -598,8 +601,9 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
                 log.end(EFIE_K_OTHER, s, tok, 0.0);
                 EFIE_CUDA(cudaMemcpyAsync(hstop.data(), w.gflags.p, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
                 EFIE_CUDA(cudaStreamSynchronize(s));
+                nrun = 0;
                 for (int f = 0; f < B; f++)
-                    if (active_host[f] && !hstop[f]) all_stop = false;
+                    if (active_host[f] && !hstop[f]) all_stop = false, nrun++;
                 if (all_stop) {
                     j++;
                     break;
@@ -617,11 +621,12 @@ efie_status efie_mixed_gmres(efie_ctx *ctx, SolveWork &w, const void *Z, size_t 
         EFIE_CUDA(cudaMemcpyAsync(hctl.data(), ctl, 64 * (size_t)B, cudaMemcpyDeviceToHost, s));
         EFIE_CUDA(cudaStreamSynchronize(s));
         all_conv = true;
+        nrun = 0;
         for (int f = 0; f < B; f++) {
             if (!active_host[f]) continue;
             const char *c = hctl.data() + 64 * f;
             if (*reinterpret_cast<const int *>(c + 36)) failed = true;
-            if (!*reinterpret_cast<const int *>(c + 28)) all_conv = false;
+            if (!*reinterpret_cast<const int *>(c + 28)) all_conv = false, nrun++;
         }
     }
     res->iters = matvecs;
