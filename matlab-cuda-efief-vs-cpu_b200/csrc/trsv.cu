@@ -11,10 +11,12 @@
 // line: the CTA that finishes a block raises every replica with atomicMax,
 // and a waiting CTA polls only its own replica, so no line is polled by more
 // than one CTA.  Waits are bounded and abort on the frequency's error flag.
-// Everything that does not depend on a counter is loaded before the wait:
-// the inverse of the diagonal block (to shared memory) and the next L/U tile
-// (to registers).
+// Nothing a CTA reads from the factors depends on a counter, so its tiles and
+// diagonal inverses stream through a TMA ring ahead of the solve (k_trsv).
 #include <algorithm>
+#include <cstdint>
+
+#include <cuda.h>
 
 #include "efie_internal.h"
 #include "solve.h"
@@ -22,7 +24,6 @@
 namespace {
 
 constexpr int NB = 64;
-constexpr int DS = NB + 1;    // padded row stride of the diagonal inverse in shared memory
 constexpr int LINE = 8;       // u64 per 64-byte progress line
 
 // Limits of the bounded waits, per device.  d_wait_spins: polls before a
@@ -53,21 +54,63 @@ __device__ __forceinline__ unsigned long long wait_progress(const volatile unsig
     return v;
 }
 
-// 16 consecutive complex entries of one row of the planes (zeros past `rows`).
-__device__ __forceinline__ void load_tile_row(float4 (&t)[8], const float *Ar, const float *Ai, size_t off,
-                                              bool valid) {
-    if (valid) {
-        const float4 *pr = reinterpret_cast<const float4 *>(Ar + off);
-        const float4 *pi = reinterpret_cast<const float4 *>(Ai + off);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            t[i] = __ldg(pr + i);
-            t[4 + i] = __ldg(pi + i);
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < 8; i++) t[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+// ---------------------------------------------------------------------------
+// TMA / mbarrier primitives (inline PTX)
+// ---------------------------------------------------------------------------
+constexpr int TS = 3;                                          // stages of the tile ring
+constexpr uint32_t STAGE_BYTES = 2u * NB * NB * sizeof(float);  // a 64 x 64 complex tile: 32 KB
+constexpr uint32_t BOX_BYTES = 32u * 32u * sizeof(float);       // one 32 x 32 box of one plane
+constexpr size_t TRSV_SMEM = TS * STAGE_BYTES + 1024 + 64;      // ring (1024-aligned) + barriers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for a stage: false after about a second of polling.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (long long i = 0; i < (1ll << 22); i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
     }
+    return false;
+}
+
+// one 32 x 32 box of the planes tensor [B][2][N][N] (column x, row y, plane, slot)
+__device__ __forceinline__ void tma_box(const CUtensorMap *map, void *dst, int x, int y, int plane, int f,
+                                        uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(plane), "r"(f), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ float2 dot16(const float4 (&t)[8], const float2 *y) {
@@ -83,61 +126,128 @@ __device__ __forceinline__ float2 dot16(const float4 (&t)[8], const float2 *y) {
     return s;
 }
 
+// Columns quarter*16 .. +15 of row `row` of a staged tile: the tile is eight
+// 32 x 32 boxes [plane][row half][column half] of 128-byte rows whose 16-byte
+// chunk q sits at chunk q ^ (row mod 8) (the TMA 128B swizzle); a warp reads
+// 32 consecutive rows, so each quarter-warp touches eight distinct chunks.
+__device__ __forceinline__ void stage_row(float4 (&t)[8], const unsigned char *stage, int row, int quarter) {
+    const int rh = row >> 5, lr = row & 31, ch = quarter >> 1, q0 = (quarter & 1) * 4;
+#pragma unroll
+    for (int pl = 0; pl < 2; pl++) {
+        const unsigned char *box = stage + ((pl * 2 + rh) * 2 + ch) * BOX_BYTES + lr * 128;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            t[pl * 4 + c] = *reinterpret_cast<const float4 *>(box + (((q0 + c) ^ (lr & 7)) << 4));
+    }
+}
+
+// Block-row solves of the items of one CTA.  Every 32 KB piece an item reads
+// -- the 64 x 64 tiles of its block row (8 TMA boxes each) and then its
+// diagonal inverse (one bulk copy) -- flows through a ring of TS stages fed
+// by thread 0 in the CTA's item order, so the loads of later tiles, and of
+// the next items, are in flight while the CTA waits for a solved block or
+// works on the current one.  The right-hand side blocks y_jb are read from
+// global memory after their publication (one block ahead when already
+// published).
 template <bool LOWER>
-__global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const float *__restrict__ planes, size_t pstride,
-                                              int ld, const float2 *__restrict__ dinv, size_t dstride,
-                                              const float2 *__restrict__ rhsb, float2 *outb, int vstride,
-                                              double2 *__restrict__ xb, unsigned long long *prog, int epoch,
-                                              char *ctl, const int *__restrict__ active) {
-    __shared__ float2 Ds[NB * DS];
+__global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtensorMap map, int N, int nblk, int B,
+                                                 const float2 *__restrict__ dinv, size_t dstride,
+                                                 const float2 *__restrict__ rhsb, float2 *outb, int vstride,
+                                                 double2 *__restrict__ xb, unsigned long long *prog, int epoch,
+                                                 char *ctl, const int *__restrict__ active) {
+    extern __shared__ unsigned char dsm[];
     __shared__ float2 acc[NB];
-    __shared__ int avail_sh;
     __shared__ float2 part[4][NB];
-    __shared__ int ok;
+    __shared__ int avail_sh, ok, fail;
+    unsigned char *ring = dsm + (((smem_u32(dsm) + 1023u) & ~1023u) - smem_u32(dsm));
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + TS * STAGE_BYTES);
     const int tid = threadIdx.x;
     const int row = tid & 63, quarter = tid >> 6;
     const int G = gridDim.x;
     const unsigned long long tag = (unsigned long long)(unsigned)epoch << 32;
     const int dir = LOWER ? 0 : 1;
     const int items = nblk * B;
+    auto live = [&](int it) -> bool {
+        const int f = it % B;
+        return active[f] && !*reinterpret_cast<const volatile int *>(ctl + 64 * f + 32);
+    };
+    // producer state (thread 0): the next piece is piece p_q of item p_it
+    // (p_q < o: tile of block column q; p_q == o: the diagonal inverse)
+    int p_it = blockIdx.x, p_q = 0, issued = 0;
+    auto produce = [&]() {
+        if (p_it >= items) return;
+        const int o = p_it / B, f = p_it - o * B, b = LOWER ? o : nblk - 1 - o;
+        unsigned char *st = ring + (issued % TS) * STAGE_BYTES;
+        uint64_t *bar = full + issued % TS;
+        mbar_expect_tx(bar, STAGE_BYTES);
+        if (p_q < o) {
+            const int jb = LOWER ? p_q : nblk - 1 - p_q;
+#pragma unroll
+            for (int pl = 0; pl < 2; pl++)
+#pragma unroll
+                for (int rh = 0; rh < 2; rh++)
+#pragma unroll
+                    for (int ch = 0; ch < 2; ch++)
+                        tma_box(&map, st + ((pl * 2 + rh) * 2 + ch) * BOX_BYTES, jb * NB + ch * 32, b * NB + rh * 32,
+                                pl, f, bar);
+        } else {
+            bulk_g2s(st, dinv + dstride * f + (size_t)b * 2 * NB * NB + (LOWER ? 0 : NB * NB), STAGE_BYTES, bar);
+        }
+        issued++;
+        if (++p_q > o) {
+            p_q = 0;
+            for (p_it += G; p_it < items && !live(p_it); p_it += G) {
+            }
+        }
+    };
+    if (tid == 0) {
+        for (int s = 0; s < TS; s++) mbar_init(full + s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fail = 0;
+        while (p_it < items && !live(p_it)) p_it += G;
+        for (int s = 0; s < TS; s++) produce();
+    }
+    __syncthreads();
+    int cc = 0;   // pieces consumed
+    // wait for the next piece (every thread), then a CTA-wide verdict
+    auto take = [&]() -> const unsigned char * {
+        if (!mbar_wait_bounded(full + cc % TS, (uint32_t)(cc / TS) & 1u)) fail = 1;
+        return ring + (cc % TS) * STAGE_BYTES;
+    };
+    // thread 0 drains the pieces in flight before the CTA returns early
+    auto drain = [&]() {
+        if (tid != 0) return;
+        for (int k = cc; k < issued; k++)
+            if (!mbar_wait_bounded(full + k % TS, (uint32_t)(k / TS) & 1u)) return;
+    };
     for (int it = blockIdx.x; it < items; it += G) {
         const int o = it / B, f = it - o * B;
-        if (!active[f]) continue;
+        if (!live(it)) continue;
         const char *c = ctl + 64 * f;
-        if (*reinterpret_cast<const volatile int *>(c + 32)) continue;  // converged: skip the whole frequency
         const volatile int *err = reinterpret_cast<const volatile int *>(c + 36);
         const int b = LOWER ? o : nblk - 1 - o;
-        const float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
         const float2 *rhs = rhsb + (size_t)vstride * f;
         float2 *out = outb + (size_t)vstride * f;
         unsigned long long *myctr = prog + ((size_t)(dir * B + f) * G + blockIdx.x) * LINE;
         const int r0 = b * NB;
         const int rows = min(NB, N - r0);
-        const bool rvalid = row < rows;
-        // independent of every counter: the diagonal inverse and the right-hand side
-        const float2 *D = dinv + dstride * f + (size_t)b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
-        for (int e = tid; e < NB * NB; e += 256) Ds[(e >> 6) * DS + (e & 63)] = __ldg(D + e);
         if (tid < NB) acc[tid] = (tid < rows) ? rhs[r0 + tid] : make_float2(0.f, 0.f);
-        if (tid == 0) ok = 1;
-        // dependencies in solve order: L needs blocks 0..b-1, U needs blocks nblk-1..b+1
-        const int ndep = o;
-        const size_t rowoff = (size_t)(r0 + (rvalid ? row : 0)) * ld + quarter * 16;
-        float4 cur[8];
-        if (ndep > 0) {
-            const int jb0 = LOWER ? 0 : nblk - 1;
-            load_tile_row(cur, Ar, Ai, rowoff + (size_t)jb0 * NB, rvalid);
-        }
-        if (tid == 0) avail_sh = 0;
+        if (tid == 0) ok = 1, avail_sh = 0;
         __syncthreads();
         // each thread keeps its quarter-row dot product in registers across the
-        // dependencies; the CTA synchronises only when it has to wait for a block
-        // that is not published yet (one observed count can cover many blocks)
+        // dependencies; the CTA synchronises to wait for a block only when the
+        // last observed count does not cover it (one count can cover many)
         float2 sdot = make_float2(0.f, 0.f);
         int avail = 0;
-        for (int q = 0; q < ndep; q++) {
+        float2 ynext[16];
+        bool have_next = false;
+        auto load_y = [&](float2 (&y)[16], int jb) {
+            const float2 *ysrc = out + jb * NB + quarter * 16;
+#pragma unroll
+            for (int k = 0; k < 16; k++) y[k] = (jb * NB + quarter * 16 + k < N) ? ysrc[k] : make_float2(0.f, 0.f);
+        };
+        for (int q = 0; q < o; q++) {
             const int jb = LOWER ? q : nblk - 1 - q;
-            float4 nxt[8];
-            if (q + 1 < ndep) load_tile_row(nxt, Ar, Ai, rowoff + (size_t)(LOWER ? jb + 1 : jb - 1) * NB, rvalid);
             if (q >= avail) {
                 if (tid == 0) {
                     const unsigned long long v = wait_progress(myctr, tag | (unsigned long long)(q + 1), err);
@@ -145,25 +255,39 @@ __global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const floa
                     avail_sh = (int)(v & 0xffffffffull);
                 }
                 __syncthreads();
-                if (!ok) return;
+                if (!ok) {
+                    drain();
+                    return;
+                }
                 avail = avail_sh;
             }
             // block jb of the solution: written by another CTA and published
-            // before `avail` was read, then never changed in this launch, so the
-            // (L1-cached) loads cannot see a stale line; a 64-entry block covers
-            // whole 128-byte lines
+            // before `avail` was read, then never changed in this launch
             float2 y16[16];
-            const float2 *ysrc = out + jb * NB + quarter * 16;
+            if (have_next) {
 #pragma unroll
-            for (int c = 0; c < 16; c++)
-                y16[c] = (jb * NB + quarter * 16 + c < N) ? ysrc[c] : make_float2(0.f, 0.f);
-            const float2 t = dot16(cur, y16);
-            sdot.x += t.x;
-            sdot.y += t.y;
-            if (q + 1 < ndep) {
-#pragma unroll
-                for (int i = 0; i < 8; i++) cur[i] = nxt[i];
+                for (int k = 0; k < 16; k++) y16[k] = ynext[k];
+            } else {
+                load_y(y16, jb);
             }
+            have_next = q + 1 < o && q + 1 < avail;
+            if (have_next) load_y(ynext, LOWER ? jb + 1 : jb - 1);
+            const unsigned char *st = take();
+            if (!fail) {
+                float4 t[8];
+                stage_row(t, st, row, quarter);
+                const float2 d = dot16(t, y16);
+                sdot.x += d.x;
+                sdot.y += d.y;
+            }
+            __syncthreads();
+            if (fail) {
+                if (tid == 0) atomicExch((int *)err, 2);
+                drain();
+                return;
+            }
+            if (tid == 0) produce();
+            cc++;
         }
         part[quarter][row] = sdot;
         __syncthreads();
@@ -174,19 +298,34 @@ __global__ void __launch_bounds__(256) k_trsv(int N, int nblk, int B, const floa
             acc[tid] = t;
         }
         __syncthreads();
-        // y_b = inv(diagonal block) * acc
+        // y_b = inv(diagonal block) * acc; the inverse is row-major float2
+        // [64][64] in the stage, read from column (k + row) mod 16 of the
+        // thread's 16 so that a warp's 32 rows spread over the banks
         {
-            const float2 *drow = Ds + row * DS + quarter * 16;
-            float2 s = make_float2(0.f, 0.f);
+            const float2 *dst = reinterpret_cast<const float2 *>(take());
+            float2 sv = make_float2(0.f, 0.f);
+            if (!fail) {
+                const float2 *drow = dst + row * NB + quarter * 16;
+                const float2 *av = acc + quarter * 16;
+                const int rot = row & 15;
 #pragma unroll
-            for (int cc = 0; cc < 16; cc++) {
-                const float2 m = drow[cc], v = acc[quarter * 16 + cc];
-                s.x += m.x * v.x - m.y * v.y;
-                s.y += m.x * v.y + m.y * v.x;
+                for (int k = 0; k < 16; k++) {
+                    const int cix = (k + rot) & 15;
+                    const float2 m = drow[cix], v = av[cix];
+                    sv.x += m.x * v.x - m.y * v.y;
+                    sv.y += m.x * v.y + m.y * v.x;
+                }
             }
-            part[quarter][row] = s;
+            part[quarter][row] = sv;
         }
         __syncthreads();
+        if (fail) {
+            if (tid == 0) atomicExch((int *)err, 2);
+            drain();
+            return;
+        }
+        if (tid == 0) produce();
+        cc++;
         if (tid < rows) {
             float2 t;
             t.x = part[0][tid].x + part[1][tid].x + part[2][tid].x + part[3][tid].x;
@@ -227,9 +366,11 @@ efie_status efie_trsv_workspace(SolveWork &w) {
     int dev = 0, sms = 0, occ = 0;
     EFIE_CUDA(cudaGetDevice(&dev));
     EFIE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    EFIE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv<true>, 256, 0));
+    EFIE_CUDA(cudaFuncSetAttribute(k_trsv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRSV_SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_trsv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRSV_SMEM));
+    EFIE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trsv<true>, 256, TRSV_SMEM));
     int occ2 = 0;
-    EFIE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_trsv<false>, 256, 0));
+    EFIE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_trsv<false>, 256, TRSV_SMEM));
     occ = std::max(1, std::min(std::min(occ, occ2), 2));
     w.grid = std::max(1, std::min(w.nblk * w.B, occ * sms));
     const size_t bytes = sizeof(unsigned long long) * LINE * 2 * (size_t)w.B * w.grid;
@@ -240,19 +381,19 @@ efie_status efie_trsv_workspace(SolveWork &w) {
     return EFIE_OK;
 }
 
+// The factors are read through the planes' tensor map (SolveWork::planes_map,
+// encoded with the workspace): 32 x 32 boxes, zeros past row and column N.
 efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs, float2 *out, void *x, int epoch) {
     int grid = w.grid;
-    const float *planes = w.planes.as<float>();
     const float2 *dinv = w.dinv.as<float2>();
     double2 *xd = static_cast<double2 *>(x);
     unsigned long long *prog = w.prog.as<unsigned long long>();
     char *ctl = w.ctl.as<char>();
     const int *active = w.active.as<int>();
-    void *args[] = {(void *)&w.N,  (void *)&w.nblk, (void *)&w.B,    (void *)&planes, (void *)&w.pstride,
-                    (void *)&w.ld, (void *)&dinv,   (void *)&w.dstride, (void *)&rhs, (void *)&out,
-                    (void *)&w.vstride, (void *)&xd, (void *)&prog, (void *)&epoch, (void *)&ctl,
-                    (void *)&active};
+    void *args[] = {(void *)w.planes_map, (void *)&w.N,   (void *)&w.nblk,    (void *)&w.B,  (void *)&dinv,
+                    (void *)&w.dstride,   (void *)&rhs,   (void *)&out,       (void *)&w.vstride,
+                    (void *)&xd,          (void *)&prog,  (void *)&epoch,     (void *)&ctl,  (void *)&active};
     const void *fn = lower ? (const void *)k_trsv<true> : (const void *)k_trsv<false>;
-    EFIE_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, 0, ctx->stream));
+    EFIE_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, TRSV_SMEM, ctx->stream));
     return EFIE_OK;
 }
