@@ -46,6 +46,7 @@
 #include <cudaTypedefs.h>
 
 #include "solve.h"
+#include "tma.h"
 
 namespace {
 
@@ -846,10 +847,8 @@ efie_status efie_tc_attrs() {
 
 extern "C" void efie_debug_disable_tensor_cores(int disable) { g_tc_disabled = disable != 0; }
 
-namespace {
-// the planes of every frequency slot as one float tensor [B][2][N][ld]
-// (innermost first: column, row, plane, slot), 32 x 32 boxes, 128B swizzle
-efie_status encode_planes_map(SolveWork &w) {
+efie_status efie_encode_tiled(void *map, CUtensorMapDataType type, int rank, void *base, const cuuint64_t *dims,
+                              const cuuint64_t *strides, const cuuint32_t *box, CUtensorMapSwizzle swizzle) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -859,16 +858,24 @@ efie_status encode_planes_map(SolveWork &w) {
             return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = encode(reinterpret_cast<CUtensorMap *>(map), type, (cuuint32_t)rank, base, dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return EFIE_OK;
+}
+
+namespace {
+// the planes of every frequency slot as one float tensor [B][2][N][ld]
+// (innermost first: column, row, plane, slot), 32 x 32 boxes, 128B swizzle
+efie_status encode_planes_map(SolveWork &w) {
     const cuuint64_t dims[4] = {(cuuint64_t)w.N, (cuuint64_t)w.N, 2, (cuuint64_t)w.B};
     const cuuint64_t strides[3] = {sizeof(float) * (cuuint64_t)w.ld, sizeof(float) * (cuuint64_t)w.ld * w.N,
                                    sizeof(float) * (cuuint64_t)w.pstride};
-    const cuuint32_t box[4] = {32, 32, 1, 1}, estr[4] = {1, 1, 1, 1};
-    const CUresult r = encode(reinterpret_cast<CUtensorMap *>(w.planes_map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                              w.planes.p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return efie_fail(EFIE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the LU planes");
-    return EFIE_OK;
+    const cuuint32_t box[4] = {32, 32, 1, 1};
+    return efie_encode_tiled(w.planes_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, w.planes.p, dims, strides, box,
+                             CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 // halves per frequency slot of a packed panel with `nchunk` K chunks

@@ -31,6 +31,7 @@
 
 #include "efie_internal.h"
 #include "solve.h"
+#include "tma.h"
 
 namespace {
 
@@ -345,13 +346,16 @@ __global__ void k_gm_reset_skip(int B, char *__restrict__ ctl, const int *__rest
 // (t = J (J + 1) / 2 + I): rows I, columns J.  It contributes Z_IJ x_J to y_I
 // and, off the diagonal, Z_IJ^T x_I to y_J; both partial vectors go to
 // P[f][t][2][ST] and k_symv_reduce adds them in a fixed order, so the
-// product is bit-reproducible.  Warp w takes the tile's columns 16 w .. 16 w
-// + 15 in four groups of four (lane l its rows l + 32 q): the sixteen 16-byte
-// loads of a group are issued before any of them is used, and the four
-// column sums of a group are reduced across the warp together (each halving
-// step exchanges half of the values still held, 6 complex shuffles per group
-// instead of 20).  Z is streamed past the caches (each entry is read once per
-// product); the vectors stay cached.  A frequency whose flag
+// product is bit-reproducible.
+//
+// k_symv_ring: one persistent CTA per SM walks its (tile, frequency) items;
+// every tile arrives as four chunks of 32 columns x 128 rows (64 KB, one TMA
+// box of the map of Z; zeros past row and column N) through a ring of three
+// stages that thread 0 refills in the CTA's item order, so the next chunks
+// -- also those of the next items -- are in flight while the CTA works.  Warp
+// w takes columns 4 w .. 4 w + 3 of each chunk (lane l its rows l + 32 q)
+// and reduces their four column sums across the warp together (each halving
+// step exchanges half of the values still held).  A frequency whose flag
 // (flags[f * fstride]) is set is skipped.
 // ---------------------------------------------------------------------------
 constexpr int ST = 128;
@@ -373,85 +377,135 @@ __device__ __forceinline__ void cadd(double2 &a, const double2 &b) {
     a.y += b.y;
 }
 
-__global__ void __launch_bounds__(256) k_symv_tiles(int N, const double2 *__restrict__ Zb, size_t zstride,
-                                                    const double2 *__restrict__ xb, double2 *__restrict__ P,
-                                                    const int *__restrict__ flags, int fstride) {
-    const int f = blockIdx.y;
-    if (flags[(size_t)f * fstride]) return;
-    int I, J;
-    tile_of(blockIdx.x, I, J);
-    const double2 *Z = Zb + zstride * f;
-    const double2 *x = xb + (size_t)N * f;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r0 = I * ST, c0 = J * ST;
-    const bool offdiag = I != J;
+constexpr int SC = 32;                                  // columns per chunk
+constexpr int SRING = 3;                                // stages of the chunk ring
+constexpr uint32_t SCHUNK = ST * SC * sizeof(double2);  // 64 KB
+constexpr size_t SYMV_SMEM = SRING * SCHUNK + 1024 + 64;
+
+__global__ void __launch_bounds__(256, 1) k_symv_ring(const __grid_constant__ CUtensorMap zmap, int N, int ntiles,
+                                                      int B, const double2 *__restrict__ xb, double2 *__restrict__ P,
+                                                      const int *__restrict__ flags, int fstride, char *ctl) {
+    using namespace efie_tma;
+    extern __shared__ unsigned char dsm[];
     __shared__ double2 rsum[8][ST];
     __shared__ double2 csum[ST];
-    double2 xr[4], rs[4];
-    bool rv[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int m = r0 + lane + 32 * q;
-        rv[q] = m < N;
-        xr[q] = rv[q] ? x[m] : make_double2(0.0, 0.0);
-        rs[q] = make_double2(0.0, 0.0);
-    }
-#pragma unroll 1
-    for (int g = 0; g < 4; g++) {
-        const int cb = warp * 16 + g * 4;   // first column of the group within the tile
-        double2 a[4][4], xn[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int n = c0 + cb + j;
-            const bool cvalid = n < N;
-            xn[j] = cvalid ? x[n] : make_double2(0.0, 0.0);
-            const double2 *col = Z + (size_t)N * (cvalid ? n : 0);
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                a[j][q] = (cvalid && rv[q]) ? __ldcs(col + r0 + lane + 32 * q) : make_double2(0.0, 0.0);
-        }
-        double2 cs[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            cs[j] = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const double2 v = a[j][q];
-                rs[q].x += v.x * xn[j].x - v.y * xn[j].y;
-                rs[q].y += v.x * xn[j].y + v.y * xn[j].x;
-                cs[j].x += v.x * xr[q].x - v.y * xr[q].y;
-                cs[j].y += v.x * xr[q].y + v.y * xr[q].x;
+    __shared__ int fail;
+    unsigned char *ring = dsm + (((smem_u32(dsm) + 1023u) & ~1023u) - smem_u32(dsm));
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + SRING * SCHUNK);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int G = gridDim.x, items = ntiles * B;
+    auto live = [&](int it) -> bool { return !flags[(size_t)(it / ntiles) * fstride]; };
+    // producer state (thread 0): chunk p_c of item p_it is the next to load
+    int p_it = blockIdx.x, p_c = 0, issued = 0;
+    auto produce = [&]() {
+        if (p_it >= items) return;
+        const int f = p_it / ntiles, t = p_it - f * ntiles;
+        int I, J;
+        tile_of(t, I, J);
+        uint64_t *bar = full + issued % SRING;
+        mbar_expect_tx(bar, SCHUNK);
+        tma_load_3d(&zmap, ring + (issued % SRING) * SCHUNK, 2 * I * ST, J * ST + p_c * SC, f, bar);
+        issued++;
+        if (++p_c == ST / SC) {
+            p_c = 0;
+            for (p_it += G; p_it < items && !live(p_it); p_it += G) {
             }
         }
-        if (offdiag) {   // block-uniform
-            // lanes with bit 4 set keep columns 2, 3 (send 0, 1), the others keep 0, 1
-            const bool b4 = lane & 16, b3 = lane & 8;
-            double2 k0 = b4 ? cs[2] : cs[0], k1 = b4 ? cs[3] : cs[1];
-            cadd(k0, shfl_xor2(b4 ? cs[0] : cs[2], 16));
-            cadd(k1, shfl_xor2(b4 ? cs[1] : cs[3], 16));
-            // bit 3 picks one of the two
-            double2 k = b3 ? k1 : k0;
-            cadd(k, shfl_xor2(b3 ? k0 : k1, 8));
-            cadd(k, shfl_xor2(k, 4));
-            cadd(k, shfl_xor2(k, 2));
-            cadd(k, shfl_xor2(k, 1));
-            // lane 8 c holds column cb + c (c = 2 b4 + b3)
-            if ((lane & 7) == 0) csum[cb + (lane >> 3)] = k;
-        }
+    };
+    if (tid == 0) {
+        for (int s = 0; s < SRING; s++) mbar_init(full + s, 1);
+        mbar_init_fence();
+        fail = 0;
+        while (p_it < items && !live(p_it)) p_it += G;
+        for (int s = 0; s < SRING; s++) produce();
     }
-#pragma unroll
-    for (int q = 0; q < 4; q++) rsum[warp][lane + 32 * q] = rs[q];
     __syncthreads();
-    double2 *out = P + ((size_t)f * gridDim.x + blockIdx.x) * 2 * ST;
-    if (threadIdx.x < ST) {
-        double2 t = make_double2(0.0, 0.0);
-        for (int w = 0; w < 8; w++) {
-            t.x += rsum[w][threadIdx.x].x;
-            t.y += rsum[w][threadIdx.x].y;
+    int cc = 0;
+    for (int it = blockIdx.x; it < items; it += G) {
+        if (!live(it)) continue;
+        const int f = it / ntiles, t = it - f * ntiles;
+        int I, J;
+        tile_of(t, I, J);
+        const double2 *x = xb + (size_t)N * f;
+        const int r0 = I * ST, c0 = J * ST;
+        const bool offdiag = I != J;
+        double2 xr[4], rs[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int m = r0 + lane + 32 * q;
+            xr[q] = m < N ? x[m] : make_double2(0.0, 0.0);
+            rs[q] = make_double2(0.0, 0.0);
         }
-        out[threadIdx.x] = t;
-    } else if (offdiag) {
-        out[threadIdx.x] = csum[threadIdx.x - ST];
+#pragma unroll 1
+        for (int c = 0; c < ST / SC; c++) {
+            if (!mbar_wait_bounded(full + cc % SRING, (uint32_t)(cc / SRING) & 1u)) fail = 1;
+            const double2 *chunk = reinterpret_cast<const double2 *>(ring + (cc % SRING) * SCHUNK);
+            const int cb = c * SC + warp * 4;   // first column of the warp's group within the tile
+            if (!fail) {
+                double2 a[4][4], xn[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int n = c0 + cb + j;
+                    xn[j] = n < N ? x[n] : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) a[j][q] = chunk[(warp * 4 + j) * ST + lane + 32 * q];
+                }
+                double2 cs[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    cs[j] = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double2 v = a[j][q];
+                        rs[q].x += v.x * xn[j].x - v.y * xn[j].y;
+                        rs[q].y += v.x * xn[j].y + v.y * xn[j].x;
+                        cs[j].x += v.x * xr[q].x - v.y * xr[q].y;
+                        cs[j].y += v.x * xr[q].y + v.y * xr[q].x;
+                    }
+                }
+                if (offdiag) {   // block-uniform
+                    // lanes with bit 4 set keep columns 2, 3 (send 0, 1), the others keep 0, 1
+                    const bool b4 = lane & 16, b3 = lane & 8;
+                    double2 k0 = b4 ? cs[2] : cs[0], k1 = b4 ? cs[3] : cs[1];
+                    cadd(k0, shfl_xor2(b4 ? cs[0] : cs[2], 16));
+                    cadd(k1, shfl_xor2(b4 ? cs[1] : cs[3], 16));
+                    // bit 3 picks one of the two
+                    double2 k = b3 ? k1 : k0;
+                    cadd(k, shfl_xor2(b3 ? k0 : k1, 8));
+                    cadd(k, shfl_xor2(k, 4));
+                    cadd(k, shfl_xor2(k, 2));
+                    cadd(k, shfl_xor2(k, 1));
+                    // lane 8 c holds column cb + c (c = 2 b4 + b3)
+                    if ((lane & 7) == 0) csum[cb + (lane >> 3)] = k;
+                }
+            }
+            __syncthreads();   // every warp is done with the stage
+            if (fail) {
+                // a chunk never arrived: every frequency of the launch falls back
+                if (tid < B) atomicExch(reinterpret_cast<int *>(ctl + 64 * tid + 36), 3);
+                if (tid == 0)
+                    for (int k = cc + 1; k < issued; k++)
+                        if (!mbar_wait_bounded(full + k % SRING, (uint32_t)(k / SRING) & 1u)) break;
+                return;
+            }
+            if (tid == 0) produce();
+            cc++;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) rsum[warp][lane + 32 * q] = rs[q];
+        __syncthreads();
+        double2 *out = P + ((size_t)f * ntiles + t) * 2 * ST;
+        if (tid < ST) {
+            double2 v = make_double2(0.0, 0.0);
+            for (int w = 0; w < 8; w++) {
+                v.x += rsum[w][tid].x;
+                v.y += rsum[w][tid].y;
+            }
+            out[tid] = v;
+        } else if (offdiag) {
+            out[tid] = csum[tid - ST];
+        }
+        __syncthreads();   // rsum and csum are free for the next item
     }
 }
 
@@ -483,14 +537,33 @@ __global__ void k_gm_stop_flags(int B, const GmState *__restrict__ st, int *__re
     if (f < B) out[f] = st[f].stop;
 }
 
+// the map of Z (all slots) for k_symv_ring: doubles [B][N][2N] (innermost
+// first: re/im of a row, column, slot), boxes of 128 rows x 32 columns
+efie_status symv_map(SolveWork &w, const void *Z, size_t zstride) {
+    if (w.zmap_base == Z && w.zmap_stride == zstride && w.zmap_n == w.N && w.zmap_b == w.B) return EFIE_OK;
+    const cuuint64_t dims[3] = {2 * (cuuint64_t)w.N, (cuuint64_t)w.N, (cuuint64_t)w.B};
+    const cuuint64_t strides[2] = {sizeof(double2) * (cuuint64_t)w.N, sizeof(double2) * (cuuint64_t)zstride};
+    const cuuint32_t box[3] = {2 * ST, SC, 1};
+    EFIE_TRY(efie_encode_tiled(w.zmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(Z), dims, strides, box,
+                               CU_TENSOR_MAP_SWIZZLE_NONE));
+    w.zmap_base = Z;
+    w.zmap_stride = zstride;
+    w.zmap_n = w.N;
+    w.zmap_b = w.B;
+    return EFIE_OK;
+}
+
 efie_status symv(efie_ctx *ctx, SolveWork &w, const void *Z, size_t zstride, const double2 *x, double2 *y,
                  const int *flags, int fstride) {
     const int nb = (w.N + ST - 1) / ST;
     const size_t ntiles = (size_t)nb * (nb + 1) / 2;
     EFIE_TRY(w.spart.reserve(sizeof(double2) * ntiles * 2 * ST * w.B));
+    EFIE_TRY(symv_map(w, Z, zstride));
+    EFIE_CUDA(cudaFuncSetAttribute(k_symv_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SYMV_SMEM));
     cudaStream_t s = ctx->stream;
-    k_symv_tiles<<<dim3((unsigned)ntiles, w.B), 256, 0, s>>>(w.N, static_cast<const double2 *>(Z), zstride, x,
-                                                              w.spart.as<double2>(), flags, fstride);
+    const int grid = (int)std::min<size_t>((size_t)ctx->num_sms, ntiles * w.B);
+    k_symv_ring<<<grid, 256, SYMV_SMEM, s>>>(*reinterpret_cast<const CUtensorMap *>(w.zmap), w.N, (int)ntiles, w.B,
+                                             x, w.spart.as<double2>(), flags, fstride, w.ctl.as<char>());
     k_symv_reduce<<<dim3(nb, w.B), ST, 0, s>>>(w.N, nb, w.spart.as<double2>(), y, flags, fstride);
     EFIE_CUDA(cudaGetLastError());
     return EFIE_OK;

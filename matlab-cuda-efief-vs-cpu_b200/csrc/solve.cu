@@ -30,6 +30,10 @@ namespace {
 
 constexpr int NB = 64;   // diagonal block size of the LU and the triangular solves
 constexpr size_t kTwoTiles = sizeof(float2) * 2 * NB * (NB + 1);
+// k_panels' tiles: rows padded to 66 complex (528 bytes, a multiple of 16) so
+// that two consecutive entries of a row load as one float4
+constexpr int PS = NB + 2;
+constexpr size_t kPanelSmem = sizeof(float2) * 2 * NB * PS;
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -352,7 +356,7 @@ __device__ __forceinline__ void emit_block(const float2 (&acc)[4][4], bool ublk,
 // the re/im planes (rows are 16-byte aligned: ld and the offsets are
 // multiples of 64).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, float *__restrict__ planes,
+__global__ void __launch_bounds__(256, 3) k_panels(int N, int k, int kb, int bi, float *__restrict__ planes,
                                                 size_t pstride, int ld, const float2 *__restrict__ dinv,
                                                 size_t dstride, const int *__restrict__ active,
                                                 float *__restrict__ lmax, float *__restrict__ umax,
@@ -362,8 +366,8 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     const int f = blockIdx.z;
     if (!active[f]) return;
     extern __shared__ float2 dyn[];
-    float2(*M)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn);               // the inverse
-    float2(*T)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn + NB * (NB + 1));  // the panel tile
+    float2(*M)[PS] = reinterpret_cast<float2(*)[PS]>(dyn);             // the inverse
+    float2(*T)[PS] = reinterpret_cast<float2(*)[PS]>(dyn + NB * PS);  // the panel tile
     float *Ar = planes + pstride * f, *Ai = Ar + (size_t)ld * N;
     const float2 *Linv = dinv + dstride * f + (size_t)bi * 2 * NB * NB, *Uinv = Linv + NB * NB;
     const int tid = threadIdx.x;
@@ -401,44 +405,52 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
     if (sym) {
         // U[k + i][off + j] = sum_q Linv[i][q] T[j][q] (T: rows off.. of the
         // lower part), and with U^-1 = L^-T D^-1 the column panel follows
-        // from it exactly: L[off + j][k + i] = U[i][j] / d_i
-        __shared__ float ured[NB][17], lred[NB][17];
+        // from it exactly: L[off + j][k + i] = U[i][j] / d_i.  Only U is kept
+        // in registers; L is formed from it where it is used, so the kernel
+        // fits three CTAs per SM.
         __shared__ float umx[NB], lmx[NB];
         __shared__ float2 rdiag[NB];
         if (tid < NB) rdiag[tid] = Uinv[tid * NB + tid];   // 1 / d_i
-        float2 au[4][4], al[4][4];
+        float2 au[4][4];
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int b = 0; b < 4; b++) au[a][b] = make_float2(0.f, 0.f);
-#pragma unroll 4
-        for (int q = 0; q < NB; q++) {
-            float2 x[4], y[4];
+        // two steps of q per pass: entries q, q + 1 of a row are one float4
+#pragma unroll 2
+        for (int q = 0; q < NB; q += 2) {
+            float4 x[4], y[4];
 #pragma unroll
             for (int a = 0; a < 4; a++) {
-                x[a] = M[ty + 16 * a][q];
-                y[a] = T[tx + 16 * a][q];
+                x[a] = *reinterpret_cast<const float4 *>(&M[ty + 16 * a][q]);
+                y[a] = *reinterpret_cast<const float4 *>(&T[tx + 16 * a][q]);
             }
 #pragma unroll
             for (int a = 0; a < 4; a++)
 #pragma unroll
-                for (int b = 0; b < 4; b++) cfma(au[a][b], x[a], y[b]);
+                for (int b = 0; b < 4; b++) {
+                    cfma(au[a][b], make_float2(x[a].x, x[a].y), make_float2(y[b].x, y[b].y));
+                    cfma(au[a][b], make_float2(x[a].z, x[a].w), make_float2(y[b].z, y[b].w));
+                }
         }
         __syncthreads();   // M, T and rdiag: M and T are free from here
+        // the maxima's partial reductions live in M until the L rows are out
+        float(*ured)[17] = reinterpret_cast<float(*)[17]>(&M[0][0]);
+        float(*lred)[17] = ured + NB;
         float cu[4] = {0.f, 0.f, 0.f, 0.f}, cl[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int b = 0; b < 4; b++) {
                 const int i = ty + 16 * a, j = tx + 16 * b;
-                al[a][b] = cmulf(au[a][b], rdiag[i]);
-                T[j][i] = al[a][b];   // L tile, row j
+                const float2 l = cmulf(au[a][b], rdiag[i]);
+                T[j][i] = l;   // L tile, row j
                 if (i < kb && j < ext) {
                     const size_t o = (size_t)(k + i) * ld + off + j;
                     Ar[o] = au[a][b].x;
                     Ai[o] = au[a][b].y;
                     cu[b] = fmaxf(cu[b], fmaxf(fabsf(au[a][b].x), fabsf(au[a][b].y)));
-                    cl[b] = fmaxf(cl[b], fmaxf(fabsf(al[a][b].x), fabsf(al[a][b].y)));
+                    cl[b] = fmaxf(cl[b], fmaxf(fabsf(l.x), fabsf(l.y)));
                 }
             }
 #pragma unroll
@@ -467,15 +479,19 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
                 lmax[mstride * f + (size_t)(off + tid) * nblk + bi] = ml;
             }
         }
-        __syncthreads();   // T (the L staging) is free
+        __syncthreads();   // T (the L staging) and M (the partial maxima) are free
         if (!emit) return;
-        // operands of the panel chain's update: L rows (columns of the U
-        // tile) always, the U block when its columns lie inside the panel
-        emit_block(al, true, lmx, reinterpret_cast<__half *>(&T[0][0]),
-                   ipl + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
+        // operands of the panel chain's update: the U block when its columns
+        // lie inside the panel, then the L rows (columns of the U tile) always
         if (off < kend)
             emit_block(au, true, umx, reinterpret_cast<__half *>(&M[0][0]),
                        ipu + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) au[a][b] = cmulf(au[a][b], rdiag[ty + 16 * a]);
+        emit_block(au, true, lmx, reinterpret_cast<__half *>(&T[0][0]),
+                   ipl + ipstride * f + (size_t)(off - k - kb) * 32, ippitch, tid, ty, tx);
         return;
     }
     float2 acc[4][4];
@@ -484,8 +500,8 @@ __global__ void __launch_bounds__(256) k_panels(int N, int k, int kb, int bi, fl
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
     // row panel: out = M * T; column panel: out = T * M
-    const float2(*X)[NB + 1] = rowp ? M : T;
-    const float2(*Y)[NB + 1] = rowp ? T : M;
+    const float2(*X)[PS] = rowp ? M : T;
+    const float2(*Y)[PS] = rowp ? T : M;
 #pragma unroll 4
     for (int q = 0; q < NB; q++) {
         float2 x[4], y[4];
@@ -813,7 +829,7 @@ __global__ void k_init_ctl(int B, char *__restrict__ ctl, double bnorm, const in
 efie_status set_smem_attrs() {
     static bool done = false;
     if (done) return EFIE_OK;
-    EFIE_CUDA(cudaFuncSetAttribute(k_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
+    EFIE_CUDA(cudaFuncSetAttribute(k_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem));
     EFIE_CUDA(cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTwoTiles));
     done = true;
@@ -954,7 +970,7 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
                                                         sym ? (g_sym_lu_disabled == 3 ? 2 : 1) : 0);
                 if (rest > 0) {
                     dim3 pg((rest + NB - 1) / NB, sym ? 1 : 2, B);
-                    k_panels<<<pg, 256, kTwoTiles, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
+                    k_panels<<<pg, 256, kPanelSmem, s>>>(N, k, kb, bi, planes, w.pstride, ld, dinv, w.dstride,
                                                         active, w.lmax.as<float>(), w.umax.as<float>(), w.mstride,
                                                         w.nblk, w.ipL.as<__half>(), w.ipU.as<__half>(), ipl.stride,
                                                         ipl.pitch, inpanel ? 1 : 0, sym ? 1 : 0, Kend);

@@ -77,6 +77,12 @@ struct SolveWork {
     // of 32 x 32: the tensor-core update adds its tiles into the factors with
     // bulk tensor reductions
     alignas(64) unsigned char planes_map[128] = {};
+    // TMA tensor map of Z (complex128, all slots) for the GMRES products, and
+    // the buffer, slot stride and sizes it was encoded for
+    alignas(64) unsigned char zmap[128] = {};
+    const void *zmap_base = nullptr;
+    size_t zmap_stride = 0;
+    int zmap_n = 0, zmap_b = 0;
     SolveWork() = default;
     SolveWork(const SolveWork &) = delete;
     SolveWork &operator=(const SolveWork &) = delete;

@@ -16,12 +16,14 @@
 #include <algorithm>
 #include <cstdint>
 
-#include <cuda.h>
 
 #include "efie_internal.h"
 #include "solve.h"
+#include "tma.h"
 
 namespace {
+
+using namespace efie_tma;
 
 constexpr int NB = 64;
 constexpr int LINE = 8;       // u64 per 64-byte progress line
@@ -54,64 +56,10 @@ __device__ __forceinline__ unsigned long long wait_progress(const volatile unsig
     return v;
 }
 
-// ---------------------------------------------------------------------------
-// TMA / mbarrier primitives (inline PTX)
-// ---------------------------------------------------------------------------
 constexpr int TS = 3;                                          // stages of the tile ring
 constexpr uint32_t STAGE_BYTES = 2u * NB * NB * sizeof(float);  // a 64 x 64 complex tile: 32 KB
 constexpr uint32_t BOX_BYTES = 32u * 32u * sizeof(float);       // one 32 x 32 box of one plane
 constexpr size_t TRSV_SMEM = TS * STAGE_BYTES + 1024 + 64;      // ring (1024-aligned) + barriers
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for a stage: false after about a second of polling.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (long long i = 0; i < (1ll << 22); i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
-    }
-    return false;
-}
-
-// one 32 x 32 box of the planes tensor [B][2][N][N] (column x, row y, plane, slot)
-__device__ __forceinline__ void tma_box(const CUtensorMap *map, void *dst, int x, int y, int plane, int f,
-                                        uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(plane), "r"(f), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
 
 __device__ __forceinline__ float2 dot16(const float4 (&t)[8], const float2 *y) {
     const float *re = reinterpret_cast<const float *>(t);
@@ -188,8 +136,8 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
                 for (int rh = 0; rh < 2; rh++)
 #pragma unroll
                     for (int ch = 0; ch < 2; ch++)
-                        tma_box(&map, st + ((pl * 2 + rh) * 2 + ch) * BOX_BYTES, jb * NB + ch * 32, b * NB + rh * 32,
-                                pl, f, bar);
+                        tma_load_4d(&map, st + ((pl * 2 + rh) * 2 + ch) * BOX_BYTES, jb * NB + ch * 32,
+                                    b * NB + rh * 32, pl, f, bar);
         } else {
             bulk_g2s(st, dinv + dstride * f + (size_t)b * 2 * NB * NB + (LOWER ? 0 : NB * NB), STAGE_BYTES, bar);
         }
@@ -202,7 +150,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
     };
     if (tid == 0) {
         for (int s = 0; s < TS; s++) mbar_init(full + s, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init_fence();
         fail = 0;
         while (p_it < items && !live(p_it)) p_it += G;
         for (int s = 0; s < TS; s++) produce();
