@@ -709,15 +709,18 @@ __global__ void __launch_bounds__(256) k_gather_z_sym(int Ne, int Nt, const Edge
     __syncthreads();
     if (pr) {
         float *pi = pr + (size_t)ld * Ne;
-        // row m = bm * 32 + j of the planes, columns n = bn * 32 + tx
-        for (int j = ty; j < 32; j += 8) {
-            const int mm = bm * 32 + j, nn = bn * 32 + tx;
-            if (mm < Ne && nn < Ne) {
-                const double2 v = tile[tx][j];
-                pr[(size_t)mm * ld + nn] = (float)v.x;
-                pi[(size_t)mm * ld + nn] = (float)v.y;
+        // the L D L^T factorization reads the lower triangle of the planes
+        // only (it writes the upper one itself): row m = bm * 32 + j,
+        // columns n = bn * 32 + tx on the diagonal tiles
+        if (bm == bn)
+            for (int j = ty; j < 32; j += 8) {
+                const int mm = bm * 32 + j, nn = bn * 32 + tx;
+                if (mm < Ne && nn < Ne) {
+                    const double2 v = tile[tx][j];
+                    pr[(size_t)mm * ld + nn] = (float)v.x;
+                    pi[(size_t)mm * ld + nn] = (float)v.y;
+                }
             }
-        }
         if (bm != bn)   // row n = bn * 32 + j, columns m = bm * 32 + tx: Z(n, m) = Z(m, n)
             for (int j = ty; j < 32; j += 8) {
                 const int nn = bn * 32 + j, mm = bm * 32 + tx;
@@ -729,6 +732,28 @@ __global__ void __launch_bounds__(256) k_gather_z_sym(int Ne, int Nt, const Edge
             }
     }
     if (bm == bn) return;
+    // with the planes (the mixed solver), Z's lower triangle is written only
+    // inside the 128 x 128 diagonal blocks that the symmetric GMRES product
+    // reads in full; efie_z_mirror completes it for the paths that need all of Z
+    if (pr && bm / 4 != bn / 4) return;
+    for (int j = ty; j < 32; j += 8) {
+        const int mm = bm * 32 + j, nn = bn * 32 + tx;
+        if (mm < Ne && nn < Ne) Z[(size_t)nn + (size_t)Ne * mm] = tile[tx][j];
+    }
+}
+
+// Z(n, m) = Z(m, n) on the 32 x 32 tiles that k_gather_z_sym leaves out with
+// the planes (upper tile (bm, bn), bm < bn, in different 128-blocks)
+__global__ void __launch_bounds__(256) k_z_mirror(int Ne, double2 *__restrict__ Z) {
+    const int bm = blockIdx.x, bn = blockIdx.y;
+    if (bm >= bn || bm / 4 == bn / 4) return;
+    __shared__ double2 tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int j = ty; j < 32; j += 8) {
+        const int m = bm * 32 + tx, n = bn * 32 + j;
+        if (m < Ne && n < Ne) tile[j][tx] = Z[(size_t)m + (size_t)Ne * n];
+    }
+    __syncthreads();
     for (int j = ty; j < 32; j += 8) {
         const int mm = bm * 32 + j, nn = bn * 32 + tx;
         if (mm < Ne && nn < Ne) Z[(size_t)nn + (size_t)Ne * mm] = tile[tx][j];
@@ -1220,9 +1245,18 @@ efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, i
         else k_gather_z<false><<<gg, 256, 0, s>>>(Ne, Nt, false, E, mom, Zd);
     }
     EFIE_CUDA(cudaGetLastError());
-    // algorithmic bytes: one read of every pair value, Z (and the planes) written once
+    // algorithmic bytes: one read of every pair value, Z written once (with
+    // the planes: Z's upper and the planes' lower triangle)
     log.end(EFIE_K_GATHER, s, tok,
-            16.0 * (g.combo ? 9.0 : 8.0) * (double)g.npairs + (pr ? 24.0 : 16.0) * (double)Ne * Ne);
+            16.0 * (g.combo ? 9.0 : 8.0) * (double)g.npairs +
+                (pr ? 12.0 * (double)Ne * (Ne + 1) : 16.0 * (double)Ne * Ne));
+    return EFIE_OK;
+}
+
+efie_status efie_z_mirror(efie_ctx *ctx, void *Z, int Ne) {
+    dim3 gs((Ne + 31) / 32, (Ne + 31) / 32);
+    k_z_mirror<<<gs, 256, 0, ctx->stream>>>(Ne, static_cast<double2 *>(Z));
+    EFIE_CUDA(cudaGetLastError());
     return EFIE_OK;
 }
 

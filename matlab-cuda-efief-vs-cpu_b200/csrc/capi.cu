@@ -754,6 +754,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         }
     }
     if (warm) EFIE_TRY(p->xall.reserve(sizeof(efie_c128) * (size_t)N * Nf));
+    auto Zslot = [&](int f) -> void * { return p->Z.as<efie_c128>() + NN * f; };
     for (int bi = 0; bi < nbat && rc == EFIE_OK; bi++) {
         const int f0 = bstart[bi], nb = bstart[bi + 1] - f0;
         int active[EFIE_MAX_BATCH] = {0};
@@ -786,6 +787,9 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 rc = efie_interp_guess(ctx, N, nb, p->x.p, p->xall.p, g);
                 if (rc != EFIE_OK) break;
             }
+            if (p->opts.refine_method == EFIE_REFINE_CLASSICAL && p->sw.planes_from_assembly)
+                for (int f = 0; f < nb && rc == EFIE_OK; f++) rc = efie_z_mirror(ctx, Zslot(f), N);
+            if (rc != EFIE_OK) break;
             if (p->opts.refine_method == EFIE_REFINE_CLASSICAL)
                 rc = efie_mixed_refine(ctx, p->sw, p->Z.p, NN, p->b.p, p->x.p, p->bnorm, p->opts.refine_tol,
                                        p->opts.refine_max_iter, active, &rr);
@@ -807,6 +811,10 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 if (nr > 0) {
                     RefineResult r2;
                     const bool pfa = p->sw.planes_from_assembly;
+                    // the general LU converts all of Z
+                    for (int f = 0; f < nb && rc == EFIE_OK; f++)
+                        if (retry[f] && pfa) rc = efie_z_mirror(ctx, Zslot(f), N);
+                    if (rc != EFIE_OK) break;
                     p->sw.sym_lu = false;
                     p->sw.planes_from_assembly = false;
                     rc = efie_mixed_factor(ctx, p->sw, p->Z.p, NN, retry);
@@ -836,7 +844,9 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         }
         for (int f = 0; f < nb && rc == EFIE_OK; f++) {
             if (mixed && !fallback[f]) continue;
-            // cuSOLVER Zgetrf/Zgetrs: timed in class OTHER, not counted as our launches
+            // cuSOLVER Zgetrf/Zgetrs on all of Z: timed in class OTHER, not counted as our launches
+            if (mixed && p->sw.planes_from_assembly) rc = efie_z_mirror(ctx, Zslot(f), N);
+            if (rc != EFIE_OK) break;
             size_t tok = log.begin(ctx->stream);
             rc = plan_solve_fp64(p, f, f0 + f);
             if (rc == EFIE_OK) log.end(EFIE_K_OTHER, ctx->stream, tok, 8.0 / 3.0 * (double)N * N * N, 0);

@@ -193,6 +193,11 @@ Physics efie_physics_k(efie_c128 k, double omega, double mu, efie_c128 eps);
 // list are computed on the device from V/F with the options `popts`
 efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_prepack *pre, int scheme,
                              int rule_order, GeomDev &g, const efie_precompute_opts *popts = nullptr);
+// The batch assembly with complex64 planes writes Z's upper triangle (and
+// its 128 x 128 diagonal blocks): this completes the lower triangle of one
+// slot for the paths that read all of Z (complex128 fallback, general-LU
+// retry, classical refinement)
+efie_status efie_z_mirror(efie_ctx *ctx, void *Z, int Ne);
 // precompute.cu: efie_precompute + efie_precompute_pack on the device, straight
 // into the plan's layout (origins, cache points, near-pair list)
 efie_status efie_geom_precompute_device(efie_ctx *ctx, const efie_mesh *mesh, const efie_precompute_opts *o,

@@ -931,7 +931,12 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     const int *active = w.active.as<int>();
     dim3 tg((N + 31) / 32, (N + 31) / 32, B);
     size_t tok = 0;
-    if (!w.planes_from_assembly) {
+    const bool sym = w.zsym && w.sym_lu && g_sym_lu_disabled != 1;
+    if (!w.planes_from_assembly || !sym) {
+        // the general LU reads the upper triangle of the planes too: from all of Z
+        if (w.planes_from_assembly)
+            for (int f = 0; f < B; f++)
+                EFIE_TRY(efie_z_mirror(ctx, static_cast<double2 *>(const_cast<void *>(Z)) + zstride * f, N));
         tok = log.begin(s0);
         k_z_to_planes<<<tg, 256, 0, s0>>>(N, static_cast<const double2 *>(Z), zstride, planes, w.pstride, ld);
         EFIE_CUDA(cudaGetLastError());
@@ -946,7 +951,6 @@ efie_status efie_mixed_factor_launch(efie_ctx *ctx, SolveWork &w, const void *Z,
     // lower triangle and the row panel is formed from the column panel's
     // tiles, U[k.., j] = L_kk^-1 A[j, k..]^T, so that L and U follow from
     // the same (lower) data
-    const bool sym = w.zsym && w.sym_lu && g_sym_lu_disabled != 1;
     const bool symtri = sym && g_sym_lu_disabled != 2;
     bool rest_pending = false;   // ev_rest holds the record of the previous D^rest
     // with per-launch timing on, D^rest goes to the chain's stream too: the
