@@ -463,6 +463,121 @@ __global__ void __launch_bounds__(256) k_self_moments(
     if (lane == 0) store_mom(mom, pair_slot(t, t, Nt, sym), t, t, m);
 }
 
+// Near and self pairs of F equally spaced frequencies in one launch (the
+// reference scheme's subdivided rules): one warp per pair as in
+// k_near_moments / k_self_moments, each point pair's R, 1/(4 pi R) and phase
+// shared by the F frequencies as in k_regular_moments_mf.
+template <int F>
+__device__ __forceinline__ void acc_qpe_mf(double (&m)[F][16], const double4 &pp, const double4 &pq, double R2,
+                                           double kr0, double ki0, double dkr, double dki) {
+    R2 = fmax(R2, 1e-30);   // R >= 1e-15
+    const double rs = rsqrt(R2);
+    const double R = R2 * rs;
+    double inv = pp.w * pq.w * (1.0 / (4.0 * kPi)) * rs;
+    double s0, c0, ss, cs;
+    sincos(kr0 * R, &s0, &c0);
+    const double x = dkr * R;
+    if (fabs(x) <= 0.5) small_sincos(x, ss, cs);
+    else sincos(x, &ss, &cs);
+    if (ki0 != 0.0) inv *= exp(ki0 * R);
+    double esr = cs, esi = -ss;   // e^{-j dk R}
+    if (dki != 0.0) {
+        const double e = exp(dki * R);
+        esr *= e;
+        esi *= e;
+    }
+    double gr = c0 * inv, gi = -s0 * inv;
+    const double dd = pp.x * pq.x + pp.y * pq.y + pp.z * pq.z;
+#pragma unroll
+    for (int f = 0; f < F; f++) {
+        m[f][0] += gr; m[f][1] += gi;
+        m[f][2] += gr * pp.x; m[f][3] += gi * pp.x;
+        m[f][4] += gr * pp.y; m[f][5] += gi * pp.y;
+        m[f][6] += gr * pp.z; m[f][7] += gi * pp.z;
+        m[f][8] += gr * pq.x; m[f][9] += gi * pq.x;
+        m[f][10] += gr * pq.y; m[f][11] += gi * pq.y;
+        m[f][12] += gr * pq.z; m[f][13] += gi * pq.z;
+        m[f][14] += gr * dd; m[f][15] += gi * dd;
+        if (f + 1 < F) {
+            const double nr = gr * esr - gi * esi;
+            gi = gr * esi + gi * esr;
+            gr = nr;
+        }
+    }
+}
+
+template <int F>
+__device__ __forceinline__ void warp_store_mf(double (&m)[F][16], int lane, const MomStores &ms, size_t slot, int t1,
+                                              int t2) {
+#pragma unroll
+    for (int f = 0; f < F; f++)
+#pragma unroll
+        for (int i = 0; i < 16; i++) m[f][i] = warp_sum(m[f][i]);
+    if (lane == 0)
+#pragma unroll
+        for (int f = 0; f < F; f++) store_mom(ms.s[f], slot, t1, t2, m[f]);
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_near_moments_mf(
+    int Nt, bool sym, int n_pairs, const int2 *__restrict__ list, int P, const double4 *__restrict__ origin,
+    const double4 *__restrict__ pts, const double *__restrict__ aeq, double near_alpha, double kr0, double ki0,
+    double dkr, double dki, MomStores ms) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_pairs) return;
+    const int2 pr = list[warp];
+    const int t1 = pr.x, t2 = pr.y;
+    const double4 o1 = origin[t1], o2 = origin[t2];
+    const double dox = o1.x - o2.x, doy = o1.y - o2.y, doz = o1.z - o2.z;
+    const double a = near_alpha * fmin(aeq[t1], aeq[t2]);
+    const double a2 = a * a;
+    double m[F][16];
+#pragma unroll
+    for (int f = 0; f < F; f++)
+#pragma unroll
+        for (int i = 0; i < 16; i++) m[f][i] = 0.0;
+    const int total = P * P;
+    for (int e = lane; e < total; e += 32) {
+        const int p = e / P, q = e - p * P;
+        const double4 pp = pts[(size_t)t1 * P + p];
+        const double4 pq = pts[(size_t)t2 * P + q];
+        const double dx = dox + pp.x - pq.x, dy = doy + pp.y - pq.y, dz = doz + pp.z - pq.z;
+        acc_qpe_mf<F>(m, pp, pq, dx * dx + dy * dy + dz * dz + a2, kr0, ki0, dkr, dki);
+    }
+    warp_store_mf<F>(m, lane, ms, pair_slot(t1, t2, Nt, sym), t1, t2);
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_self_moments_mf(int Nt, bool sym, int P, int Nq2,
+                                                         const double4 *__restrict__ pts,
+                                                         const double *__restrict__ self_a, int NsS, double kr0,
+                                                         double ki0, double dkr, double dki, MomStores ms) {
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= Nt) return;
+    double m[F][16];
+#pragma unroll
+    for (int f = 0; f < F; f++)
+#pragma unroll
+        for (int i = 0; i < 16; i++) m[f][i] = 0.0;
+    const int total = P * P;
+    for (int e = lane; e < total; e += 32) {
+        const int p = e / P, q = e - p * P;
+        const double4 pp = pts[(size_t)t * P + p];
+        const double4 pq = pts[(size_t)t * P + q];
+        const double dx = pp.x - pq.x, dy = pp.y - pq.y, dz = pp.z - pq.z;
+        double R2 = dx * dx + dy * dy + dz * dz;
+        const int sp = p / Nq2, sq = q / Nq2;
+        if (sp == sq) {
+            const double aS = self_a[(size_t)t * NsS + sp];
+            R2 += aS * aS;
+        }
+        acc_qpe_mf<F>(m, pp, pq, R2, kr0, ki0, dkr, dki);
+    }
+    warp_store_mf<F>(m, lane, ms, pair_slot(t, t, Nt, sym), t, t);
+}
+
 // ---------------------------------------------------------------------------
 // Extraction scheme (no reference counterpart): on self and vertex-adjacent
 // pairs G = 1/(4 pi R) + (exp(-jkR) - 1)/(4 pi R).  The static part is
@@ -1126,6 +1241,27 @@ void launch_regular_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, cons
     }
 }
 
+template <int F>
+void launch_nearself_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, const MomStores &ms, double &qpe,
+                        int &nl) {
+    const double dkr = (ph[F - 1].kr - ph[0].kr) / (F - 1), dki = (ph[F - 1].ki - ph[0].ki) / (F - 1);
+    const double4 *org = g.origin.as<double4>();
+    if (g.n_near > 0) {
+        const int P = g.NsN * g.Nq2;
+        k_near_moments_mf<F><<<(g.n_near + 7) / 8, 256, 0, s>>>(g.Nt, g.symmetric, g.n_near, g.near_list.as<int2>(),
+                                                                P, org, g.near_pts.as<double4>(), g.aeq.as<double>(),
+                                                                g.near_alpha, ph[0].kr, ph[0].ki, dkr, dki, ms);
+        nl++;
+        qpe += (double)g.n_near * P * P;
+    }
+    const int P = g.NsS * g.Nq2;
+    k_self_moments_mf<F><<<(g.Nt + 7) / 8, 256, 0, s>>>(g.Nt, g.symmetric, P, g.Nq2, g.self_pts.as<double4>(),
+                                                        g.self_a.as<double>(), g.NsS, ph[0].kr, ph[0].ki, dkr, dki,
+                                                        ms);
+    nl++;
+    qpe += (double)g.Nt * P * P;
+}
+
 // k_f = k0 + f dk within 1e-12 |k_f| for f < n
 bool equally_spaced(const Physics *ph, int n) {
     if (n < 2) return false;
@@ -1139,7 +1275,8 @@ bool equally_spaced(const Physics *ph, int n) {
 
 }  // namespace
 
-efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld);
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld,
+                                 bool nearself_done = false);
 
 efie_status efie_assemble_device(efie_ctx *ctx, GeomDev &g, const Physics &ph, void *Z, float *pr, int ld) {
     cudaStream_t s = ctx->stream;
@@ -1189,15 +1326,28 @@ efie_status efie_assemble_batch(efie_ctx *ctx, GeomDev &g, const Physics *ph, in
         else launch_regular_mf<4>(g, ctx->stream, ph + f0, ms);
         EFIE_CUDA(cudaGetLastError());
         ctx->log.end(EFIE_K_QUAD, ctx->stream, tok, n * regular_pairs(g) * (double)g.Nq * g.Nq);
+        // the reference scheme's near and self pairs of the group, likewise
+        const bool ns = g.scheme == EFIE_SCHEME_REF;
+        if (ns) {
+            tok = ctx->log.begin(ctx->stream);
+            double qpe = 0;
+            int nl = 0;
+            if (n == 2) launch_nearself_mf<2>(g, ctx->stream, ph + f0, ms, qpe, nl);
+            else if (n == 3) launch_nearself_mf<3>(g, ctx->stream, ph + f0, ms, qpe, nl);
+            else launch_nearself_mf<4>(g, ctx->stream, ph + f0, ms, qpe, nl);
+            EFIE_CUDA(cudaGetLastError());
+            ctx->log.end(EFIE_K_NEARSELF, ctx->stream, tok, n * qpe, nl);
+        }
         for (int j = 0; j < n; j++)
-            EFIE_TRY(efie_assemble_finish(ctx, g, ph[f0 + j], j, Z[f0 + j], planes(f0 + j), ld));
+            EFIE_TRY(efie_assemble_finish(ctx, g, ph[f0 + j], j, Z[f0 + j], planes(f0 + j), ld, ns));
         f0 += n;
     }
     return EFIE_OK;
 }
 
 // Near/self (or singular) pairs of one frequency into store j, then its gather.
-efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld) {
+efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, int j, void *Z, float *pr, int ld,
+                                 bool nearself_done) {
     cudaStream_t s = ctx->stream;
     KernelLog &log = ctx->log;
     const int Nt = g.Nt, Ne = g.Ne;
@@ -1206,7 +1356,8 @@ efie_status efie_assemble_finish(efie_ctx *ctx, GeomDev &g, const Physics &ph, i
     size_t tok = log.begin(s);
     int nl = 0;
     double qpe = 0;
-    if (g.scheme == EFIE_SCHEME_EXTRACT) {
+    if (nearself_done) {
+    } else if (g.scheme == EFIE_SCHEME_EXTRACT) {
         k_singular_moments<<<(g.n_adj + 7) / 8, 256, 0, s>>>(Nt, g.n_adj, g.adj_list.as<int2>(), g.Nq, org,
                                                             g.reg_pts.as<double4>(), g.tri_vtx.as<double4>(), ph.kr,
                                                             ph.ki, mom);
