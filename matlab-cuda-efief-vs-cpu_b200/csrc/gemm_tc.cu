@@ -107,6 +107,18 @@ __device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
     l = __float2half_rn(v - __half2float(h));
 }
 
+// four consecutive values times the scale, split into hi and lo halves, each
+// set of four stored as one 8-byte word (4 consecutive k of a swizzled row)
+__device__ __forceinline__ void split4(const float4 &v, float sc, __half *hi, __half *lo) {
+    __half h[4], l[4];
+    split_half(v.x * sc, h[0], l[0]);
+    split_half(v.y * sc, h[1], l[1]);
+    split_half(v.z * sc, h[2], l[2]);
+    split_half(v.w * sc, h[3], l[3]);
+    *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<const uint2 *>(h);
+    *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<const uint2 *>(l);
+}
+
 // the four 128-row component tiles of one chunk to their planes
 __device__ __forceinline__ void store_planes(const __half *t, __half *dst, int pitch) {
     for (int e = threadIdx.x; e < CHUNK_HALVES / 8; e += blockDim.x) {
@@ -132,19 +144,36 @@ __global__ void __launch_bounds__(256) k_pack_l(int N, int r0, int r1, int kcol,
             row < r1 ? pow2_scale(row_max(lmaxb + mstride * f, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < SUB; e += 256) {
-        const int r = e >> 5, kq = e & 31;           // consecutive threads: consecutive k
+    // four groups of four consecutive k per thread (eight 16-byte loads in
+    // flight), split into halves that sit next to each other in the swizzled
+    // row: one 8-byte store per component and group
+    float4 vr[4], vi[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int e = threadIdx.x + 256 * i;
+        const int r = e >> 3, kq = (e & 7) * 4;
         const int k = chunk * KC + kq;
         const int row = r0 + tile * TR + r;
-        float vr = 0.f, vi = 0.f;
-        if (row < r1 && k < K) {
+        vr[i] = vi[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row < r1) {
             const size_t o = (size_t)row * ld + kcol + k;
-            vr = Ar[o] * rscale[r];                   // exact: a power of two
-            vi = Ai[o] * rscale[r];
+            if (k + 3 < K) {
+                vr[i] = __ldg(reinterpret_cast<const float4 *>(Ar + o));
+                vi[i] = __ldg(reinterpret_cast<const float4 *>(Ai + o));
+            } else {
+                float *pr = &vr[i].x, *pi = &vi[i].x;
+                for (int j = 0; j < 4 && k + j < K; j++) pr[j] = Ar[o + j], pi[j] = Ai[o + j];
+            }
         }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int e = threadIdx.x + 256 * i;
+        const int r = e >> 3, kq = (e & 7) * 4;
+        const float sc = rscale[r];                   // exact: a power of two
         const uint32_t off = swz(r, kq) >> 1;
-        split_half(vr, t[off], t[SUB + off]);
-        split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
+        split4(vr[i], sc, t + off, t + SUB + off);
+        split4(vi[i], sc, t + 2 * SUB + off, t + 3 * SUB + off);
     }
     __syncthreads();
     store_planes(t, outb + ostride * f + ((size_t)chunk * 4 * pitch + (size_t)tile * TR) * KC, pitch);
@@ -167,19 +196,34 @@ __global__ void __launch_bounds__(256) k_pack_u(int N, int c0, int c1, int krow,
             col < c1 ? pow2_scale(col_max(umaxb + mstride * f, ld, col, krow / 64, (krow + K + 63) / 64)) : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < SUB; e += 256) {
-        const int kq = e >> 7, n = e & (TR - 1);     // consecutive threads: consecutive columns
+    // one column and four consecutive k per thread and group (loads coalesced
+    // across the warp's consecutive columns), four groups in flight
+    float4 vr[4], vi[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int e = threadIdx.x + 256 * i;
+        const int n = e & (TR - 1), kq = (e >> 7) * 4;
         const int k = chunk * KC + kq;
         const int col = c0 + tile * TR + n;
-        float vr = 0.f, vi = 0.f;
-        if (col < c1 && k < K) {
-            const size_t o = (size_t)(krow + k) * ld + col;
-            vr = Ar[o] * cscale[n];
-            vi = Ai[o] * cscale[n];
+        float *pr = &vr[i].x, *pi = &vi[i].x;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            pr[j] = pi[j] = 0.f;
+            if (col < c1 && k + j < K) {
+                const size_t o = (size_t)(krow + k + j) * ld + col;
+                pr[j] = Ar[o];
+                pi[j] = Ai[o];
+            }
         }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int e = threadIdx.x + 256 * i;
+        const int n = e & (TR - 1), kq = (e >> 7) * 4;
+        const float sc = cscale[n];
         const uint32_t off = swz(n, kq) >> 1;
-        split_half(vr, t[off], t[SUB + off]);
-        split_half(vi, t[2 * SUB + off], t[3 * SUB + off]);
+        split4(vr[i], sc, t + off, t + SUB + off);
+        split4(vi[i], sc, t + 2 * SUB + off, t + 3 * SUB + off);
     }
     __syncthreads();
     store_planes(t, outb + ostride * f + ((size_t)chunk * 4 * pitch + (size_t)tile * TR) * KC, pitch);
