@@ -227,14 +227,19 @@ __device__ __forceinline__ void store_combo(const MomStore &M, size_t slot, cons
     }
 }
 
+// t2 rows per CTA of the multi-frequency kernel: 32 x 4 pairs in 128 threads,
+// so that two CTAs share an SM (the 64 accumulators of four frequencies allow
+// eight warps) and one's loads and stores overlap the other's arithmetic
+constexpr int MF_RY = 4;
+
 template <int NQ, int F>
-__global__ void __launch_bounds__(256) k_regular_moments_mf(
+__global__ void __launch_bounds__(32 * MF_RY) k_regular_moments_mf(
     int Nt, bool sym, const int2 *__restrict__ tiles, const double4 *__restrict__ origin,
     const double4 *__restrict__ pts, const uint8_t *__restrict__ skip, double kr0, double ki0, double dkr,
     double dki, MomStores ms) {
-    __shared__ double4 sp[8][NQ];
-    __shared__ double4 so[8];
-    __shared__ double4 sd1[32][3], sd2[8][3];
+    __shared__ double4 sp[MF_RY][NQ];
+    __shared__ double4 so[MF_RY];
+    __shared__ double4 sd1[32][3], sd2[MF_RY][3];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     int bx = blockIdx.x, by = blockIdx.y;
     if (tiles) {
@@ -243,19 +248,19 @@ __global__ void __launch_bounds__(256) k_regular_moments_mf(
         by = tl.y;
     }
     const int t1 = bx * 32 + tx;
-    const int t2b = by * 8;
-    if (sym && bx * 32 > t2b + 7) return;  // whole tile below the diagonal
+    const int t2b = by * MF_RY;
+    if (sym && bx * 32 > t2b + MF_RY - 1) return;  // whole tile below the diagonal
     const double4 *tri_d = ms.s[0].tri_d;
-    for (int i = threadIdx.x; i < 8 * NQ; i += blockDim.x) {
+    for (int i = threadIdx.x; i < MF_RY * NQ; i += blockDim.x) {
         int tt = t2b + i / NQ;
         sp[i / NQ][i % NQ] = tt < Nt ? pts[(size_t)tt * NQ + i % NQ] : make_double4(0, 0, 0, 0);
     }
-    if (threadIdx.x < 8) {
+    if (threadIdx.x < MF_RY) {
         int tt = t2b + threadIdx.x;
         so[threadIdx.x] = tt < Nt ? origin[tt] : make_double4(0, 0, 0, 0);
     }
     if (tri_d) {
-        for (int i = threadIdx.x; i < 40 * 3; i += blockDim.x) {
+        for (int i = threadIdx.x; i < (32 + MF_RY) * 3; i += blockDim.x) {
             const int r = i / 3, l = i % 3;
             const int tt = r < 32 ? bx * 32 + r : t2b + (r - 32);
             const double4 v = tt < Nt ? tri_d[3 * (size_t)tt + l] : make_double4(0, 0, 0, 0);
@@ -1182,11 +1187,11 @@ efie_status efie_geom_upload(efie_ctx *ctx, const efie_mesh *mesh, const efie_pr
     }
     g.npairs = g.symmetric ? (size_t)Nt * (Nt + 1) / 2 : (size_t)Nt * Nt;
     if (g.symmetric) {
-        // the 32 x 8 tiles of the regular-pair launches with t1 block <= t2 block
+        // the 32 x MF_RY tiles of the multi-frequency launches with t1 block <= t2 block
         std::vector<int2> tl;
-        const int ntx = (Nt + 31) / 32, nty = (Nt + 7) / 8;
+        const int ntx = (Nt + 31) / 32, nty = (Nt + MF_RY - 1) / MF_RY;
         for (int by = 0; by < nty; by++)
-            for (int bx = 0; bx < ntx && bx * 32 <= by * 8 + 7; bx++) tl.push_back(make_int2(bx, by));
+            for (int bx = 0; bx < ntx && bx * 32 <= by * MF_RY + MF_RY - 1; bx++) tl.push_back(make_int2(bx, by));
         g.n_reg_tiles = (int)tl.size();
         EFIE_TRY(up(g.reg_tiles, tl.data(), sizeof(int2) * tl.size()));
     }
@@ -1224,18 +1229,18 @@ template <int F>
 void launch_regular_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, const MomStores &ms) {
     // symmetric pairs: the tiles on or above the diagonal from the list
     const bool lst = g.symmetric && g.n_reg_tiles > 0;
-    dim3 grid = lst ? dim3((unsigned)g.n_reg_tiles) : dim3((g.Nt + 31) / 32, (g.Nt + 7) / 8);
+    dim3 grid = lst ? dim3((unsigned)g.n_reg_tiles) : dim3((g.Nt + 31) / 32, (g.Nt + MF_RY - 1) / MF_RY);
     const int2 *tiles = lst ? g.reg_tiles.as<int2>() : nullptr;
     const double4 *org = g.origin.as<double4>(), *pts = g.reg_pts.as<double4>();
     const uint8_t *skip = g.near_mask.as<uint8_t>();
     const double dkr = (ph[F - 1].kr - ph[0].kr) / (F - 1), dki = (ph[F - 1].ki - ph[0].ki) / (F - 1);
     switch (g.Nq) {
     case 3:
-        k_regular_moments_mf<3, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
+        k_regular_moments_mf<3, F><<<grid, 32 * MF_RY, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
                                                         dkr, dki, ms);
         break;
     case 7:
-        k_regular_moments_mf<7, F><<<grid, 256, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
+        k_regular_moments_mf<7, F><<<grid, 32 * MF_RY, 0, s>>>(g.Nt, g.symmetric, tiles, org, pts, skip, ph[0].kr, ph[0].ki,
                                                         dkr, dki, ms);
         break;
     }
