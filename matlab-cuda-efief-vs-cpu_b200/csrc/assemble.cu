@@ -230,6 +230,7 @@ __device__ __forceinline__ void store_combo(const MomStore &M, size_t slot, cons
 // t2 rows per CTA of the multi-frequency kernel: 32 x 4 pairs in 128 threads,
 // so that two CTAs share an SM (the 64 accumulators of four frequencies allow
 // eight warps) and one's loads and stores overlap the other's arithmetic
+// (32 x 2 tiles in 64 threads measured the same)
 constexpr int MF_RY = 4;
 
 template <int NQ, int F>
@@ -471,7 +472,9 @@ __global__ void __launch_bounds__(256) k_self_moments(
 // Near and self pairs of F equally spaced frequencies in one launch (the
 // reference scheme's subdivided rules): one warp per pair as in
 // k_near_moments / k_self_moments, each point pair's R, 1/(4 pi R) and phase
-// shared by the F frequencies as in k_regular_moments_mf.
+// shared by the F frequencies as in k_regular_moments_mf.  Two warps per CTA:
+// at up to 252 registers an SM holds eight warps either way, and small CTAs
+// free their slots as soon as their own pairs are done.
 template <int F>
 __device__ __forceinline__ void acc_qpe_mf(double (&m)[F][16], const double4 &pp, const double4 &pq, double R2,
                                            double kr0, double ki0, double dkr, double dki) {
@@ -524,7 +527,7 @@ __device__ __forceinline__ void warp_store_mf(double (&m)[F][16], int lane, cons
 }
 
 template <int F>
-__global__ void __launch_bounds__(256) k_near_moments_mf(
+__global__ void __launch_bounds__(64) k_near_moments_mf(
     int Nt, bool sym, int n_pairs, const int2 *__restrict__ list, int P, const double4 *__restrict__ origin,
     const double4 *__restrict__ pts, const double *__restrict__ aeq, double near_alpha, double kr0, double ki0,
     double dkr, double dki, MomStores ms) {
@@ -554,7 +557,7 @@ __global__ void __launch_bounds__(256) k_near_moments_mf(
 }
 
 template <int F>
-__global__ void __launch_bounds__(256) k_self_moments_mf(int Nt, bool sym, int P, int Nq2,
+__global__ void __launch_bounds__(64) k_self_moments_mf(int Nt, bool sym, int P, int Nq2,
                                                          const double4 *__restrict__ pts,
                                                          const double *__restrict__ self_a, int NsS, double kr0,
                                                          double ki0, double dkr, double dki, MomStores ms) {
@@ -1253,14 +1256,14 @@ void launch_nearself_mf(const GeomDev &g, cudaStream_t s, const Physics *ph, con
     const double4 *org = g.origin.as<double4>();
     if (g.n_near > 0) {
         const int P = g.NsN * g.Nq2;
-        k_near_moments_mf<F><<<(g.n_near + 7) / 8, 256, 0, s>>>(g.Nt, g.symmetric, g.n_near, g.near_list.as<int2>(),
+        k_near_moments_mf<F><<<(g.n_near + 1) / 2, 64, 0, s>>>(g.Nt, g.symmetric, g.n_near, g.near_list.as<int2>(),
                                                                 P, org, g.near_pts.as<double4>(), g.aeq.as<double>(),
                                                                 g.near_alpha, ph[0].kr, ph[0].ki, dkr, dki, ms);
         nl++;
         qpe += (double)g.n_near * P * P;
     }
     const int P = g.NsS * g.Nq2;
-    k_self_moments_mf<F><<<(g.Nt + 7) / 8, 256, 0, s>>>(g.Nt, g.symmetric, P, g.Nq2, g.self_pts.as<double4>(),
+    k_self_moments_mf<F><<<(g.Nt + 1) / 2, 64, 0, s>>>(g.Nt, g.symmetric, P, g.Nq2, g.self_pts.as<double4>(),
                                                         g.self_a.as<double>(), g.NsS, ph[0].kr, ph[0].ki, dkr, dki,
                                                         ms);
     nl++;
