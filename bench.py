@@ -485,12 +485,13 @@ def run_ours(args):
     classes = {k: dict(v) for k, v in plan.stats["classes"].items()}
     plan.close()
 
-    # e2e: the public API call with host arrays (upload + sweep + results) per step
+    # e2e: the public API call with host arrays (upload + sweep + results) per
+    # step, after one untimed call (the first call after the resident plan's
+    # release refills the device pool)
     e2e_ms = []
     h2d = _nbytes(inp["args"]) + B * 8
-    for s in range(max(1, args.steps)):
-        fr = batch(args.warmup + s)
-        t0 = time.perf_counter()
+
+    def e2e_call(fr):
         if args.scheme == "ref":
             m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"],
                                         opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb, tile_chain=tiles[0],
@@ -505,6 +506,12 @@ def run_ours(args):
                              rule_order=RULE[args.scheme])
             p2.run(fr)
             p2.close()
+
+    e2e_call(batch(args.warmup))
+    for s in range(max(1, args.steps)):
+        fr = batch(args.warmup + s)
+        t0 = time.perf_counter()
+        e2e_call(fr)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e = sum(e2e_ms)
     if dist:
@@ -548,7 +555,7 @@ def run_ours(args):
                                 scheme=SCHEME_NAME[args.scheme],
                                 l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
                     e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
-                             d2h_bytes_per_step=2 * 16 * B),
+                             d2h_bytes_per_step=2 * 16 * B, ms_per_step=[round(x, 2) for x in e2e_ms]),
                     gpu_launches=launches, clocks=clk.summary(),
                     accuracy=accuracy, fp64_gpu=fp64,
                     roofline=roofline(classes),
