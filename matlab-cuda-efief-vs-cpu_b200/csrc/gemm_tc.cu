@@ -8,8 +8,9 @@
 // duplicated.  Every operand is split into two FP16 terms after an exact
 // power-of-two scaling: each complex row of L21 by s_i and each column of
 // U12 by t_j so that the largest magnitude of the row (column) over the
-// update's K range lies in [1/2, 1); then x = hi + lo with hi = fp16(x),
-// lo = fp16(x - hi) (22 significant bits).  The three products hi*hi + hi*lo
+// update's K range lies in [2^14, 2^15); then x = hi + lo with hi = fp16(x),
+// lo = fp16(x - hi) (22 significant bits, the lo half a normal FP16 number
+// for entries down to 2^-18 of the maximum).  The three products hi*hi + hi*lo
 // + lo*hi accumulate in FP32 in tensor memory (TMEM, kind::f16, K = 16 per
 // instruction) and the epilogue multiplies by 1/(s_i t_j), which is exact.
 // The update stays close to FP32 accuracy normwise (the LU is then refined in

@@ -14,13 +14,17 @@ __host__ __device__ __forceinline__ uint32_t efie_swz64(uint32_t r, uint32_t k) 
     return r * 64u + ((((k >> 3) ^ (r >> 1)) & 3u) << 4) + ((k & 7u) << 1);
 }
 
-// The split's exact scale 2^-e of a row (column) with largest magnitude mx:
-// mx * 2^-e in [1/2, 1); 1 for a zero maximum.
+// The split's exact scale 2^(15-e) of a row (column) with largest magnitude
+// mx: mx * 2^(15-e) in [2^14, 2^15), the top binade below FP16's largest
+// power of two, so that the lo halves x - fp16(x) of entries down to 2^-18
+// of the maximum are still normal FP16 numbers (with the maximum at 1/2..1
+// they turn subnormal, and lose bits, below 2^-3); 1 for a zero maximum.  The
+// exponent is capped so that the scale stays a finite FP32 power of two.
 __device__ __forceinline__ float efie_pow2_scale(float mx) {
     if (!(mx > 0.f)) return 1.f;
     int e;
     frexpf(mx, &e);
-    return ldexpf(1.f, -e);
+    return ldexpf(1.f, min(15 - e, 126));
 }
 
 struct SolveWork {
