@@ -21,7 +21,7 @@ import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned.json")
-BATCHES = (8, 16, 32)
+BATCHES = (0, 16, 32)    # 0: the library's automatic, balanced batches
 PANELS = (128, 256, 512)
 # (tile_chain, tile_bulk, resident_chain, resident_bulk)
 TILES = ((256, 256, 0, 0), (128, 256, 0, 0), (256, 128, 0, 0), (128, 128, 0, 0), (256, 256, 1, 0),
@@ -59,8 +59,8 @@ def tuned_opts(Ne, sms=None):
 
 def _time(plan_args, freqs, repeats, **kw):
     from .api import SweepPlan, sweep_opts
-    plan = SweepPlan(*plan_args, opts=sweep_opts(**kw))
-    plan.run(freqs[:kw["batch"]])                    # warm-up: workspaces, kernels, graph
+    plan = SweepPlan(*plan_args, opts=sweep_opts(nfreq_hint=len(freqs), **kw))
+    plan.run(freqs)                                  # warm-up: workspaces, kernels, graph
     t0 = time.perf_counter()
     ok = True
     for _ in range(repeats):

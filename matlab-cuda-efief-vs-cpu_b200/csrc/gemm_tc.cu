@@ -70,7 +70,15 @@ struct Tile {
     static constexpr int UH = BN / 2;                           // U columns per CTA
     static constexpr int USUB = UH * KC;                        // halves per U component sub-tile
     static constexpr int STAGE = CHUNK_HALVES + 4 * USUB;       // L chunk + U half chunk
-    static constexpr int NST = BN == 256 ? 3 : 4;               // stages of the ring (192 KB either way)
+    // stages of the ring: 192 KB for BN = 256 (one CTA per SM); 96 KB for
+    // BN = 128, so that two CTAs (pairs) share an SM and one's set-up, drain
+    // and reductions overlap the other's MMAs (2 x 256 TMEM columns)
+    static constexpr int NST = BN == 256 ? 3 : 2;
+    static constexpr int CTAS = BN == 256 ? 1 : 2;              // CTAs per SM
+    // 4 KB reduction tiles per epilogue warp in the freed stages (at most 4)
+    static constexpr int ER = (int)(NST * STAGE * sizeof(__half) / (8 * 4096)) < 4
+                                  ? (int)(NST * STAGE * sizeof(__half) / (8 * 4096))
+                                  : 4;
     static constexpr int NBAR = 3 * NST + 1;                    // full[], empty[], pair_full[], done
     static constexpr int BAR_WORDS = (NBAR + 1 + 1) & ~1;       // + TMEM slot and flag, 16-byte aligned
     static constexpr size_t SMEM = sizeof(__half) * NST * STAGE + 1024 + 8 * BAR_WORDS + sizeof(float) * BN;
@@ -375,7 +383,7 @@ __host__ __device__ __forceinline__ int tri_cols(int p, int nct, int kb, int bn)
 // clusters of two CTAs along x, 256 threads.
 // ---------------------------------------------------------------------------
 template <int BN>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, Tile<BN>::CTAS)
     k_update_tc(const __grid_constant__ CUtensorMap cmap, int N, int r0, int r1, int c0, int c1, int nchunk,
                 const __half *__restrict__ Lpackb, size_t lstride, int lpitch, int loff,
                 const __half *__restrict__ Upackb, size_t ustride, int upitch, int uoff, const float *__restrict__ lmaxb,
@@ -550,16 +558,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
             const int row = rowq + lane;
             const float rs = row < r1 ? 1.f / pow2_scale(row_max(lm, row, nblk, kcol / 64, (kcol + K + 63) / 64)) : 0.f;
             const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(pl * BN);
-            // the stages are free once the MMAs are done: four 4 KB tiles per warp
-            float *ring = reinterpret_cast<float *>(stage) + warp * 4 * 1024;
+            // the stages are free once the MMAs are done: ER 4 KB tiles per warp
+            constexpr int ER = T::ER;
+            float *ring = reinterpret_cast<float *>(stage) + warp * ER * 1024;
             constexpr int NJ = BN / 32;
 #pragma unroll 1
             for (int j = 0; j < NJ && j * 32 < ncol; j++) {
                 uint32_t v[32];
                 tmem_ld32(tbase + j * 32, v);
-                float *tile = ring + (j & 3) * 1024;
-                if (j >= 4) {   // the reduction that read this tile four blocks ago is done with it
-                    if (lane == 0) bulk_wait_read<3>();
+                float *tile = ring + (j % ER) * 1024;
+                if (j >= ER) {   // the reduction that read this tile ER blocks ago is done with it
+                    if (lane == 0) bulk_wait_read<ER - 1>();
                     __syncwarp();
                 }
                 // row `lane` of the tile; 16-byte chunk q sits at chunk q ^ (lane mod 8)
@@ -885,6 +894,7 @@ efie_status efie_tc_attrs() {
                                    (int)Tile<256>::SMEM));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)Tile<128>::SMEM));
+    EFIE_CUDA(cudaFuncSetAttribute(k_update_tc<128>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     EFIE_CUDA(cudaFuncSetAttribute(k_update_tc_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     done = true;
     return EFIE_OK;
