@@ -59,7 +59,13 @@ def tuned_opts(Ne, sms=None):
 
 def _time(plan_args, freqs, repeats, **kw):
     from .api import SweepPlan, sweep_opts
-    plan = SweepPlan(*plan_args, opts=sweep_opts(nfreq_hint=len(freqs), **kw))
+    from . import _native
+    try:
+        plan = SweepPlan(*plan_args, opts=sweep_opts(nfreq_hint=len(freqs), **kw))
+    except _native.MexError as e:
+        if e.identifier != "efie:nomem":
+            raise
+        return len(plan_args[2]), None   # a batch too large for this GPU: no candidate
     plan.run(freqs)                                  # warm-up: workspaces, kernels, graph
     t0 = time.perf_counter()
     ok = True
