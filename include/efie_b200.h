@@ -185,6 +185,12 @@ typedef struct efie_sweep_opts {
                                 with batch = 0, the automatic batch is cut to the
                                 balanced size for that many; efie_patch_sweep_fastquad
                                 sets it to Nf                                   */
+    int32_t share_factors;   /* 1 (default): with the mixed solver's coarse-to-fine
+                                batches, every second batch is not factored: each of
+                                its frequencies is refined (GMRES, same residual
+                                target) with the complex64 factors of the nearest
+                                frequency of the batch before it, which stay in the
+                                plan's slots; 0: every frequency is factored */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */
@@ -218,6 +224,7 @@ typedef struct efie_sweep_stats {
     int32_t n_wait_timeouts;    /* frequencies whose bounded device wait gave up (then
                                    re-solved by the complex128 LU)                */
     int32_t n_zero_pivots;      /* frequencies whose complex64 LU met a zero pivot */
+    int32_t n_shared_factors;   /* frequencies refined with a neighbour's factors  */
 } efie_sweep_stats;
 
 /* Replaces patch_sweep_fastquad_cuda.cu:461-844 (mexFunction):

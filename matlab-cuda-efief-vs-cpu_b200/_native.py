@@ -46,7 +46,7 @@ class EfieSweepOpts(C.Structure):
                 ("lu_nb", C.c_int32), ("timing", C.c_int32), ("batch", C.c_int32),
                 ("refine_method", C.c_int32), ("graphs", C.c_int32), ("tile_chain", C.c_int32),
                 ("tile_bulk", C.c_int32), ("resident_chain", C.c_int32), ("resident_bulk", C.c_int32),
-                ("nfreq_hint", C.c_int32)]
+                ("nfreq_hint", C.c_int32), ("share_factors", C.c_int32)]
 
 
 KERNEL_CLASSES = ("quad", "nearself", "gather", "gemm", "panel", "trsv", "residual", "other")
@@ -58,7 +58,8 @@ class EfieSweepStats(C.Structure):
                 ("ms_assemble", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
                 ("n_launches", C.c_int32),
                 ("class_launches", C.c_int32 * 8), ("class_ms", C.c_double * 8), ("class_work", C.c_double * 8),
-                ("n_wait_timeouts", C.c_int32), ("n_zero_pivots", C.c_int32)]
+                ("n_wait_timeouts", C.c_int32), ("n_zero_pivots", C.c_int32),
+                ("n_shared_factors", C.c_int32)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("class_")}

@@ -73,6 +73,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->resident_chain = 0;
     o->resident_bulk = 0;
     o->nfreq_hint = 0;
+    o->share_factors = 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -755,10 +756,32 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     }
     if (warm) EFIE_TRY(p->xall.reserve(sizeof(efie_c128) * (size_t)N * Nf));
     auto Zslot = [&](int f) -> void * { return p->Z.as<efie_c128>() + NN * f; };
+    // Shared factors: with coarse-to-fine batches every second batch is not
+    // factored.  Its frequencies lie between those of the batch before it,
+    // whose complex64 factors are still in the plan's slots; each is refined
+    // with the factors of the nearest of them (its assembly then leaves the
+    // planes alone).  GMRES converges to the same residual target in a few
+    // more steps; a frequency that does not gets the retry below, with its
+    // own factors.
+    const bool share = mixed && warm && p->opts.share_factors != 0 && p->sw.zsym && p->sw.sym_lu &&
+                       p->opts.refine_method == EFIE_REFINE_GMRES;
+    bool prev_factored = false;      // the batch before this one was factored into the slots
+    bool fsrc_identity = true;       // p->sw.fsrc maps every slot to itself
+    std::vector<int> fsrc_host(p->B);
+    auto set_fsrc = [&](bool identity) -> efie_status {
+        if (identity && fsrc_identity) return EFIE_OK;
+        if (identity)
+            for (int f = 0; f < p->B; f++) fsrc_host[f] = f;
+        EFIE_CUDA(cudaMemcpyAsync(p->sw.fsrc.p, fsrc_host.data(), sizeof(int) * p->B, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        fsrc_identity = identity;
+        return EFIE_OK;
+    };
     for (int bi = 0; bi < nbat && rc == EFIE_OK; bi++) {
         const int f0 = bstart[bi], nb = bstart[bi + 1] - f0;
         int active[EFIE_MAX_BATCH] = {0};
         for (int f = 0; f < nb; f++) active[f] = 1;
+        const bool shared = share && (bi & 1) && prev_factored;
         {
             Physics ph[EFIE_MAX_BATCH];
             void *Zf[EFIE_MAX_BATCH];
@@ -771,14 +794,34 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                     rc = efie_assemble_centroid_device(ctx, &p->cmesh, p->self_alpha, ph[f], Zf[f], p->scratch);
             } else {
                 const PlanesOut po{p->sw.planes.as<float>(), p->sw.pstride, p->sw.ld};
-                rc = efie_assemble_batch(ctx, p->g, ph, nb, Zf, p->sw.planes_from_assembly ? &po : nullptr);
+                rc = efie_assemble_batch(ctx, p->g, ph, nb, Zf,
+                                         p->sw.planes_from_assembly && !shared ? &po : nullptr);
             }
         }
         if (rc != EFIE_OK) break;
         bool fallback[EFIE_MAX_BATCH] = {false};
         if (mixed) {
-            rc = plan_factor(p, active, nb);
+            if (shared) {
+                // each slot refines with the factors of the previous batch's
+                // slot holding the nearest frequency
+                const int p0 = bstart[bi - 1], np_ = f0 - p0;
+                for (int f = 0; f < p->B; f++) fsrc_host[f] = f;
+                for (int f = 0; f < nb; f++) {
+                    int best = 0;
+                    for (int s2 = 1; s2 < np_; s2++)
+                        if (std::abs(posq[p0 + s2] - posq[f0 + f]) < std::abs(posq[p0 + best] - posq[f0 + f]))
+                            best = s2;
+                    fsrc_host[f] = best;
+                }
+                rc = set_fsrc(false);
+                if (rc == EFIE_OK) rc = efie_mixed_factor_prepare(ctx, p->sw, active);
+                S->n_shared_factors += nb;
+            } else {
+                rc = set_fsrc(true);
+                if (rc == EFIE_OK) rc = plan_factor(p, active, nb);
+            }
             if (rc != EFIE_OK) break;
+            prev_factored = !shared;
             RefineResult rr;
             const bool guess = warm && bi > 0;
             if (guess) {
@@ -811,6 +854,9 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 if (nr > 0) {
                     RefineResult r2;
                     const bool pfa = p->sw.planes_from_assembly;
+                    // the retried frequencies refine with their own factors
+                    rc = set_fsrc(true);
+                    if (rc != EFIE_OK) break;
                     // the general LU converts all of Z
                     for (int f = 0; f < nb && rc == EFIE_OK; f++)
                         if (retry[f] && pfa) rc = efie_z_mirror(ctx, Zslot(f), N);

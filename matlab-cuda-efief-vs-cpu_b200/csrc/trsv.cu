@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
                                                  const float2 *__restrict__ dinv, size_t dstride,
                                                  const float2 *__restrict__ rhsb, float2 *outb, int vstride,
                                                  double2 *__restrict__ xb, unsigned long long *prog, int epoch,
-                                                 char *ctl, const int *__restrict__ active) {
+                                                 char *ctl, const int *__restrict__ active,
+                                                 const int *__restrict__ fsrc) {
     extern __shared__ unsigned char dsm[];
     __shared__ float2 acc[NB];
     __shared__ float2 part[4][NB];
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
     int p_it = blockIdx.x, p_q = 0, issued = 0;
     auto produce = [&]() {
         if (p_it >= items) return;
-        const int o = p_it / B, f = p_it - o * B, b = LOWER ? o : nblk - 1 - o;
+        const int o = p_it / B, b = LOWER ? o : nblk - 1 - o;
+        const int f = fsrc[p_it - o * B];   // the slot whose factors precondition this frequency
         unsigned char *st = ring + (issued % TS) * STAGE_BYTES;
         uint64_t *bar = full + issued % TS;
         mbar_expect_tx(bar, STAGE_BYTES);
@@ -338,9 +340,11 @@ efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs
     unsigned long long *prog = w.prog.as<unsigned long long>();
     char *ctl = w.ctl.as<char>();
     const int *active = w.active.as<int>();
+    const int *fsrc = w.fsrc.as<int>();
     void *args[] = {(void *)w.planes_map, (void *)&w.N,   (void *)&w.nblk,    (void *)&w.B,  (void *)&dinv,
                     (void *)&w.dstride,   (void *)&rhs,   (void *)&out,       (void *)&w.vstride,
-                    (void *)&xd,          (void *)&prog,  (void *)&epoch,     (void *)&ctl,  (void *)&active};
+                    (void *)&xd,          (void *)&prog,  (void *)&epoch,     (void *)&ctl,  (void *)&active,
+                    (void *)&fsrc};
     const void *fn = lower ? (const void *)k_trsv<true> : (const void *)k_trsv<false>;
     EFIE_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(256), args, TRSV_SMEM, ctx->stream));
     return EFIE_OK;
