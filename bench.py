@@ -436,7 +436,8 @@ def run_ours(args):
                 args.resident_bulk if args.resident_bulk >= 0 else (tuned[5] if tuned else 0))
     opts = m.sweep_opts(solver=args.solver, timing=False, scheme=args.scheme,
                         batch=B if B < 8 else 0, lu_nb=args.lu_nb, tile_chain=tiles[0], tile_bulk=tiles[1],
-                        resident_chain=resident[0], resident_bulk=resident[1], nfreq_hint=B)
+                        resident_chain=resident[0], resident_bulk=resident[1], nfreq_hint=B,
+                        share_factors=args.share_factors)
     pargs = list(inp["args"])
     if args.scheme == "extract":
         pargs[-1] = None   # no prepack: the rule points come from the mesh
@@ -457,6 +458,7 @@ def run_ours(args):
     fallback = 0
     relres = 0.0
     iters = 0
+    shared = 0
     with ClockSampler(local) as clk:
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
@@ -469,6 +471,7 @@ def run_ours(args):
             fallback += st["n_fp64_fallback"]
             relres = max(relres, st["max_relres"])
             iters = max(iters, st["refine_iters_max"])
+            shared += st["n_shared_factors"]
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
@@ -496,13 +499,15 @@ def run_ours(args):
             m.patch_sweep_fastquad_cuda(*inp["args"], fr, *inp["tail"],
                                         opts=m.sweep_opts(solver=args.solver, lu_nb=args.lu_nb, tile_chain=tiles[0],
                                                           tile_bulk=tiles[1], resident_chain=resident[0],
-                                                          resident_bulk=resident[1]))
+                                                          resident_bulk=resident[1],
+                                                          share_factors=args.share_factors))
         else:
             # plan create (host mesh upload) + run + destroy through the C ABI
             p2 = m.SweepPlan(*pargs, *inp["tail"],
                              opts=m.sweep_opts(solver=args.solver, scheme="extract", lu_nb=args.lu_nb,
                                                tile_chain=tiles[0], tile_bulk=tiles[1], resident_chain=resident[0],
-                                               resident_bulk=resident[1], nfreq_hint=B),
+                                               resident_bulk=resident[1], nfreq_hint=B,
+                                               share_factors=args.share_factors),
                              rule_order=RULE[args.scheme])
             p2.run(fr)
             p2.close()
@@ -523,7 +528,8 @@ def run_ours(args):
     # the metric's FP64 arm: the plain FP64 GPU path on the same points, and
     # the Zin error of every point of the last timed step against it
     fp64 = None
-    accuracy = dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback)
+    accuracy = dict(max_relres=relres, refine_iters_max=iters, fp64_fallbacks=fallback,
+                    points_on_shared_factors=shared, points_timed=args.steps * B)
     if args.solver == "mixed" and not args.no_fp64_arm:
         v64, Z64 = fp64_arm(m, pargs, inp["tail"], fr_last, stream, scheme=args.scheme)
         fp64 = dict(value=v64, unit="freq points/s", points=len(fr_last),
@@ -553,6 +559,7 @@ def run_ours(args):
                                          % ("128 resident" if resident[0] else tiles[0] or 256,
                                             "128 resident" if resident[1] else tiles[1] or 256),
                                 scheme=SCHEME_NAME[args.scheme],
+                                share_factors=(args.share_factors or "auto") if args.solver == "mixed" else 1,
                                 l2="working set per step > L2 (Z c128 %.0f MB)" % (16e-6 * inp["Ne"] ** 2)),
                     e2e=dict(value=e2e_value, unit="freq points/s", h2d_bytes_per_step=h2d,
                              d2h_bytes_per_step=2 * 16 * B, ms_per_step=[round(x, 2) for x in e2e_ms]),
@@ -560,6 +567,7 @@ def run_ours(args):
                     accuracy=accuracy, fp64_gpu=fp64,
                     roofline=roofline(classes),
                     roofline_assembly=roofline(classes, "quad", fp64_peak),
+                    roofline_tensor=roofline(classes, "gemm"),
                     # the HBM-bound classes: algorithmic bytes over their event time
                     roofline_hbm={k: roofline(classes, k) for k in ("trsv", "residual", "gather")},
                     phases_ms_per_point={k: v["ms"] / B for k, v in classes.items()},
@@ -776,6 +784,10 @@ def main():
                     help="tensor-core tile width of the outer panels' updates (0: the autotuner's table)")
     ap.add_argument("--resident-chain", type=int, default=-1, choices=[-1, 0, 1],
                     help="1: the LU's K = 64 updates on resident, pipelined CTA pairs (-1: the autotuner's table)")
+    ap.add_argument("--share-factors", type=int, default=0,
+                    help="mixed solver: factor only the first of each group of this many coarse-to-fine batches; "
+                         "the others refine with their nearest neighbours' factors (1: factor every frequency, "
+                         "0: the library's automatic choice)")
     ap.add_argument("--resident-bulk", type=int, default=-1, choices=[-1, 0, 1],
                     help="1: the LU's outer-panel updates on resident, pipelined CTA pairs (-1: the autotuner's "
                          "table)")

@@ -185,12 +185,15 @@ typedef struct efie_sweep_opts {
                                 with batch = 0, the automatic batch is cut to the
                                 balanced size for that many; efie_patch_sweep_fastquad
                                 sets it to Nf                                   */
-    int32_t share_factors;   /* 1 (default): with the mixed solver's coarse-to-fine
-                                batches, every second batch is not factored: each of
-                                its frequencies is refined (GMRES, same residual
-                                target) with the complex64 factors of the nearest
-                                frequency of the batch before it, which stay in the
-                                plan's slots; 0: every frequency is factored */
+    int32_t share_factors;   /* g >= 2: with the mixed solver's coarse-to-fine
+                                batches, only the first batch of each group of g is
+                                factored; every frequency of the others is refined
+                                (GMRES, same residual target) with the complex64
+                                factors of the nearest frequency of that batch, which
+                                stay in the plan's slots, and the automatic batch
+                                size gives a sweep at least g batches.  1: every
+                                frequency is factored.  0 (default): automatic,
+                                g ~ Ne / 1200 within [2, 8] */
 } efie_sweep_opts;
 
 /* Fill `o` with the defaults listed above. */

@@ -291,12 +291,14 @@ def assemble_ZV_EFIE_RWG_DIFF_GPU_FAST(*args, nargout=2):
 # ---------------------------------------------------------------------------
 def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-10, refine_max_iter=30,
                timing=False, batch=0, lu_nb=0, refine="gmres", graphs=True, tile_chain=0, tile_bulk=0,
-               resident_chain=0, resident_bulk=0, nfreq_hint=0, share_factors=True):
+               resident_chain=0, resident_bulk=0, nfreq_hint=0, share_factors=0):
     """efie_sweep_opts: solver 'mixed'|'fp64', port_model 'gauss'|'edge',
     scheme 'ref'|'extract', refine 'gmres'|'classical' (mixed solver only),
     tile_chain / tile_bulk: tensor-core tile widths 128 | 256 (0 = tuned),
-    share_factors: every second coarse-to-fine batch refines with the factors
-    of its neighbours in the batch before it instead of factoring."""
+    share_factors: g >= 2 factors only the first of each group of g
+    coarse-to-fine batches, the others refine with the factors of their
+    nearest neighbours in it; 1: every frequency is factored; 0: automatic
+    (g ~ Ne / 1200 within [2, 8])."""
     o = nat.EfieSweepOpts()
     nat.lib().efie_sweep_opts_default(C.byref(o))
     o.solver = {"fp64": nat.SOLVER_FP64, "mixed": nat.SOLVER_MIXED}[solver]
@@ -314,7 +316,7 @@ def sweep_opts(solver="mixed", port_model="gauss", scheme="ref", refine_tol=1e-1
     o.resident_chain = int(resident_chain)
     o.resident_bulk = int(resident_bulk)
     o.nfreq_hint = int(nfreq_hint)
-    o.share_factors = 1 if share_factors else 0
+    o.share_factors = int(share_factors)
     return o
 
 

@@ -73,7 +73,7 @@ extern "C" void efie_sweep_opts_default(efie_sweep_opts *o) {
     o->resident_chain = 0;
     o->resident_bulk = 0;
     o->nfreq_hint = 0;
-    o->share_factors = 1;
+    o->share_factors = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -401,6 +401,7 @@ struct efie_plan {
     double self_alpha = 0.20;
     int Ne = 0;
     int B = 1;                   // frequencies per batch
+    int share_group = 1;         // batches per factored batch (1: every frequency factored)
     double mu = 0, V0 = 0, Z0 = 0;
     efie_c128 eps{0, 0};
     int pe = 0, ge = 0;
@@ -510,7 +511,21 @@ efie_status plan_solve_fp64(efie_plan *p, int slot, int fi) {
 // smaller batches give more warm-started GMRES runs).  With the number of
 // frequencies a sweep will solve (nf > 0), the slots are cut to the balanced
 // batch size of that many batches: no slot stays idle.
-int choose_batch(int N, int requested, int solver, int nf) {
+// Batches per factored batch with shared factors: the caller's g >= 2, 1 for
+// none, else (0) automatic.  A factorization costs O(N^3) and the GMRES steps
+// it saves O(N^2) each, so larger problems share each factorization among
+// more frequencies: measured on one B200, 6 is best at N 6968 (347 against
+// 333 for 4 and 323 for 8 points/s) and 8 at N 19936 (36.2 against 29.3
+// for 4), so g ~ N / 1200 within [2, 8].
+int choose_share_group(int N, int requested) {
+    if (requested == 1) return 1;
+    if (requested >= 2) return std::min(requested, 16);
+    return std::max(2, std::min(8, (int)std::lround(N / 1200.0)));
+}
+
+// group: batches per factored batch with shared factors (> 1): a sweep of nf
+// frequencies then has at least that many batches
+int choose_batch(int N, int requested, int solver, int nf, int group = 1) {
     if (solver == EFIE_SOLVER_FP64) return 1;
     if (requested > 0) return std::min(requested, EFIE_MAX_BATCH);
     size_t freeb = 0, total = 0;
@@ -522,7 +537,7 @@ int choose_batch(int N, int requested, int solver, int nf) {
     int B = (int)std::floor(0.45 * (double)freeb / per);
     B = std::max(1, std::min(B, N >= 4096 ? EFIE_MAX_BATCH : 32));
     if (nf > 0) {
-        const int nbat = (nf + B - 1) / B;
+        const int nbat = std::max((nf + B - 1) / B, std::min(std::max(group, 1), nf));
         B = (nf + nbat - 1) / nbat;
     }
     return B;
@@ -569,7 +584,10 @@ efie_status plan_common(efie_plan *p, const efie_mesh *mesh, double mu, efie_c12
         bn += rhs[e] * rhs[e];
     }
     p->bnorm = std::sqrt(bn);
-    p->B = choose_batch(N, p->opts.batch, p->opts.solver, p->opts.nfreq_hint);
+    p->share_group = p->opts.solver == EFIE_SOLVER_MIXED && p->opts.refine_method == EFIE_REFINE_GMRES
+                         ? choose_share_group(N, p->opts.share_factors)
+                         : 1;
+    p->B = choose_batch(N, p->opts.batch, p->opts.solver, p->opts.nfreq_hint, p->share_group);
     EFIE_TRY(p->Z.reserve(sizeof(efie_c128) * (size_t)N * N * p->B));
     EFIE_TRY(p->b.reserve(sizeof(efie_c128) * N));
     EFIE_TRY(p->x.reserve(sizeof(efie_c128) * (size_t)N * p->B));
@@ -763,25 +781,24 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     // planes alone).  GMRES converges to the same residual target in a few
     // more steps; a frequency that does not gets the retry below, with its
     // own factors.
-    const bool share = mixed && warm && p->opts.share_factors != 0 && p->sw.zsym && p->sw.sym_lu &&
+    const int group = p->share_group;   // batches per factored batch
+    const bool share = mixed && warm && group > 1 && p->sw.zsym && p->sw.sym_lu &&
                        p->opts.refine_method == EFIE_REFINE_GMRES;
-    bool prev_factored = false;      // the batch before this one was factored into the slots
-    bool fsrc_identity = true;       // p->sw.fsrc maps every slot to itself
+    bool prev_factored = false;      // the group's first batch was factored into the slots
     std::vector<int> fsrc_host(p->B);
+    p->sw.fsrc_on = false;
     auto set_fsrc = [&](bool identity) -> efie_status {
-        if (identity && fsrc_identity) return EFIE_OK;
-        if (identity)
-            for (int f = 0; f < p->B; f++) fsrc_host[f] = f;
+        p->sw.fsrc_on = !identity;
+        if (identity) return EFIE_OK;
         EFIE_CUDA(cudaMemcpyAsync(p->sw.fsrc.p, fsrc_host.data(), sizeof(int) * p->B, cudaMemcpyHostToDevice,
                                   ctx->stream));
-        fsrc_identity = identity;
         return EFIE_OK;
     };
     for (int bi = 0; bi < nbat && rc == EFIE_OK; bi++) {
         const int f0 = bstart[bi], nb = bstart[bi + 1] - f0;
         int active[EFIE_MAX_BATCH] = {0};
         for (int f = 0; f < nb; f++) active[f] = 1;
-        const bool shared = share && (bi & 1) && prev_factored;
+        const bool shared = share && (bi % group) != 0 && prev_factored;
         {
             Physics ph[EFIE_MAX_BATCH];
             void *Zf[EFIE_MAX_BATCH];
@@ -802,9 +819,9 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
         bool fallback[EFIE_MAX_BATCH] = {false};
         if (mixed) {
             if (shared) {
-                // each slot refines with the factors of the previous batch's
-                // slot holding the nearest frequency
-                const int p0 = bstart[bi - 1], np_ = f0 - p0;
+                // each slot refines with the factors of the group's factored
+                // batch's slot holding the nearest frequency
+                const int gb = bi - bi % group, p0 = bstart[gb], np_ = bstart[gb + 1] - p0;
                 for (int f = 0; f < p->B; f++) fsrc_host[f] = f;
                 for (int f = 0; f < nb; f++) {
                     int best = 0;
@@ -821,7 +838,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 if (rc == EFIE_OK) rc = plan_factor(p, active, nb);
             }
             if (rc != EFIE_OK) break;
-            prev_factored = !shared;
+            if (!shared) prev_factored = true;
             RefineResult rr;
             const bool guess = warm && bi > 0;
             if (guess) {

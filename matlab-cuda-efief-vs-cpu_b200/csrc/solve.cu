@@ -869,12 +869,8 @@ efie_status efie_mixed_workspace(SolveWork &w, int N, int B, int kb_outer) {
     EFIE_TRY(w.lmax.reserve(sizeof(float) * w.mstride * B));
     EFIE_TRY(w.umax.reserve(sizeof(float) * w.mstride * B));
     EFIE_TRY(w.active.reserve(sizeof(int) * B));
-    {
-        std::vector<int> ident(B);
-        for (int f = 0; f < B; f++) ident[f] = f;
-        EFIE_TRY(w.fsrc.reserve(sizeof(int) * B));
-        EFIE_CUDA(cudaMemcpy(w.fsrc.p, ident.data(), sizeof(int) * B, cudaMemcpyHostToDevice));
-    }
+    EFIE_TRY(w.fsrc.reserve(sizeof(int) * B));
+    w.fsrc_on = false;
     EFIE_TRY(efie_trsv_workspace(w));
     EFIE_TRY(efie_gemm_workspace(w));
     if (!w.hi) {

@@ -48,9 +48,11 @@ struct SolveWork {
     DevBuf rpart;    // residual-norm partial sums: double [B][ceil(N/32)]
     DevBuf active;   // int[B]: slot holds a frequency of this batch
     // int[B]: the slot whose complex64 factors (planes, dinv) precondition
-    // slot f's refinement -- f itself, or, in a batch that shares the factors
-    // of the batch before it, the slot of the nearest factored frequency
+    // slot f's refinement in a batch that shares the factors of an earlier
+    // batch (the slot of the nearest factored frequency); read only while
+    // fsrc_on, else every slot uses its own factors
     DevBuf fsrc;
+    bool fsrc_on = false;
     // tensor-core operands, FP16 hi/lo packed once per panel (see PackView):
     // the outer panel's L and U by parity of the panel (packL[2], packU[2]),
     // the 64-wide block of the panel chain written by the panel kernel (ipL, ipU)

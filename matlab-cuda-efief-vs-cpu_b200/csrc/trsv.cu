@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
     auto produce = [&]() {
         if (p_it >= items) return;
         const int o = p_it / B, b = LOWER ? o : nblk - 1 - o;
-        const int f = fsrc[p_it - o * B];   // the slot whose factors precondition this frequency
+        const int f = fsrc ? fsrc[p_it - o * B] : p_it - o * B;   // the slot whose factors precondition it
         unsigned char *st = ring + (issued % TS) * STAGE_BYTES;
         uint64_t *bar = full + issued % TS;
         mbar_expect_tx(bar, STAGE_BYTES);
@@ -340,7 +340,7 @@ efie_status efie_trsv(efie_ctx *ctx, SolveWork &w, bool lower, const float2 *rhs
     unsigned long long *prog = w.prog.as<unsigned long long>();
     char *ctl = w.ctl.as<char>();
     const int *active = w.active.as<int>();
-    const int *fsrc = w.fsrc.as<int>();
+    const int *fsrc = w.fsrc_on ? w.fsrc.as<int>() : nullptr;
     void *args[] = {(void *)w.planes_map, (void *)&w.N,   (void *)&w.nblk,    (void *)&w.B,  (void *)&dinv,
                     (void *)&w.dstride,   (void *)&rhs,   (void *)&out,       (void *)&w.vstride,
                     (void *)&xd,          (void *)&prog,  (void *)&epoch,     (void *)&ctl,  (void *)&active,

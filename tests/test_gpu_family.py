@@ -25,7 +25,7 @@ def test_concurrent_family_sweep_matches_designs_swept_alone():
         for f in ("edge", "plusTri", "minusTri", "plusSign", "minusSign", "rp", "rm", "Ap", "Am", "len"):
             assert np.array_equal(xh["rwg"][f], xd["rwg"][f]), f
         assert (xh["pe"], xh["ge"]) == (xd["pe"], xd["ge"])
-        plan = sur.design_plan(d, inputs=xh)
+        plan = sur.design_plan(d, inputs=xh, nfreq=nf)   # the same batches as in the family
         Z1, _ = plan.run(d.band(nf))
         plan.close()
         assert np.array_equal(Zin, Z1)
