@@ -274,3 +274,41 @@ def test_repeated_frequencies_in_warm_started_sweep():
     assert (np.abs(Zin - Zo) / np.abs(Zo)).max() <= 1e-6
     assert abs(Zin[1] - Zin[2]) <= 1e-7 * abs(Zin[1]) and abs(Zin[4] - Zin[5]) <= 1e-7 * abs(Zin[4])
     assert st["n_fp64_fallback"] == 0
+
+
+@pytest.mark.parametrize("group", [2, 4])
+def test_shared_factors_match_every_frequency_factored(group):
+    """With shared factors only the first of each group of coarse-to-fine
+    batches is factored; the other frequencies refine with the complex64
+    factors of their nearest factored neighbour.  GMRES reaches the same
+    residual target, so Zin agrees with the sweep that factors every
+    frequency and with the oracle, every solved current meets the residual
+    target, and the stats count the frequencies that shared factors."""
+    m = pkg()
+    d = config1_design("grid")
+    p = eo.build_problem(d)
+    r = p["rwg"]
+    args = [p["V"], p["F"], r["edge"], r["plusTri"], r["minusTri"], r["plusSign"], r["minusSign"], r["rp"], r["rm"],
+            r["Ap"], r["Am"], r["len"], p["prepack"], d.mu, d.eps, p["patchEdge"], p["groundEdge"], d.V0, p["spread"],
+            d.Z0]
+    freqs = np.linspace(d.freqs[0], d.freqs[-1], 17)
+    full = m.SweepPlan(*args, opts=m.sweep_opts(share_factors=1, nfreq_hint=len(freqs)))
+    Zf, _ = full.run(freqs)
+    assert full.stats["n_shared_factors"] == 0
+    full.close()
+    plan = m.SweepPlan(*args, opts=m.sweep_opts(share_factors=group, nfreq_hint=len(freqs)))
+    Zs, _, Is = plan.run(freqs, return_currents=True)
+    st = plan.stats
+    plan.close()
+    # `group` balanced batches, one group: every frequency outside the first
+    # batch (sorted positions 0, g, 2g, ...) shares its factors
+    assert st["n_shared_factors"] == len(freqs) - -(-len(freqs) // group)
+    assert st["n_fp64_fallback"] == 0
+    assert st["max_relres"] <= 1e-10
+    assert (np.abs(Zs - Zf) / np.abs(Zf)).max() <= 1e-7
+    Zo, _ = _oracle(p, freqs)
+    assert (np.abs(Zs - Zo) / np.abs(Zo)).max() <= 1e-6
+    for j in (1, 8, 15):
+        omega, k, _, _ = eo.physics(freqs[j], d.mu, d.eps)
+        Z = oc.assemble_z(r, p["prepack"], k, omega, d.mu, d.eps)
+        assert np.linalg.norm(p["b"] - Z @ Is[:, j]) / np.linalg.norm(p["b"]) < 1e-9
