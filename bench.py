@@ -358,8 +358,8 @@ def fp64_arm(m, pargs, tail, freqs, stream, scheme="ref"):
 
 
 def secondary_block(m, stream):
-    """cfg2 with the BASELINE quadrature (Dunavant 7-point rule + analytic
-    extraction) on all 101 points, and cfg5 (Ne 19936) on 8 points: points/s
+    """cfg2 with the benchmark configuration's own quadrature (Dunavant 7-point
+    rule + analytic extraction) on all 101 points, and cfg5 (Ne 19936) on 8 points: points/s
     of the mixed solver and Zin error against the FP64 GPU path."""
     out = {}
     inp = build_inputs(m, "cfg2")

@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(256, 2) k_trsv(const __grid_constant__ CUtenso
     }
     __syncthreads();
     int cc = 0;   // pieces consumed
-    // wait for the next piece (every thread), then a CTA-wide verdict
+    // wait for the next piece (every thread); the CTA decides together after its barrier
     auto take = [&]() -> const unsigned char * {
         if (!mbar_wait_bounded(full + cc % TS, (uint32_t)(cc / TS) & 1u)) fail = 1;
         return ring + (cc % TS) * STAGE_BYTES;
