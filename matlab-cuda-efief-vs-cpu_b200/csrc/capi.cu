@@ -774,17 +774,18 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
     }
     if (warm) EFIE_TRY(p->xall.reserve(sizeof(efie_c128) * (size_t)N * Nf));
     auto Zslot = [&](int f) -> void * { return p->Z.as<efie_c128>() + NN * f; };
-    // Shared factors: with coarse-to-fine batches every second batch is not
-    // factored.  Its frequencies lie between those of the batch before it,
-    // whose complex64 factors are still in the plan's slots; each is refined
-    // with the factors of the nearest of them (its assembly then leaves the
-    // planes alone).  GMRES converges to the same residual target in a few
-    // more steps; a frequency that does not gets the retry below, with its
-    // own factors.
+    // Shared factors: with coarse-to-fine batches only the first batch of each
+    // group of `group` is factored.  The frequencies of the group's other
+    // batches lie between its frequencies, whose complex64 factors stay in
+    // the plan's slots; each is refined with the factors of the nearest of
+    // them (its assembly then leaves the planes alone).  GMRES converges to
+    // the same residual target in a few more steps; a frequency that does
+    // not gets the retry below, with its own factors -- which converts Z to
+    // planes in every slot, so the rest of the group then factors itself.
     const int group = p->share_group;   // batches per factored batch
     const bool share = mixed && warm && group > 1 && p->sw.zsym && p->sw.sym_lu &&
                        p->opts.refine_method == EFIE_REFINE_GMRES;
-    bool prev_factored = false;      // the group's first batch was factored into the slots
+    bool prev_factored = false;      // the slots hold the factors of the group's first batch
     std::vector<int> fsrc_host(p->B);
     p->sw.fsrc_on = false;
     auto set_fsrc = [&](bool identity) -> efie_status {
@@ -838,7 +839,7 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 if (rc == EFIE_OK) rc = plan_factor(p, active, nb);
             }
             if (rc != EFIE_OK) break;
-            if (!shared) prev_factored = true;
+            if (!shared && bi % group == 0) prev_factored = true;
             RefineResult rr;
             const bool guess = warm && bi > 0;
             if (guess) {
@@ -871,9 +872,11 @@ extern "C" efie_status efie_plan_run(efie_plan *p, const double *freqs, int32_t 
                 if (nr > 0) {
                     RefineResult r2;
                     const bool pfa = p->sw.planes_from_assembly;
-                    // the retried frequencies refine with their own factors
+                    // the retried frequencies refine with their own factors;
+                    // the slots no longer hold the group's factors
                     rc = set_fsrc(true);
                     if (rc != EFIE_OK) break;
+                    prev_factored = false;
                     // the general LU converts all of Z
                     for (int f = 0; f < nb && rc == EFIE_OK; f++)
                         if (retry[f] && pfa) rc = efie_z_mirror(ctx, Zslot(f), N);
