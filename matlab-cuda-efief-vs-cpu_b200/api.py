@@ -421,7 +421,7 @@ class SweepPlan:
             from .autotune import tuned_opts
             t = tuned_opts(Ne)
             opts = (sweep_opts(batch=t[0], lu_nb=t[1], tile_chain=t[2], tile_bulk=t[3], resident_chain=t[4],
-                               resident_bulk=t[5]) if t else sweep_opts())
+                               resident_bulk=t[5], share_factors=t[6]) if t else sweep_opts())
         self.opts = opts
         h = C.c_void_p()
         cx = ctx if ctx is not None else nat.context()

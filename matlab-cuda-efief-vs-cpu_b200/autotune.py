@@ -3,10 +3,10 @@ and the tensor-core tile widths of the LU's trailing updates.
 
 For a given geometry it times short sweeps over the candidate settings and
 keeps the fastest whose refinement still converges (no FP64 fallback): first
-(batch, panel width) with 256-column tiles, then the four tile-width pairs
+(batch, panel width) with 256-column tiles, then the tile-width pairs
 (128 or 256 complex columns per CTA pair, for the panel chain's K = 64
-updates and for the outer panels' updates) at the winning batch and panel
-width.  The winners are cached in ``tuned.json`` next to this file, keyed by
+updates and for the outer panels' updates) and resident variants at the
+winning batch and panel width, then the batches per shared factorization.  The winners are cached in ``tuned.json`` next to this file, keyed by
 the Ne bucket (powers of two) and the GPU's SM count; ``tuned_opts()`` looks
 them up so that a SweepPlan created without explicit options uses them.
 
@@ -26,6 +26,8 @@ PANELS = (128, 256, 512)
 # (tile_chain, tile_bulk, resident_chain, resident_bulk)
 TILES = ((256, 256, 0, 0), (128, 256, 0, 0), (256, 128, 0, 0), (128, 128, 0, 0), (256, 256, 1, 0),
          (256, 256, 0, 1), (256, 256, 1, 1))
+# batches per shared factorization (0: the library's automatic choice)
+SHARES = (0, 2, 4, 6, 8)
 
 
 def _key(Ne, sms):
@@ -46,15 +48,16 @@ def load_table():
 
 
 def tuned_opts(Ne, sms=None):
-    """(batch, lu_nb, tile_chain, tile_bulk, resident_chain, resident_bulk)
-    for this size on this GPU, or None when untuned (0 = the library's default)."""
+    """(batch, lu_nb, tile_chain, tile_bulk, resident_chain, resident_bulk,
+    share_factors) for this size on this GPU, or None when untuned (0 = the
+    library's default)."""
     try:
         sms = sms or _sms()
     except Exception:  # noqa: BLE001 - no torch/GPU: no table lookup
         return None
     e = load_table().get(_key(Ne, sms))
     return ((e["batch"], e["lu_nb"], e.get("tile_chain", 0), e.get("tile_bulk", 0), e.get("resident_chain", 0),
-             e.get("resident_bulk", 0)) if e else None)
+             e.get("resident_bulk", 0), e.get("share_factors", 0)) if e else None)
 
 
 def _time(plan_args, freqs, repeats, **kw):
@@ -78,39 +81,57 @@ def _time(plan_args, freqs, repeats, **kw):
     return Ne, ((repeats * len(freqs) / dt) if ok else None)
 
 
-def tune(plan_args, freqs, candidates=None, repeats=1, save=True, tiles=True):
+def tune(plan_args, freqs, candidates=None, repeats=1, save=True, tiles=True, shares=True):
     """Time every (batch, lu_nb) candidate on the sweep of ``freqs``, then
-    (with ``tiles``) the tile-width pairs at the winner.
+    (with ``tiles``) the tile-width pairs and resident variants at the
+    winner, then (with ``shares``) the batches per shared factorization.
 
     plan_args: the positional arguments of SweepPlan (geometry .. Z0).
     Returns (best, results): best = (batch, lu_nb, tile_chain, tile_bulk,
-    resident_chain, resident_bulk), results[best-like tuple] = points/s or None.
+    resident_chain, resident_bulk, share_factors), results[best-like tuple]
+    = points/s or None.  A later stage's variant replaces the earlier
+    winner only if it is more than 1 % faster (the run-to-run noise of a
+    sweep).
     """
     cands = candidates or [(b, p) for b in BATCHES for p in PANELS]
     results = {}
     Ne = None
+
+    def run(key):
+        nonlocal Ne
+        if key not in results:
+            b, p, tc, tb, rc, rb, g = key
+            Ne, results[key] = _time(plan_args, freqs, repeats, batch=b, lu_nb=p, tile_chain=tc, tile_bulk=tb,
+                                     resident_chain=rc, resident_bulk=rb, share_factors=g)
+
+    def pick(keys, base):
+        good = {k: results[k] for k in keys if results.get(k)}
+        if not good:
+            return None
+        best = max(good, key=good.get)
+        if results.get(base) and good[best] < 1.01 * results[base]:
+            return base
+        return best
+
     for batch, panel in cands:
-        Ne, results[(batch, panel, 256, 256, 0, 0)] = _time(plan_args, freqs, repeats, batch=batch, lu_nb=panel,
-                                                            tile_chain=256, tile_bulk=256)
+        run((batch, panel, 256, 256, 0, 0, 0))
     good = {k: v for k, v in results.items() if v}
     best = max(good, key=good.get) if good else None
     if best and tiles:
-        for tc, tb, rc, rb in TILES:
-            key = (best[0], best[1], tc, tb, rc, rb)
-            if key not in results:
-                _, results[key] = _time(plan_args, freqs, repeats, batch=best[0], lu_nb=best[1], tile_chain=tc,
-                                        tile_bulk=tb, resident_chain=rc, resident_bulk=rb)
-        good = {k: v for k, v in results.items() if v}
-        best = max(good, key=good.get)
-        # a variant must beat the default kernels by more than 1 % (run-to-run
-        # noise of a sweep) to replace them
-        base = good.get(tuple(best[:2]) + (256, 256, 0, 0))
-        if base and good[best] < 1.01 * base:
-            best = tuple(best[:2]) + (256, 256, 0, 0)
+        keys = [best[:2] + t + (0,) for t in TILES]
+        for k in keys:
+            run(k)
+        best = pick(keys, best[:2] + (256, 256, 0, 0, 0))
+    if best and shares:
+        keys = [best[:6] + (g,) for g in SHARES]
+        for k in keys:
+            run(k)
+        best = pick(keys, best[:6] + (0,))
     if save and best:
         table = load_table()
         table[_key(Ne, _sms())] = dict(batch=best[0], lu_nb=best[1], tile_chain=best[2], tile_bulk=best[3],
-                                       resident_chain=best[4], resident_bulk=best[5], points_per_s=good[best],
+                                       resident_chain=best[4], resident_bulk=best[5], share_factors=best[6],
+                                       points_per_s=results[best],
                                        candidates={"/".join(str(x) for x in k): v for k, v in results.items()})
         with open(TABLE, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
